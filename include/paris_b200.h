@@ -1,0 +1,196 @@
+/*
+ * paris_b200.h -- C-ABI of the B200 (sm_100a) grid core of the PARIS two-phase
+ * flow solver: split PLIC VOF advection, height-function curvature with the CSF
+ * surface-tension force, and the variable-density multigrid pressure projection.
+ *
+ * Every entry point takes plain pointers and sizes and returns an int status
+ * (PARIS_OK on success).  Host arrays use the reference's Fortran layout:
+ * real(8) arrays dimensioned (imin:imax, jmin:jmax, kmin:kmax) with Ng ghost
+ * layers, i fastest, exactly as the module globals of PARIS are allocated
+ * (paris.f90:3016-3031, vofmodules.f90:430).  The matrix A has the layout
+ * A(is:ie, js:je, ks:ke, 8) (modules.f90:2729).  Fields live on the device
+ * between calls; upload/download move them to and from the Fortran arrays.
+ *
+ * A Fortran driver binds these with ISO_C_BINDING; the interface module that
+ * keeps the original subroutine names is shown in INTEGRATION.md.
+ */
+#ifndef PARIS_B200_H
+#define PARIS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PARIS_OK             0
+#define PARIS_NOT_CONVERGED  1  /* solver hit maxit: the reference sets it=maxit+1 and warns (MGsolver.f90:402) */
+#define PARIS_NAN_DETECTED   2  /* NaN in A or p (newsolver.f90:138-173 catch_divergence) */
+#define PARIS_BAD_ARGS       3  /* invalid sizes, options or pointers */
+#define PARIS_CUDA_ERROR     4  /* a CUDA runtime call failed */
+#define PARIS_SETUP_ERROR    5  /* check_poisson_setup failed (newsolver.f90:275-344) */
+#define PARIS_NO_DEVICE      6  /* no usable CUDA device */
+
+/* ---- boundary conditions ----------------------------------------------- */
+/* BDRY_COND of the &PARAMETERS namelist (order x- y- z- x+ y+ z+).          */
+#define PARIS_BC_WALL      0
+#define PARIS_BC_PERIODIC  1
+#define PARIS_BC_SHEAR     2   /* a wall for the pressure equation (modules.f90:925) */
+/* vofbdry_cond of &VOFPARAMETERS (SetVOFBC, vofmodules.f90:1694-1825).      */
+#define PARIS_VOFBC_DRY       0
+#define PARIS_VOFBC_WET       1
+#define PARIS_VOFBC_PERIODIC  3
+#define PARIS_VOFBC_OUTFLOW   4
+
+/* VOF_advect of &VOFPARAMETERS */
+#define PARIS_ADVECT_CIAM  0   /* 'CIAM'      -> swpz (vofnonmodule.f90:126)  */
+#define PARIS_ADVECT_WY    1   /* 'Dick_Yue'  -> swpr (vofnonmodule.f90:664)  */
+
+/* DensMean / ViscMean flags of linfunc (vofmodules.f90:171) */
+#define PARIS_MEAN_ARITH  101  /* ArithMean, vofmodules.f90:109 */
+#define PARIS_MEAN_HARM   102  /* HarmMean,  vofmodules.f90:110 */
+
+/* ---- grid and physical parameters -------------------------------------- */
+typedef struct paris_grid_desc {
+    int32_t nx, ny, nz;          /* Nx, Ny, Nz: interior cells (one rank, no MPI split) */
+    int32_t ng;                  /* Ng of the host arrays; must be 2 (modules.f90 Ng) */
+    int32_t bdry_cond[6];        /* PARIS_BC_*, order x- y- z- x+ y+ z+ */
+    int32_t vofbdry_cond[6];     /* PARIS_VOFBC_* */
+    double  xlength, ylength, zlength;  /* XLENGTH/YLENGTH/ZLENGTH; uniform grid (xform=0) */
+    int32_t vof_advect;          /* PARIS_ADVECT_* */
+    int32_t dens_mean;           /* PARIS_MEAN_* used by paris_linfunc for rho */
+    int32_t visc_mean;           /* PARIS_MEAN_* used by paris_linfunc for mu */
+    int32_t nfilter;             /* 0 or 1 (27-point filter in linfunc) */
+    double  rho1, rho2;          /* RHO1 (cvof=0), RHO2 (cvof=1) */
+    double  mu1, mu2;            /* MU1, MU2 */
+    double  sigma;               /* SIGMA */
+    double  epsc;                /* EPSC, default 1e-12 */
+    int32_t nrelax;              /* smoothing sweeps per level of the reference MG (default 3) */
+    int32_t sym_mg;              /* sym_MG flag of the reference MG */
+    int32_t device;              /* CUDA device ordinal */
+    int32_t mixed_heights;       /* mixed_heights flag of the curvature (default 1) */
+    int32_t use_full_heights;    /* use_full_heights flag (default 1) */
+    int32_t do_rotation;         /* do_rotation flag of the paraboloid fit (default 0) */
+    int32_t reserved[4];
+} paris_grid_desc;
+
+typedef struct paris_ctx* paris_handle_t;
+
+/* ---- fields ------------------------------------------------------------ */
+#define PARIS_FIELD_CVOF      0   /* cvof, cell centres */
+#define PARIS_FIELD_U         1   /* u at faces i+1/2 */
+#define PARIS_FIELD_V         2
+#define PARIS_FIELD_W         3
+#define PARIS_FIELD_RHO       4
+#define PARIS_FIELD_P         5
+#define PARIS_FIELD_DU        6   /* momentum source du,dv,dw (surfaceForce output) */
+#define PARIS_FIELD_DV        7
+#define PARIS_FIELD_DW        8
+#define PARIS_FIELD_KAPPA     9   /* curvature (cell units, 2e6 = uncomputed) */
+#define PARIS_FIELD_MU       10
+#define PARIS_FIELD_VOF_FLAG 11   /* integer vof_flag (host int32) */
+#define PARIS_FIELD_A        12   /* A(is:ie,js:je,ks:ke,8), no ghosts */
+#define PARIS_FIELD_HEIGHT   13   /* height(imin:imax,...,6) */
+#define PARIS_FIELD_VOF_PHASE 14  /* integer vof_phase (host int32) */
+#define PARIS_NFIELDS        15
+
+/* ---- life cycle (replaces the allocations of initialize/initialize_VOF,
+ *      paris.f90:3016-3031 and init_MG, MGsolver.f90:34-65) --------------- */
+int paris_gpu_init(const paris_grid_desc* desc, paris_handle_t* out);
+int paris_gpu_finalize(paris_handle_t h);
+/* Copy one field between the device mirror and a host array in the reference
+ * layout (ghost layers included; only the interior is transferred, ghosts are
+ * rebuilt on the device from the boundary conditions).  VOF_FLAG/VOF_PHASE
+ * take int32 arrays, every other field real(8).                           */
+int paris_gpu_upload(paris_handle_t h, int32_t field, const void* host);
+int paris_gpu_download(paris_handle_t h, int32_t field, void* host);
+/* Block until all work queued on the handle's stream has finished. */
+int paris_gpu_sync(paris_handle_t h);
+/* The cudaStream_t the handle issues all work on (as void*). */
+void* paris_gpu_stream(paris_handle_t h);
+/* Device pointer of a field (interior-only, i fastest; A: 8 components). */
+void* paris_gpu_field_ptr(paris_handle_t h, int32_t field);
+/* Text of the last error recorded on the handle (never NULL). */
+const char* paris_gpu_last_error(paris_handle_t h);
+/* Number of kernels this handle launched since creation (launch counter). */
+int64_t paris_gpu_launch_count(paris_handle_t h);
+
+/* ---- VOF (replaces vofsweeps, vofmodules.f90:1340-1361, with
+ *      swp/swpz/swpr, vofnonmodule.f90:27-48,126-237,664-754) ------------ */
+int paris_vof_sweeps(paris_handle_t h, int32_t tswap, double dt);
+/* linfunc(field,a1,a2,MeanFlag), vofmodules.f90:171-218; which = RHO or MU */
+int paris_linfunc(paris_handle_t h, int32_t which);
+/* Initial condition: union of spheres by ls2vof_refined
+ * (vofmodules.f90:1195-1293 with shapes2ls :973-993).                      */
+int paris_init_spheres(paris_handle_t h, int32_t nb, const double* xc, const double* yc,
+                       const double* zc, const double* rad, int32_t refinement);
+
+/* ---- heights, curvature, CSF ------------------------------------------- */
+/* get_all_heights, surface_tension.f90:185-260 */
+int paris_get_all_heights(paris_handle_t h);
+/* get_all_curvatures, surface_tension.f90:620-755; kappa_host may be NULL  */
+int paris_get_all_curvatures(paris_handle_t h, double* kappa_host);
+/* surfaceForce(du,dv,dw,rho), paris.f90:2862-2957 (adds to du,dv,dw) */
+int paris_surface_force(paris_handle_t h);
+
+/* ---- pressure projection ---------------------------------------------- */
+/* SetPressureBC + SetupPoisson + Poisson_BCs + check_poisson_setup,
+ * modules.f90:916-949,2722-2892; newsolver.f90:275-344                     */
+int paris_setup_poisson(paris_handle_t h, double dt, double volume_source);
+/* Setup_testMG, modules.f90:3160-3192 (known-answer RHS)                   */
+int paris_setup_test_mg(paris_handle_t h);
+
+#define PARIS_MG_REFERENCE  0  /* FP64, the reference V-cycle step for step (MGsolver.f90:253-405) */
+#define PARIS_MG_FP64       1  /* FP64 V(nu1,nu2) cycles in an FP64 defect-correction loop     */
+#define PARIS_MG_MIXED      2  /* FP32 V(nu1,nu2) cycles in an FP64 defect-correction loop     */
+
+typedef struct paris_solve_opts {
+    double  max_error;   /* stop when the residual norm (order `norm`, RMS) < max_error:
+                            the reference's maxError/MaxDt (paris.f90:499)              */
+    double  rel_tol;     /* if > 0, stop instead when ||r||_2 / ||b||_2 < rel_tol        */
+    double  beta;        /* BETA, relaxation factor of RedBlackRelax                     */
+    int32_t maxit;       /* MAXIT                                                         */
+    int32_t norm;        /* ResNormOrderPressure: 1 or 2                                  */
+    int32_t mode;        /* PARIS_MG_*                                                    */
+    int32_t nu1, nu2;    /* pre/post smoothing sweeps of the FP64/MIXED cycles (2,2)      */
+    int32_t pcg;         /* FP64/MIXED: 1 = use the V-cycle as a CG preconditioner        */
+    int32_t reserved[3];
+} paris_solve_opts;
+
+typedef struct paris_solve_result {
+    int32_t it;          /* cycles run; maxit+1 when not converged (reference convention) */
+    int32_t reserved;
+    double  res;         /* tres2: residual in the reference norm at exit                 */
+    double  rel_res;     /* ||r||_2 / ||b||_2 at exit                                     */
+    double  res0;        /* residual norm before the first cycle                          */
+} paris_solve_result;
+
+/* NewSolver(A,p,maxError,beta,maxit,it,ierr,norm), newsolver.f90:34-57 ->
+ * NewSolverMG, MGsolver.f90:346-405.  Solves for p (device field P) with the
+ * matrix built by paris_setup_poisson (or uploaded as PARIS_FIELD_A).       */
+int paris_new_solver(paris_handle_t h, const paris_solve_opts* opts, paris_solve_result* res);
+/* calcResiduals, modules.f90:3313-3387: out[0..2] = L1, L2, Linf */
+int paris_calc_residuals(paris_handle_t h, double* out3);
+/* get_MGtest_err, MGsolver.f90:407-426 (L1 error vs sin*sin*sin / L1 ref) */
+int paris_mg_test_err(paris_handle_t h, double* err);
+/* project_velocity, paris.f90:882-909 */
+int paris_project_velocity(paris_handle_t h, double dt);
+
+/* ---- projection adjoint (no counterpart in the reference: the transpose of
+ *      SetupPoisson modules.f90:2735-2745 + solve + project_velocity
+ *      paris.f90:898-909).  With u = u* - dt*B*G*p and A(B) p = -D u*,
+ *      given g_u = dL/du (three face fields, reference layout with ghosts),
+ *      returns dL/du* (three face fields) and dL/dB, B being the face
+ *      coefficient 2/(rho_c + rho_n) of each face (three face fields).
+ *      The forward p (checkpointed on the device by the last solve) is used.  */
+int paris_projection_adjoint(paris_handle_t h, double dt,
+                             const double* gu, const double* gv, const double* gw,
+                             double* gus, double* gvs, double* gws,
+                             double* gbx, double* gby, double* gbz,
+                             const paris_solve_opts* opts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PARIS_B200_H */

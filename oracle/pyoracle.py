@@ -1,0 +1,214 @@
+"""ctypes binding of the CPU oracle (liboracle.so).
+
+Test infrastructure only: the parity checker used by tests/, by
+__graft_entry__.smoke() and by the cpu_baseline leg of bench.py.  Arrays are
+numpy float64/int32 arrays of shape (Nzt, Nyt, Nxt) (= Fortran
+(imin:imax,jmin:jmax,kmin:kmax), i fastest), the matrix A has shape
+(8, nz, ny, nx) (= A(is:ie,js:je,ks:ke,8)).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+
+def _grid_desc_type():
+    import sys
+    root = os.path.dirname(HERE)
+    if root not in sys.path:
+        sys.path.insert(0, root)
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    return pkg.capi
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        _lib = ctypes.CDLL(LIB)
+        P = ctypes.c_void_p
+        D = ctypes.c_double
+        I = ctypes.c_int
+        capi = _grid_desc_type()
+        G = ctypes.POINTER(capi.GridDesc)
+        protos = {
+            "og_setup_poisson": (I, [G, P, P, P, P, D, D, P]),
+            "og_setup_testmg": (I, [G, P, P]),
+            "og_new_solver_mg": (I, [G, P, P, D, D, I, I, P, P, P]),
+            "og_calc_residual": (D, [G, P, P, I]),
+            "og_mgtest_err": (D, [G, P]),
+            "og_project_velocity": (I, [G, P, P, P, P, P, D]),
+            "og_fill_ghosts": (None, [G, P]),
+            "og_vofsweeps": (I, [G, I, D, P, P, P, P, P, P]),
+            "og_flags_clip": (I, [G, P, P]),
+            "og_linfunc": (I, [G, P, P, D, D, I]),
+            "og_init_spheres": (I, [G, I, P, P, P, P, I, I, P, P, P]),
+            "og_fastmg_solve": (I, [G, P, P, D, I, I, I, I, I, P]),
+            "og_al3d": (D, [P, D]),
+            "og_cc3d": (D, [P, D]),
+            "og_fl3d": (D, [P, D, P, P]),
+            "og_area3d": (D, [P, D]),
+            "og_area_centroid": (None, [P, D, P]),
+            "og_mycs": (None, [P, P]),
+            "og_fd32": (None, [P, P]),
+        }
+        for name, (res, args) in protos.items():
+            f = getattr(_lib, name)
+            f.restype = res
+            f.argtypes = args
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def shape(desc):
+    return (desc.nz + 2 * desc.ng, desc.ny + 2 * desc.ng, desc.nx + 2 * desc.ng)
+
+
+def zeros(desc, dtype=np.float64):
+    return np.zeros(shape(desc), dtype=dtype)
+
+
+def interior(desc, a):
+    g = desc.ng
+    return a[g:g + desc.nz, g:g + desc.ny, g:g + desc.nx]
+
+
+def fill_ghosts(desc, F):
+    lib().og_fill_ghosts(ctypes.byref(desc), _p(F))
+
+
+def setup_poisson(desc, u, v, w, rho, dt, volsrc=0.0):
+    A = np.zeros((8, desc.nz, desc.ny, desc.nx))
+    st = lib().og_setup_poisson(ctypes.byref(desc), _p(u), _p(v), _p(w), _p(rho), dt, volsrc, _p(A))
+    return st, A
+
+
+def setup_testmg(desc, rho):
+    A = np.zeros((8, desc.nz, desc.ny, desc.nx))
+    lib().og_setup_testmg(ctypes.byref(desc), _p(rho), _p(A))
+    return A
+
+
+def new_solver_mg(desc, A, p, max_error, beta=1.0, maxit=20, norm=2):
+    """NewSolverMG on (A, p); p updated in place. Returns (status, it, tres2, history)."""
+    it = ctypes.c_int(0)
+    t = ctypes.c_double(0)
+    hist = np.zeros(max(maxit, 1))
+    st = lib().og_new_solver_mg(ctypes.byref(desc), _p(np.ascontiguousarray(A)), _p(p), max_error,
+                                beta, maxit, norm, ctypes.byref(it), ctypes.byref(t), _p(hist))
+    return st, it.value, t.value, hist[:min(it.value, maxit)]
+
+
+def calc_residual(desc, A, p, normorder):
+    return lib().og_calc_residual(ctypes.byref(desc), _p(A), _p(p), normorder)
+
+
+def mgtest_err(desc, p):
+    return lib().og_mgtest_err(ctypes.byref(desc), _p(p))
+
+
+def project_velocity(desc, u, v, w, p, rho, dt):
+    return lib().og_project_velocity(ctypes.byref(desc), _p(u), _p(v), _p(w), _p(p), _p(rho), dt)
+
+
+def vofsweeps(desc, tswap, dt, cvof, flag, u, v, w, phase=None):
+    return lib().og_vofsweeps(ctypes.byref(desc), tswap, dt, _p(cvof), _p(flag), _p(phase),
+                              _p(u), _p(v), _p(w))
+
+
+def flags_clip(desc, c, f):
+    return lib().og_flags_clip(ctypes.byref(desc), _p(c), _p(f))
+
+
+def linfunc(desc, cvof, a1, a2, meanflag):
+    field = zeros(desc)
+    lib().og_linfunc(ctypes.byref(desc), _p(field), _p(cvof), a1, a2, meanflag)
+    return field
+
+
+def init_spheres(desc, centers, radii, refinement=8, jacobi=False):
+    """levelset2vof(shapes2ls): jacobi=False is the reference's in-place loop
+    order; True reads pass-1 flags only (the device's order-free variant)."""
+    c = np.ascontiguousarray(np.asarray(centers, dtype=np.float64).reshape(-1, 3))
+    r = np.ascontiguousarray(np.asarray(radii, dtype=np.float64).reshape(-1))
+    xc, yc, zc = (np.ascontiguousarray(c[:, a]) for a in range(3))
+    cvof = zeros(desc)
+    flag = zeros(desc, np.int32)
+    phase = zeros(desc, np.int32)
+    lib().og_init_spheres(ctypes.byref(desc), len(r), _p(xc), _p(yc), _p(zc), _p(r), refinement,
+                          1 if jacobi else 0, _p(cvof), _p(flag), _p(phase))
+    return cvof, flag, phase
+
+
+def _v3(n):
+    return np.ascontiguousarray(np.asarray(n, dtype=np.float64).reshape(3))
+
+
+def al3d(n, c):
+    return lib().og_al3d(_p(_v3(n)), c)
+
+
+def cc3d(n, alpha):
+    return lib().og_cc3d(_p(_v3(n)), alpha)
+
+
+def fl3d(n, alpha, x0, dx):
+    return lib().og_fl3d(_p(_v3(n)), alpha, _p(_v3(x0)), _p(_v3(dx)))
+
+
+def area3d(n, c):
+    return lib().og_area3d(_p(_v3(n)), c)
+
+
+def area_centroid(n, c):
+    out = np.zeros(3)
+    lib().og_area_centroid(_p(_v3(n)), c, _p(out))
+    return out
+
+
+def mycs(block):
+    """block: 3x3x3 array indexed [i,j,k] (Fortran c(0:2,0:2,0:2))."""
+    b = np.ascontiguousarray(np.asarray(block, dtype=np.float64).transpose(2, 1, 0))
+    out = np.zeros(3)
+    lib().og_mycs(_p(b), _p(out))
+    return out
+
+
+def grid_coords(desc):
+    """x, xh, dx, dxh (and y, z) of paris.f90:3057-3100, index = Fortran-1."""
+    out = {}
+    for ax, n, L in (("x", desc.nx, desc.xlength), ("y", desc.ny, desc.ylength), ("z", desc.nz, desc.zlength)):
+        ng = desc.ng
+        nt = n + 2 * ng
+        xh = np.array([L * (0.0 * s * (0.5 - s) * (1.0 - s) + s) for s in ((f - ng) / n for f in range(1, nt + 1))])
+        x = np.zeros(nt)
+        x[1:] = 0.5 * (xh[1:] + xh[:-1])
+        x[0] = 2.0 * xh[0] - x[1]
+        out[ax] = x
+        out[ax + "h"] = xh
+    return out
+
+
+def fastmg_solve(desc, A, p_int, rel_tol, maxit=100, mixed=True, pcg=False, nu1=2, nu2=2):
+    """The B200 solver's own MG restated on the CPU; p_int: interior (nz,ny,nx)."""
+    hist = np.zeros(maxit)
+    p = np.ascontiguousarray(p_int, dtype=np.float64)
+    it = lib().og_fastmg_solve(ctypes.byref(desc), _p(np.ascontiguousarray(A)), _p(p), rel_tol, maxit,
+                               1 if mixed else 0, 1 if pcg else 0, nu1, nu2, _p(hist))
+    return p, it, hist[:it]

@@ -1,0 +1,165 @@
+"""ctypes view of the C-ABI declared in include/paris_b200.h.
+
+The structures mirror the header field for field; `load_library()` opens the
+in-tree shared library built by `build.py` and declares every entry point.
+There is no fallback: a missing or unloadable library raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBNAME = "libparis_b200.so"
+
+# status codes
+OK, NOT_CONVERGED, NAN_DETECTED, BAD_ARGS, CUDA_ERROR, SETUP_ERROR, NO_DEVICE = range(7)
+STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "NAN_DETECTED", 3: "BAD_ARGS",
+                4: "CUDA_ERROR", 5: "SETUP_ERROR", 6: "NO_DEVICE"}
+
+# boundary conditions
+BC_WALL, BC_PERIODIC, BC_SHEAR = 0, 1, 2
+VOFBC_DRY, VOFBC_WET, VOFBC_PERIODIC, VOFBC_OUTFLOW = 0, 1, 3, 4
+ADVECT_CIAM, ADVECT_WY = 0, 1
+MEAN_ARITH, MEAN_HARM = 101, 102
+
+# fields
+(F_CVOF, F_U, F_V, F_W, F_RHO, F_P, F_DU, F_DV, F_DW, F_KAPPA, F_MU, F_VOF_FLAG,
+ F_A, F_HEIGHT, F_VOF_PHASE) = range(15)
+
+# solver modes
+MG_REFERENCE, MG_FP64, MG_MIXED = 0, 1, 2
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+        ("ng", ctypes.c_int32),
+        ("bdry_cond", ctypes.c_int32 * 6),
+        ("vofbdry_cond", ctypes.c_int32 * 6),
+        ("xlength", ctypes.c_double), ("ylength", ctypes.c_double), ("zlength", ctypes.c_double),
+        ("vof_advect", ctypes.c_int32),
+        ("dens_mean", ctypes.c_int32),
+        ("visc_mean", ctypes.c_int32),
+        ("nfilter", ctypes.c_int32),
+        ("rho1", ctypes.c_double), ("rho2", ctypes.c_double),
+        ("mu1", ctypes.c_double), ("mu2", ctypes.c_double),
+        ("sigma", ctypes.c_double),
+        ("epsc", ctypes.c_double),
+        ("nrelax", ctypes.c_int32),
+        ("sym_mg", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+        ("mixed_heights", ctypes.c_int32),
+        ("use_full_heights", ctypes.c_int32),
+        ("do_rotation", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 4),
+    ]
+
+
+class SolveOpts(ctypes.Structure):
+    _fields_ = [
+        ("max_error", ctypes.c_double),
+        ("rel_tol", ctypes.c_double),
+        ("beta", ctypes.c_double),
+        ("maxit", ctypes.c_int32),
+        ("norm", ctypes.c_int32),
+        ("mode", ctypes.c_int32),
+        ("nu1", ctypes.c_int32), ("nu2", ctypes.c_int32),
+        ("pcg", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 3),
+    ]
+
+
+class SolveResult(ctypes.Structure):
+    _fields_ = [
+        ("it", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("res", ctypes.c_double), ("rel_res", ctypes.c_double), ("res0", ctypes.c_double),
+    ]
+
+
+def make_desc(n, length=(1.0, 1.0, 1.0), bc="periodic", vofbc=None, advect=ADVECT_CIAM,
+              rho1=1.0, rho2=1.0, mu1=0.0, mu2=0.0, sigma=0.0, epsc=1e-12, nrelax=3,
+              sym_mg=0, nfilter=0, dens_mean=MEAN_ARITH, visc_mean=MEAN_ARITH, device=0,
+              mixed_heights=1, use_full_heights=1, do_rotation=0):
+    """Grid descriptor with the reference's namelist defaults.
+
+    bc: "periodic", "wall", or a 6-sequence of BDRY_COND codes (x- y- z- x+ y+ z+).
+    vofbc: None (periodic where bc is periodic, 'dry' at walls) or 6 codes.
+    """
+    d = GridDesc()
+    d.nx, d.ny, d.nz = (int(v) for v in n)
+    d.ng = 2
+    if bc == "periodic":
+        bcs = [BC_PERIODIC] * 6
+    elif bc == "wall":
+        bcs = [BC_WALL] * 6
+    else:
+        bcs = list(bc)
+    if vofbc is None:
+        vofbc = [VOFBC_PERIODIC if b == BC_PERIODIC else VOFBC_DRY for b in bcs]
+    for i in range(6):
+        d.bdry_cond[i] = bcs[i]
+        d.vofbdry_cond[i] = vofbc[i]
+    d.xlength, d.ylength, d.zlength = (float(v) for v in length)
+    d.vof_advect = advect
+    d.dens_mean, d.visc_mean, d.nfilter = dens_mean, visc_mean, nfilter
+    d.rho1, d.rho2, d.mu1, d.mu2, d.sigma, d.epsc = rho1, rho2, mu1, mu2, sigma, epsc
+    d.nrelax, d.sym_mg, d.device = nrelax, sym_mg, device
+    d.mixed_heights, d.use_full_heights, d.do_rotation = mixed_heights, use_full_heights, do_rotation
+    return d
+
+
+def lib_path():
+    return os.path.join(HERE, LIBNAME)
+
+
+_LIB = None
+
+_P = ctypes.c_void_p
+_D = ctypes.c_double
+_I = ctypes.c_int32
+_PROTOS = {
+    "paris_gpu_init": (_I, [ctypes.POINTER(GridDesc), ctypes.POINTER(_P)]),
+    "paris_gpu_finalize": (_I, [_P]),
+    "paris_gpu_upload": (_I, [_P, _I, _P]),
+    "paris_gpu_download": (_I, [_P, _I, _P]),
+    "paris_gpu_sync": (_I, [_P]),
+    "paris_gpu_stream": (_P, [_P]),
+    "paris_gpu_field_ptr": (_P, [_P, _I]),
+    "paris_gpu_last_error": (ctypes.c_char_p, [_P]),
+    "paris_gpu_launch_count": (ctypes.c_int64, [_P]),
+    "paris_vof_sweeps": (_I, [_P, _I, _D]),
+    "paris_linfunc": (_I, [_P, _I]),
+    "paris_init_spheres": (_I, [_P, _I, _P, _P, _P, _P, _I]),
+    "paris_get_all_heights": (_I, [_P]),
+    "paris_get_all_curvatures": (_I, [_P, _P]),
+    "paris_surface_force": (_I, [_P]),
+    "paris_setup_poisson": (_I, [_P, _D, _D]),
+    "paris_setup_test_mg": (_I, [_P]),
+    "paris_new_solver": (_I, [_P, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveResult)]),
+    "paris_calc_residuals": (_I, [_P, _P]),
+    "paris_mg_test_err": (_I, [_P, _P]),
+    "paris_project_velocity": (_I, [_P, _D]),
+    "paris_projection_adjoint": (_I, [_P, _D, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                                      ctypes.POINTER(SolveOpts)]),
+}
+
+
+def exported_names():
+    return list(_PROTOS)
+
+
+def load_library(path=None):
+    """Open the CUDA library; raises OSError when it is missing (no fallback)."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = path or lib_path()
+    if not os.path.exists(p):
+        raise OSError(f"{p} not built: run __graft_entry__.build() (nvcc, sm_100a)")
+    lib = ctypes.CDLL(p)
+    for name, (res, args) in _PROTOS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _LIB = lib
+    return lib

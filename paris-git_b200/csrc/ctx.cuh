@@ -1,0 +1,87 @@
+// ctx.cuh -- the device-resident state behind a paris_handle_t and the
+// internal entry points shared by the .cu files of the library.
+#pragma once
+#include <vector>
+#include "common.cuh"
+
+// One level of the reference multigrid (DataMG/pMG/EMG of MGsolver.f90:26-30),
+// interior-only arrays; the one-layer halo is resolved in the kernels
+// (periodic wrap, zero at walls where ghost_MG_* never writes).
+struct RefLevel {
+    int n[3];
+    long N;
+    double* K;   // 8*N
+    double* p;   // pMG
+    double* e;   // EMG
+};
+
+// One level of the B200 multigrid: face coefficients (east/north/top of each
+// cell) and work vectors, in T = float (inner cycle of the mixed solver) and
+// double (the FP64 solver).
+template <typename T>
+struct FastLevel {
+    int n[3];
+    long N;
+    T *cx, *cy, *cz;
+    T *b, *x;
+};
+
+struct paris_ctx {
+    paris_grid_desc d;
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    Layout L;
+    Bnd bnd;
+    long N = 0;               // interior cells
+    // metrics (index i+ng, i interior-relative), device copies
+    double *dx = nullptr, *dxh = nullptr, *dy = nullptr, *dyh = nullptr, *dz = nullptr, *dzh = nullptr;
+    double *xc = nullptr, *yc = nullptr, *zc = nullptr;   // cell centres x(i), y(j), z(k)
+    std::vector<double> h_dx, h_dxh, h_dy, h_dyh, h_dz, h_dzh, h_x, h_y, h_z;
+    // ghosted fields (index PARIS_FIELD_*; VOF_FLAG/A/HEIGHT/PHASE kept apart)
+    double* fld[PARIS_NFIELDS] = {};
+    double* c2 = nullptr;          // second cvof buffer of the sweeps
+    int8_t* flag = nullptr;        // vof_flag (ghosted)
+    uint8_t* cg = nullptr;         // c_mask of the Weymouth-Yue sweeps
+    double* height = nullptr;      // 6 ghosted fields
+    int32_t* i32stage = nullptr;   // staging for int32 host transfers
+    // pressure equation, compact interior arrays (N each)
+    double *cx = nullptr, *cy = nullptr, *cz = nullptr, *rhs = nullptr;
+    double* A = nullptr;           // 8*N, reference layout, built on demand
+    int have_matrix = 0;           // cx/cy/cz/rhs valid
+    int A_valid = 0;               // A consistent with cx/cy/cz/rhs
+    int A_from_upload = 0;         // A given by the caller (not rebuilt)
+    double setup_dt = 0.0;
+    // reductions
+    double* red_part = nullptr;    // kRedBlocks partials * 4 slots
+    double* red_out = nullptr;     // device scalars
+    double* red_host = nullptr;    // pinned
+    // multigrid hierarchies
+    int ref_lmg = 0;
+    std::vector<RefLevel> ref;     // index 1..LMG
+    int fast_nl = 0;
+    std::vector<FastLevel<float>> fl32;
+    std::vector<FastLevel<double>> fl64;
+    double* fast_r64 = nullptr;    // PCG vectors (N each)
+    double* fast_d64 = nullptr;
+    double* fast_q64 = nullptr;
+    double* fast_z64 = nullptr;
+    double* fast_zold64 = nullptr;
+    int64_t launches = 0;
+    char err[512] = {0};
+};
+
+static constexpr int kRedBlocks = 1184;   // 148 SMs x 8
+
+// internal API (ctx.cu)
+int ctx_alloc_field(paris_ctx* c, int field);
+int ctx_ghost_fill(paris_ctx* c, double* f);         // do_all_ghost (periodic wrap)
+int ctx_ghost_fill_i8(paris_ctx* c, int8_t* f);
+int ctx_reduce_finish(paris_ctx* c, int nslots, double* out_host, int op_max = 0);
+int ctx_ensure_matrix(paris_ctx* c);
+
+// poisson.cu
+int poisson_build_full_A(paris_ctx* c);
+// mg_ref.cu
+int mg_ref_solve(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* r);
+// mg_fast.cu
+int mg_fast_solve(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* r);

@@ -1,0 +1,541 @@
+// mg_fast.cu -- the B200 multigrid for the variable-density pressure
+// equation (PARIS_MG_FP64 / PARIS_MG_MIXED).  It solves the system that
+// SetupPoisson builds (modules.f90:2735-2745), using that A is symmetric on
+// the uniform grid (A2(i) == A1(i+1)), so one coefficient per face is stored:
+//   level 0 faces = A2, A4, A6 of each cell; coarse face = (sum of the four
+//   fine faces across it) / 16; restriction = mean of the 8 children;
+//   prolongation = injection; red-black Gauss-Seidel V(nu1,nu2) cycles with
+//   the colours reversed after the coarse correction (symmetric cycle).
+// The inner cycle runs in T = float (mixed) or double; the outer loop is FP64:
+// defect correction p += V(b - A p), or CG preconditioned by the V-cycle.
+// Levels at or below kCoarseCells cells run in one single-block kernel.
+#include "ctx.cuh"
+
+static constexpr long kCoarseCells = 4096;   // 16^3
+static constexpr int kMaxLevels = 16;
+static constexpr int kCoarseSweeps = 8;
+
+template <typename T>
+struct LV {
+    const T *cx, *cy, *cz;
+    T *b, *x;
+    int n0, n1, n2;
+    long N;
+};
+
+template <typename T>
+struct LVSet {
+    LV<T> l[kMaxLevels];
+};
+
+// west/south/bottom face coefficient of cell (i,j,k)
+template <typename T>
+__device__ inline void west_coefs(const LV<T>& v, const Bnd& B, int i, int j, int k, long m, T& a1, T& a3, T& a5) {
+    a1 = i > 0 ? v.cx[m - 1] : (B.per[0] ? v.cx[m + v.n0 - 1] : (T)0);
+    a3 = j > 0 ? v.cy[m - v.n0] : (B.per[1] ? v.cy[m + (long)v.n0 * (v.n1 - 1)] : (T)0);
+    a5 = k > 0 ? v.cz[m - (long)v.n0 * v.n1] : (B.per[2] ? v.cz[m + (long)v.n0 * v.n1 * (v.n2 - 1)] : (T)0);
+}
+
+template <typename T>
+__device__ inline void nbrs(const LV<T>& v, const T* __restrict__ x, const Bnd& B, int i, int j, int k, long m, T& xw,
+                            T& xe, T& xs, T& xn, T& xb, T& xt) {
+    long sy = v.n0, sz = (long)v.n0 * v.n1;
+    xw = i > 0 ? x[m - 1] : (B.per[0] ? x[m + v.n0 - 1] : (T)0);
+    xe = i < v.n0 - 1 ? x[m + 1] : (B.per[0] ? x[m - (v.n0 - 1)] : (T)0);
+    xs = j > 0 ? x[m - sy] : (B.per[1] ? x[m + sy * (v.n1 - 1)] : (T)0);
+    xn = j < v.n1 - 1 ? x[m + sy] : (B.per[1] ? x[m - sy * (v.n1 - 1)] : (T)0);
+    xb = k > 0 ? x[m - sz] : (B.per[2] ? x[m + sz * (v.n2 - 1)] : (T)0);
+    xt = k < v.n2 - 1 ? x[m + sz] : (B.per[2] ? x[m - sz * (v.n2 - 1)] : (T)0);
+}
+
+template <typename T>
+__device__ inline void smooth_cell(const LV<T>& v, const Bnd& B, int i, int j, int k) {
+    long m = cidx(v.n0, v.n1, i, j, k);
+    T a1, a3, a5, xw, xe, xs, xn, xb, xt;
+    west_coefs(v, B, i, j, k, m, a1, a3, a5);
+    T a2 = v.cx[m], a4 = v.cy[m], a6 = v.cz[m];
+    nbrs(v, v.x, B, i, j, k, m, xw, xe, xs, xn, xb, xt);
+    T d = a1 + a2 + a3 + a4 + a5 + a6;
+    T s = a1 * xw + a2 * xe + a3 * xs + a4 * xn + a5 * xb + a6 * xt + v.b[m];
+    if (d > (T)0) v.x[m] = s / d;
+}
+
+template <typename T>
+__device__ inline T resid_cell(const LV<T>& v, const Bnd& B, int i, int j, int k) {
+    long m = cidx(v.n0, v.n1, i, j, k);
+    T a1, a3, a5, xw, xe, xs, xn, xb, xt;
+    west_coefs(v, B, i, j, k, m, a1, a3, a5);
+    T a2 = v.cx[m], a4 = v.cy[m], a6 = v.cz[m];
+    nbrs(v, v.x, B, i, j, k, m, xw, xe, xs, xn, xb, xt);
+    T d = a1 + a2 + a3 + a4 + a5 + a6;
+    return v.b[m] - d * v.x[m] + a1 * xw + a2 * xe + a3 * xs + a4 * xn + a5 * xb + a6 * xt;
+}
+
+// coarse rhs = mean of the 8 fine residuals
+template <typename T>
+__device__ inline void restrict_cell(const LV<T>& f, const LV<T>& c, const Bnd& B, int i, int j, int k) {
+    T s = 0;
+    for (int dk = 0; dk < 2; dk++)
+        for (int dj = 0; dj < 2; dj++)
+            for (int di = 0; di < 2; di++) s += resid_cell(f, B, 2 * i + di, 2 * j + dj, 2 * k + dk);
+    c.b[cidx(c.n0, c.n1, i, j, k)] = (T)0.125 * s;
+}
+
+template <typename T>
+__global__ void k_fast_smooth(const LV<T> v, const Bnd B, int color) {
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    int h0 = (v.n0 + 1) >> 1;
+    if (t >= (long)h0 * v.n1 * v.n2) return;
+    int ih = (int)(t % h0), j = (int)((t / h0) % v.n1), k = (int)(t / ((long)h0 * v.n1));
+    int i = 2 * ih + ((j + k + color) & 1);
+    if (i < v.n0) smooth_cell(v, B, i, j, k);
+}
+
+template <typename T>
+__global__ void k_fast_restrict(const LV<T> f, const LV<T> c, const Bnd B) {
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= c.N) return;
+    int i = (int)(t % c.n0), j = (int)((t / c.n0) % c.n1), k = (int)(t / ((long)c.n0 * c.n1));
+    restrict_cell(f, c, B, i, j, k);
+}
+
+template <typename T>
+__global__ void k_fast_prolong(const LV<T> f, const LV<T> c) {
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= f.N) return;
+    int i = (int)(t % f.n0), j = (int)((t / f.n0) % f.n1), k = (int)(t / ((long)f.n0 * f.n1));
+    f.x[t] += c.x[cidx(c.n0, c.n1, i >> 1, j >> 1, k >> 1)];
+}
+
+// The V-cycle from level L0 down to the coarsest, in one block.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_fast_coarse_cycle(const LVSet<T> S, int L0, int nl, const Bnd B, int nu1,
+                                                            int nu2) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    auto smooth = [&](const LV<T>& v, int color) {
+        int h0 = (v.n0 + 1) >> 1;
+        long tot = (long)h0 * v.n1 * v.n2;
+        for (long t = tid; t < tot; t += nt) {
+            int ih = (int)(t % h0), j = (int)((t / h0) % v.n1), k = (int)(t / ((long)h0 * v.n1));
+            int i = 2 * ih + ((j + k + color) & 1);
+            if (i < v.n0) smooth_cell(v, B, i, j, k);
+        }
+        __syncthreads();
+    };
+    for (int L = L0; L < nl; L++) {
+        const LV<T>& v = S.l[L];
+        for (long t = tid; t < v.N; t += nt) v.x[t] = (T)0;
+        __syncthreads();
+        if (L == nl - 1) {
+            for (int s = 0; s < kCoarseSweeps; s++) { smooth(v, 0); smooth(v, 1); }
+            for (int s = 0; s < kCoarseSweeps; s++) { smooth(v, 1); smooth(v, 0); }
+            break;
+        }
+        for (int s = 0; s < nu1; s++) { smooth(v, 0); smooth(v, 1); }
+        const LV<T>& c = S.l[L + 1];
+        for (long t = tid; t < c.N; t += nt) {
+            int i = (int)(t % c.n0), j = (int)((t / c.n0) % c.n1), k = (int)(t / ((long)c.n0 * c.n1));
+            restrict_cell(v, c, B, i, j, k);
+        }
+        __syncthreads();
+    }
+    for (int L = nl - 2; L >= L0; L--) {
+        const LV<T>& v = S.l[L];
+        const LV<T>& c = S.l[L + 1];
+        for (long t = tid; t < v.N; t += nt) {
+            int i = (int)(t % v.n0), j = (int)((t / v.n0) % v.n1), k = (int)(t / ((long)v.n0 * v.n1));
+            v.x[t] += c.x[cidx(c.n0, c.n1, i >> 1, j >> 1, k >> 1)];
+        }
+        __syncthreads();
+        for (int s = 0; s < nu2; s++) { smooth(v, 1); smooth(v, 0); }
+    }
+}
+
+// level-0 coefficients from the FP64 compact matrix
+template <typename T>
+__global__ void k_fast_coef0(const double* __restrict__ cx, const double* __restrict__ cy,
+                             const double* __restrict__ cz, T* ox, T* oy, T* oz, long N) {
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= N) return;
+    ox[t] = (T)cx[t]; oy[t] = (T)cy[t]; oz[t] = (T)cz[t];
+}
+
+// coarse face = (sum of the four fine faces on it) / 16
+template <typename T>
+__global__ void k_fast_coarsen(const LV<T> f, const LV<T> c, T* ccx, T* ccy, T* ccz) {
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= c.N) return;
+    int i = (int)(t % c.n0), j = (int)((t / c.n0) % c.n1), k = (int)(t / ((long)c.n0 * c.n1));
+    int I = 2 * i, J = 2 * j, K = 2 * k;
+    ccx[t] = (T)0.0625 * (f.cx[cidx(f.n0, f.n1, I + 1, J, K)] + f.cx[cidx(f.n0, f.n1, I + 1, J + 1, K)] +
+                          f.cx[cidx(f.n0, f.n1, I + 1, J, K + 1)] + f.cx[cidx(f.n0, f.n1, I + 1, J + 1, K + 1)]);
+    ccy[t] = (T)0.0625 * (f.cy[cidx(f.n0, f.n1, I, J + 1, K)] + f.cy[cidx(f.n0, f.n1, I + 1, J + 1, K)] +
+                          f.cy[cidx(f.n0, f.n1, I, J + 1, K + 1)] + f.cy[cidx(f.n0, f.n1, I + 1, J + 1, K + 1)]);
+    ccz[t] = (T)0.0625 * (f.cz[cidx(f.n0, f.n1, I, J, K + 1)] + f.cz[cidx(f.n0, f.n1, I + 1, J, K + 1)] +
+                          f.cz[cidx(f.n0, f.n1, I, J + 1, K + 1)] + f.cz[cidx(f.n0, f.n1, I + 1, J + 1, K + 1)]);
+}
+
+// ---- FP64 outer loop --------------------------------------------------------
+__device__ inline double pfield(const double* __restrict__ p, const Layout& L, const Bnd& B, int i, int j, int k) {
+    if (i < 0 || i >= L.n[0]) { if (!B.per[0]) return 0.0; i = i < 0 ? i + L.n[0] : i - L.n[0]; }
+    if (j < 0 || j >= L.n[1]) { if (!B.per[1]) return 0.0; j = j < 0 ? j + L.n[1] : j - L.n[1]; }
+    if (k < 0 || k >= L.n[2]) { if (!B.per[2]) return 0.0; k = k < 0 ? k + L.n[2] : k - L.n[2]; }
+    return p[lidx(L, i, j, k)];
+}
+
+// (A x)_m with the symmetric face form: A1 = cx(i-1), A2 = cx(i), ...,
+// A7 = A1+..+A6 in the reference's order.  x: ghosted field or compact.
+struct Mat64 {
+    const double *cx, *cy, *cz, *rhs;
+};
+
+__device__ inline double ax_compact(const Mat64& A, const double* __restrict__ x, const Layout& L, const Bnd& B,
+                                    int i, int j, int k, long m) {
+    LV<double> v{A.cx, A.cy, A.cz, nullptr, nullptr, L.n[0], L.n[1], L.n[2], 0};
+    double a1, a3, a5, xw, xe, xs, xn, xb, xt;
+    west_coefs(v, B, i, j, k, m, a1, a3, a5);
+    double a2 = A.cx[m], a4 = A.cy[m], a6 = A.cz[m];
+    nbrs(v, x, B, i, j, k, m, xw, xe, xs, xn, xb, xt);
+    double d = a1 + a2 + a3 + a4 + a5 + a6;
+    return d * x[m] - (a1 * xw + a2 * xe + a3 * xs + a4 * xn + a5 * xb + a6 * xt);
+}
+
+// r = b - A p on the ghosted p (wrap in the kernel); writes r as T into the
+// level-0 right-hand side (and as double into r64 when given).
+// slots: 0 = sum r^2, 1 = sum |r|, 2 = sum b^2
+template <typename T>
+__global__ void k_fast_residual64(const Mat64 A, const double* __restrict__ p, const Layout L, const Bnd B,
+                                  T* __restrict__ rT, double* __restrict__ r64, double* part) {
+    __shared__ double sh[32];
+    double s2 = 0.0, s1 = 0.0, sb = 0.0;
+    long N = (long)L.n[0] * L.n[1] * L.n[2];
+    for (long m = blockIdx.x * (long)blockDim.x + threadIdx.x; m < N; m += (long)gridDim.x * blockDim.x) {
+        int i = (int)(m % L.n[0]), j = (int)((m / L.n[0]) % L.n[1]), k = (int)(m / ((long)L.n[0] * L.n[1]));
+        double a1 = i > 0 ? A.cx[m - 1] : (B.per[0] ? A.cx[m + L.n[0] - 1] : 0.0);
+        double a3 = j > 0 ? A.cy[m - L.n[0]] : (B.per[1] ? A.cy[m + (long)L.n[0] * (L.n[1] - 1)] : 0.0);
+        long sz = (long)L.n[0] * L.n[1];
+        double a5 = k > 0 ? A.cz[m - sz] : (B.per[2] ? A.cz[m + sz * (L.n[2] - 1)] : 0.0);
+        double a2 = A.cx[m], a4 = A.cy[m], a6 = A.cz[m];
+        long n = lidx(L, i, j, k);
+        double d = a1 + a2 + a3 + a4 + a5 + a6;
+        double b = A.rhs[m];
+        double r = b - d * p[n] + a1 * pfield(p, L, B, i - 1, j, k) + a2 * pfield(p, L, B, i + 1, j, k) +
+                   a3 * pfield(p, L, B, i, j - 1, k) + a4 * pfield(p, L, B, i, j + 1, k) +
+                   a5 * pfield(p, L, B, i, j, k - 1) + a6 * pfield(p, L, B, i, j, k + 1);
+        if (rT) rT[m] = (T)r;
+        if (r64) r64[m] = r;
+        s2 += r * r;
+        s1 += fabs(r);
+        sb += b * b;
+    }
+    s2 = block_sum<256>(s2, sh);
+    s1 = block_sum<256>(s1, sh);
+    sb = block_sum<256>(sb, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = s2;
+        part[kRedBlocks + blockIdx.x] = s1;
+        part[2 * kRedBlocks + blockIdx.x] = sb;
+    }
+}
+
+// p += x (the level-0 correction) on the ghosted field
+template <typename T>
+__global__ void k_fast_correct(double* __restrict__ p, const T* __restrict__ x, const Layout L, double alpha) {
+    long m = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    long N = (long)L.n[0] * L.n[1] * L.n[2];
+    if (m >= N) return;
+    int i = (int)(m % L.n[0]), j = (int)((m / L.n[0]) % L.n[1]), k = (int)(m / ((long)L.n[0] * L.n[1]));
+    long n = lidx(L, i, j, k);
+    p[n] = p[n] + alpha * (double)x[m];
+}
+
+// ---- PCG helpers (FP64 compact vectors) --------------------------------------
+// q = A d ; slot 0 = d.q
+__global__ void k_pcg_matvec(const Mat64 A, const double* __restrict__ d, double* __restrict__ q, const Layout L,
+                             const Bnd B, double* part) {
+    __shared__ double sh[32];
+    double s = 0.0;
+    long N = (long)L.n[0] * L.n[1] * L.n[2];
+    for (long m = blockIdx.x * (long)blockDim.x + threadIdx.x; m < N; m += (long)gridDim.x * blockDim.x) {
+        int i = (int)(m % L.n[0]), j = (int)((m / L.n[0]) % L.n[1]), k = (int)(m / ((long)L.n[0] * L.n[1]));
+        double v = ax_compact(A, d, L, B, i, j, k, m);
+        q[m] = v;
+        s += d[m] * v;
+    }
+    s = block_sum<256>(s, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// p += alpha d (ghosted p), r -= alpha q ; slots 0 = r.r, 1 = sum |r|
+__global__ void k_pcg_update(double* __restrict__ p, double* __restrict__ r, const double* __restrict__ d,
+                             const double* __restrict__ q, double alpha, const Layout L, double* part) {
+    __shared__ double sh[32];
+    double s2 = 0.0, s1 = 0.0;
+    long N = (long)L.n[0] * L.n[1] * L.n[2];
+    for (long m = blockIdx.x * (long)blockDim.x + threadIdx.x; m < N; m += (long)gridDim.x * blockDim.x) {
+        int i = (int)(m % L.n[0]), j = (int)((m / L.n[0]) % L.n[1]), k = (int)(m / ((long)L.n[0] * L.n[1]));
+        long n = lidx(L, i, j, k);
+        p[n] = p[n] + alpha * d[m];
+        double rr = r[m] - alpha * q[m];
+        r[m] = rr;
+        s2 += rr * rr;
+        s1 += fabs(rr);
+    }
+    s2 = block_sum<256>(s2, sh);
+    s1 = block_sum<256>(s1, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = s2;
+        part[kRedBlocks + blockIdx.x] = s1;
+    }
+}
+
+template <typename T>
+__global__ void k_to_T(const double* __restrict__ a, T* __restrict__ b, long N) {
+    long m = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (m < N) b[m] = (T)a[m];
+}
+
+// zold = z; z = x0 ; slots 0 = r.z, 1 = r.zold
+template <typename T>
+__global__ void k_pcg_takez(const T* __restrict__ x0, double* __restrict__ z, double* __restrict__ zold,
+                            const double* __restrict__ r, long N, double* part) {
+    __shared__ double sh[32];
+    double s0 = 0.0, s1 = 0.0;
+    for (long m = blockIdx.x * (long)blockDim.x + threadIdx.x; m < N; m += (long)gridDim.x * blockDim.x) {
+        double zo = z[m];
+        double zn = (double)x0[m];
+        zold[m] = zo;
+        z[m] = zn;
+        s0 += r[m] * zn;
+        s1 += r[m] * zo;
+    }
+    s0 = block_sum<256>(s0, sh);
+    s1 = block_sum<256>(s1, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = s0;
+        part[kRedBlocks + blockIdx.x] = s1;
+    }
+}
+
+__global__ void k_pcg_dir(double* __restrict__ d, const double* __restrict__ z, double beta, long N) {
+    long m = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (m < N) d[m] = z[m] + beta * d[m];
+}
+
+// ---- host side ---------------------------------------------------------------
+template <typename T>
+static std::vector<FastLevel<T>>& levels(paris_ctx* c);
+template <>
+std::vector<FastLevel<float>>& levels<float>(paris_ctx* c) { return c->fl32; }
+template <>
+std::vector<FastLevel<double>>& levels<double>(paris_ctx* c) { return c->fl64; }
+
+static int fast_depth(const paris_ctx* c) {
+    int n0[3] = {c->d.nx, c->d.ny, c->d.nz};
+    int nl = 1;
+    while (nl < kMaxLevels) {
+        bool even = true, big = true;
+        for (int a = 0; a < 3; a++) {
+            if ((n0[a] >> (nl - 1)) % 2) even = false;
+            if ((n0[a] >> nl) < 2) big = false;
+        }
+        if (!even || !big) break;
+        nl++;
+    }
+    return nl;
+}
+
+template <typename T>
+static int fast_alloc(paris_ctx* c) {
+    auto& lv = levels<T>(c);
+    if (!lv.empty()) return PARIS_OK;
+    int nl = fast_depth(c);
+    c->fast_nl = nl;
+    lv.resize(nl);
+    for (int L = 0; L < nl; L++) {
+        FastLevel<T>& l = lv[L];
+        l.n[0] = c->d.nx >> L; l.n[1] = c->d.ny >> L; l.n[2] = c->d.nz >> L;
+        l.N = (long)l.n[0] * l.n[1] * l.n[2];
+        for (T** p : {&l.cx, &l.cy, &l.cz, &l.b, &l.x}) PARIS_CUDA_TRY(c, cudaMalloc(p, l.N * sizeof(T)));
+    }
+    return PARIS_OK;
+}
+
+template <typename T>
+static LV<T> view(const FastLevel<T>& l) {
+    return LV<T>{l.cx, l.cy, l.cz, l.b, l.x, l.n[0], l.n[1], l.n[2], l.N};
+}
+
+template <typename T>
+static int fast_coefs(paris_ctx* c) {
+    auto& lv = levels<T>(c);
+    PARIS_LAUNCH(c, k_fast_coef0<T>, div_up(c->N, 256), 256, 0, c->cx, c->cy, c->cz, lv[0].cx, lv[0].cy, lv[0].cz,
+                 c->N);
+    for (int L = 1; L < (int)lv.size(); L++)
+        PARIS_LAUNCH(c, k_fast_coarsen<T>, div_up(lv[L].N, 256), 256, 0, view(lv[L - 1]), view(lv[L]), lv[L].cx,
+                     lv[L].cy, lv[L].cz);
+    return PARIS_OK;
+}
+
+// one V(nu1,nu2) cycle on level 0 from x0 = 0 with the right-hand side in b0
+template <typename T>
+static int vcycle(paris_ctx* c, int nu1, int nu2) {
+    auto& lv = levels<T>(c);
+    int nl = (int)lv.size();
+    int Lc = 0;
+    while (Lc < nl - 1 && lv[Lc].N > kCoarseCells) Lc++;
+    if (Lc > 0) PARIS_CUDA_TRY(c, cudaMemsetAsync(lv[0].x, 0, lv[0].N * sizeof(T), c->stream));
+    for (int L = 0; L < Lc; L++) {
+        LV<T> v = view(lv[L]);
+        long nh = (long)((v.n0 + 1) / 2) * v.n1 * v.n2;
+        for (int s = 0; s < nu1; s++) {
+            PARIS_LAUNCH(c, k_fast_smooth<T>, div_up(nh, 256), 256, 0, v, c->bnd, 0);
+            PARIS_LAUNCH(c, k_fast_smooth<T>, div_up(nh, 256), 256, 0, v, c->bnd, 1);
+        }
+        LV<T> cv = view(lv[L + 1]);
+        PARIS_LAUNCH(c, k_fast_restrict<T>, div_up(cv.N, 256), 256, 0, v, cv, c->bnd);
+        if (L + 1 < Lc) PARIS_CUDA_TRY(c, cudaMemsetAsync(lv[L + 1].x, 0, lv[L + 1].N * sizeof(T), c->stream));
+    }
+    LVSet<T> S;
+    for (int L = 0; L < nl; L++) S.l[L] = view(lv[L]);
+    PARIS_LAUNCH(c, k_fast_coarse_cycle<T>, 1, 1024, 0, S, Lc, nl, c->bnd, nu1, nu2);
+    for (int L = Lc - 1; L >= 0; L--) {
+        LV<T> v = view(lv[L]);
+        PARIS_LAUNCH(c, k_fast_prolong<T>, div_up(v.N, 256), 256, 0, v, view(lv[L + 1]));
+        long nh = (long)((v.n0 + 1) / 2) * v.n1 * v.n2;
+        for (int s = 0; s < nu2; s++) {
+            PARIS_LAUNCH(c, k_fast_smooth<T>, div_up(nh, 256), 256, 0, v, c->bnd, 1);
+            PARIS_LAUNCH(c, k_fast_smooth<T>, div_up(nh, 256), 256, 0, v, c->bnd, 0);
+        }
+    }
+    return PARIS_OK;
+}
+
+static bool converged(const paris_solve_opts* o, double s2, double s1, double bn2, long N, double* tres,
+                      double* rel) {
+    *rel = bn2 > 0.0 ? sqrt(s2 / bn2) : sqrt(s2);
+    *tres = o->norm == 1 ? s1 / (double)N : sqrt(s2 / (double)N);
+    if (o->rel_tol > 0.0) return *rel < o->rel_tol;
+    return *tres < o->max_error;
+}
+
+template <typename T>
+static int solve_dc(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* res) {
+    auto& lv = levels<T>(c);
+    Mat64 A{c->cx, c->cy, c->cz, c->rhs};
+    double* p = c->fld[PARIS_FIELD_P];
+    double s[3], tres, rel;
+    PARIS_LAUNCH(c, k_fast_residual64<T>, kRedBlocks, 256, 0, A, p, c->L, c->bnd, lv[0].b, (double*)nullptr,
+                 c->red_part);
+    PARIS_CHECK(ctx_reduce_finish(c, 3, s));
+    double bn2 = s[2];
+    bool done = converged(o, s[0], s[1], bn2, c->N, &tres, &rel);
+    res->res0 = tres;
+    int it = 0;
+    int nu1 = o->nu1 > 0 ? o->nu1 : 2, nu2 = o->nu2 > 0 ? o->nu2 : 2;
+    while (!done && it < o->maxit) {
+        PARIS_CHECK(vcycle<T>(c, nu1, nu2));
+        PARIS_LAUNCH(c, k_fast_correct<T>, div_up(c->N, 256), 256, 0, p, lv[0].x, c->L, 1.0);
+        PARIS_LAUNCH(c, k_fast_residual64<T>, kRedBlocks, 256, 0, A, p, c->L, c->bnd, lv[0].b, (double*)nullptr,
+                     c->red_part);
+        PARIS_CHECK(ctx_reduce_finish(c, 3, s));
+        it++;
+        done = converged(o, s[0], s[1], bn2, c->N, &tres, &rel);
+        if (tres != tres) {
+            ctx_set_error(c, "pressure residual is NaN after %d cycles", it);
+            res->it = it; res->res = tres; res->rel_res = rel;
+            return PARIS_NAN_DETECTED;
+        }
+    }
+    res->it = done ? it : o->maxit + 1;
+    res->res = tres;
+    res->rel_res = rel;
+    return done ? PARIS_OK : PARIS_NOT_CONVERGED;
+}
+
+static int alloc_vec(paris_ctx* c, double** p) {
+    if (!*p) PARIS_CUDA_TRY(c, cudaMalloc(p, c->N * sizeof(double)));
+    return PARIS_OK;
+}
+
+template <typename T>
+static int precondition(paris_ctx* c, int nu1, int nu2, double* rz, double* rzold) {
+    auto& lv = levels<T>(c);
+    PARIS_LAUNCH(c, k_to_T<T>, div_up(c->N, 256), 256, 0, c->fast_r64, lv[0].b, c->N);
+    PARIS_CHECK(vcycle<T>(c, nu1, nu2));
+    PARIS_LAUNCH(c, k_pcg_takez<T>, kRedBlocks, 256, 0, lv[0].x, c->fast_z64, c->fast_zold64, c->fast_r64, c->N,
+                 c->red_part);
+    double s[2];
+    PARIS_CHECK(ctx_reduce_finish(c, 2, s));
+    *rz = s[0];
+    *rzold = s[1];
+    return PARIS_OK;
+}
+
+template <typename T>
+static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* res) {
+    for (double** v : {&c->fast_r64, &c->fast_d64, &c->fast_q64, &c->fast_z64, &c->fast_zold64})
+        PARIS_CHECK(alloc_vec(c, v));
+    Mat64 A{c->cx, c->cy, c->cz, c->rhs};
+    double* p = c->fld[PARIS_FIELD_P];
+    double s[3], tres, rel;
+    PARIS_LAUNCH(c, k_fast_residual64<T>, kRedBlocks, 256, 0, A, p, c->L, c->bnd, (T*)nullptr, c->fast_r64,
+                 c->red_part);
+    PARIS_CHECK(ctx_reduce_finish(c, 3, s));
+    double bn2 = s[2];
+    bool done = converged(o, s[0], s[1], bn2, c->N, &tres, &rel);
+    res->res0 = tres;
+    int it = 0;
+    int nu1 = o->nu1 > 0 ? o->nu1 : 2, nu2 = o->nu2 > 0 ? o->nu2 : 2;
+    double rz = 0.0, rzo = 0.0;
+    if (!done) {
+        PARIS_CUDA_TRY(c, cudaMemsetAsync(c->fast_z64, 0, c->N * sizeof(double), c->stream));
+        PARIS_CHECK(precondition<T>(c, nu1, nu2, &rz, &rzo));
+        PARIS_CUDA_TRY(c, cudaMemcpyAsync(c->fast_d64, c->fast_z64, c->N * sizeof(double), cudaMemcpyDeviceToDevice,
+                                          c->stream));
+    }
+    while (!done && it < o->maxit) {
+        double dq;
+        PARIS_LAUNCH(c, k_pcg_matvec, kRedBlocks, 256, 0, A, c->fast_d64, c->fast_q64, c->L, c->bnd, c->red_part);
+        PARIS_CHECK(ctx_reduce_finish(c, 1, &dq));
+        if (!(dq > 0.0)) break;
+        double alpha = rz / dq;
+        PARIS_LAUNCH(c, k_pcg_update, kRedBlocks, 256, 0, p, c->fast_r64, c->fast_d64, c->fast_q64, alpha, c->L,
+                     c->red_part);
+        PARIS_CHECK(ctx_reduce_finish(c, 2, s));
+        it++;
+        done = converged(o, s[0], s[1], bn2, c->N, &tres, &rel);
+        if (tres != tres) {
+            ctx_set_error(c, "pressure residual is NaN after %d iterations", it);
+            res->it = it; res->res = tres; res->rel_res = rel;
+            return PARIS_NAN_DETECTED;
+        }
+        if (done) break;
+        double rz_new, r_zold;
+        PARIS_CHECK(precondition<T>(c, nu1, nu2, &rz_new, &r_zold));
+        double beta = (rz_new - r_zold) / rz;   // flexible (Polak-Ribiere) form
+        rz = rz_new;
+        PARIS_LAUNCH(c, k_pcg_dir, div_up(c->N, 256), 256, 0, c->fast_d64, c->fast_z64, beta, c->N);
+    }
+    (void)rzo;
+    res->it = done ? it : o->maxit + 1;
+    res->res = tres;
+    res->rel_res = rel;
+    return done ? PARIS_OK : PARIS_NOT_CONVERGED;
+}
+
+int mg_fast_solve(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* res) {
+    if (!c->have_matrix) return PARIS_BAD_ARGS;
+    int st;
+    if (o->mode == PARIS_MG_MIXED) {
+        PARIS_CHECK(fast_alloc<float>(c));
+        PARIS_CHECK(fast_coefs<float>(c));
+        st = o->pcg ? solve_pcg<float>(c, o, res) : solve_dc<float>(c, o, res);
+    } else {
+        PARIS_CHECK(fast_alloc<double>(c));
+        PARIS_CHECK(fast_coefs<double>(c));
+        st = o->pcg ? solve_pcg<double>(c, o, res) : solve_dc<double>(c, o, res);
+    }
+    if (st == PARIS_OK || st == PARIS_NOT_CONVERGED) PARIS_CHECK(ctx_ghost_fill(c, c->fld[PARIS_FIELD_P]));
+    return st;
+}

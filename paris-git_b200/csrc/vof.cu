@@ -1,0 +1,525 @@
+// vof.cu -- split PLIC VOF advection on the B200: vofsweeps
+// (vofmodules.f90:1340-1361) with swp (vofnonmodule.f90:27-48), the CIAM sweep
+// swpz (:126-237) and the Weymouth-Yue sweep swpr (:664-754), the flags and
+// clipping of get_flags_and_clip (vofmodules.f90:549-571), SetVOFBC
+// (:1694-1825), linfunc (:171-218) and the sphere initialisation
+// ls2vof_refined (:1195-1293).  Built with -fmad=false.
+//
+// One kernel per split direction: a block owns a tile of cells, computes the
+// fluxes vof1/vof2/vof3 of the tile plus one cell on each side along the
+// sweep direction into shared memory (full and empty cells in closed form,
+// mixed cells through a per-block work queue so that the PLIC geometry runs
+// without warp divergence), then writes the new, clipped volume fraction and
+// the flag of the tile into the second buffer.  A ghost kernel then applies
+// SetVOFBC and the periodic wrap.
+#include "ctx.cuh"
+#include "plic.cuh"
+
+static constexpr int kSweepThreads = 256;
+static constexpr int kMaxFlux = 320;    // (32+2)*8 or 32*(8+2)
+
+struct SweepArgs {
+    const double* c;     // old cvof (ghosted)
+    double* cn;          // new cvof (ghosted)
+    int8_t* flag;        // new flags
+    const double* us;    // face velocity of the sweep direction
+    const uint8_t* cg;   // c_mask (WY)
+    Layout L;
+    int d;               // 0,1,2
+    int wy;              // 1: swpr
+    double dt, dxyz;     // a = us*dt/dxyz with dxyz = dxh(is) (vofnonmodule.f90:140,682)
+    double epsc;
+};
+
+// tile shape (cells) of a sweep along d
+__host__ __device__ inline void tile_shape(int d, int& tx, int& ty, int& tz) {
+    tx = 32;
+    ty = d == 2 ? 1 : 8;
+    tz = d == 2 ? 8 : 1;
+}
+
+__global__ void __launch_bounds__(kSweepThreads) k_vof_sweep(const SweepArgs a) {
+    __shared__ double v1[kMaxFlux], v2[kMaxFlux], v3[kMaxFlux];
+    __shared__ int queue[kMaxFlux];
+    __shared__ int nq;
+    const Layout& L = a.L;
+    int tx, ty, tz;
+    tile_shape(a.d, tx, ty, tz);
+    const int i0 = blockIdx.x * tx, j0 = blockIdx.y * ty, k0 = blockIdx.z * tz;
+    // extended tile along d
+    int ex = tx + (a.d == 0 ? 2 : 0), ey = ty + (a.d == 1 ? 2 : 0), ez = tz + (a.d == 2 ? 2 : 0);
+    int ox = a.d == 0 ? -1 : 0, oy = a.d == 1 ? -1 : 0, oz = a.d == 2 ? -1 : 0;
+    const int nflux = ex * ey * ez;
+    const long od = a.d == 0 ? 1 : (a.d == 1 ? L.pitch : L.plane);
+    if (threadIdx.x == 0) nq = 0;
+    __syncthreads();
+    // phase 1: closed-form fluxes, queue the mixed cells
+    for (int e = threadIdx.x; e < nflux; e += blockDim.x) {
+        int li = e % ex, lj = (e / ex) % ey, lk = e / (ex * ey);
+        int i = i0 + ox + li, j = j0 + oy + lj, k = k0 + oz + lk;
+        double f1 = 0.0, f2 = 0.0, f3 = 0.0;
+        bool in = i >= -1 && i <= L.n[0] && j >= -1 && j <= L.n[1] && k >= -1 && k <= L.n[2];
+        if (in) {
+            long n = lidx(L, i, j, k);
+            double cc = a.c[n];
+            double a2 = a.us[n] * a.dt / a.dxyz;
+            double a1 = a.us[n - od] * a.dt / a.dxyz;
+            if (cc == 1.0) {
+                f1 = plic::dmax1(-a1, 0.0);
+                f2 = a.wy ? 0.0 : 1.0 - plic::dmax1(a1, 0.0) + plic::dmin1(a2, 0.0);
+                f3 = plic::dmax1(a2, 0.0);
+            } else if (cc > 0.0) {
+                int q = atomicAdd(&nq, 1);
+                queue[q] = e;
+            }
+        }
+        v1[e] = f1; v2[e] = f2; v3[e] = f3;
+    }
+    __syncthreads();
+    // phase 1b: PLIC fluxes of the mixed cells
+    for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+        int e = queue[q];
+        int li = e % ex, lj = (e / ex) % ey, lk = e / (ex * ey);
+        int i = i0 + ox + li, j = j0 + oy + lj, k = k0 + oz + lk;
+        long n = lidx(L, i, j, k);
+        double cc = a.c[n];
+        double a2 = a.us[n] * a.dt / a.dxyz;
+        double a1 = a.us[n - od] * a.dt / a.dxyz;
+        double st[27];
+#pragma unroll
+        for (int i1 = -1; i1 <= 1; i1++)
+#pragma unroll
+            for (int j1 = -1; j1 <= 1; j1++)
+#pragma unroll
+                for (int k1 = -1; k1 <= 1; k1++)
+                    st[(i1 + 1) + 3 * (j1 + 1) + 9 * (k1 + 1)] = a.c[n + i1 + j1 * L.pitch + k1 * L.plane];
+        double m[3], x0[3] = {0.0, 0.0, 0.0}, dx[3] = {1.0, 1.0, 1.0};
+        plic::mycs(st, m);
+        double f1 = 0.0, f2 = 0.0, f3 = 0.0;
+        if (!a.wy) {
+            // fit_plane_new (vofnonmodule.f90:633-655) and the three fluxes of swpz
+            if (!(m[0] == 0.0 && m[1] == 0.0 && m[2] == 0.0)) {
+                double alpha = plic::al3d(m, cc);
+                m[a.d] = m[a.d] / (1.0 - a1 + a2);
+                alpha = alpha + m[a.d] * a1;
+                double mm1 = plic::dmax1(a1, 0.0);
+                double mm2 = 1.0 - mm1 + plic::dmin1(0.0, a2);
+                if (a1 < 0.0) {
+                    x0[a.d] = a1; dx[a.d] = -a1;
+                    f1 = plic::fl3d(m, alpha, x0, dx);
+                }
+                if (a2 > 0.0) {
+                    x0[a.d] = 1.0; dx[a.d] = a2;
+                    f3 = plic::fl3d(m, alpha, x0, dx);
+                }
+                x0[a.d] = mm1; dx[a.d] = mm2;
+                f2 = plic::fl3d(m, alpha, x0, dx);
+            }
+        } else {
+            double alpha = plic::al3d(m, cc);
+            if (a1 < 0.0) {
+                dx[a.d] = -a1;
+                f1 = plic::fl3d(m, alpha, x0, dx);
+            }
+            if (a2 > 0.0) {
+                x0[a.d] = 1.0 - a2; dx[a.d] = a2;
+                f3 = plic::fl3d(m, alpha, x0, dx);
+            }
+        }
+        v1[e] = f1; v2[e] = f2; v3[e] = f3;
+    }
+    __syncthreads();
+    // phase 2: the update of the tile's cells, clipping and flags
+    const int eo = a.d == 0 ? 1 : (a.d == 1 ? ex : ex * ey);   // flux-tile stride along d
+    for (int e = threadIdx.x; e < tx * ty * tz; e += blockDim.x) {
+        int li = e % tx, lj = (e / tx) % ty, lk = e / (tx * ty);
+        int i = i0 + li, j = j0 + lj, k = k0 + lk;
+        if (i >= L.n[0] || j >= L.n[1] || k >= L.n[2]) continue;
+        int f = (li - ox) + ex * ((lj - oy) + ey * (lk - oz));
+        long n = lidx(L, i, j, k);
+        double cnew;
+        if (!a.wy) {
+            cnew = v3[f - eo] + v2[f] + v1[f + eo];
+            cnew = plic::dmax1(0.0, plic::dmin1(1.0, cnew));
+        } else {
+            double a2 = a.us[n] * a.dt / a.dxyz;
+            double a1 = a.us[n - od] * a.dt / a.dxyz;
+            cnew = a.c[n] - (v3[f] - v1[f + eo]) + (v3[f - eo] - v1[f]) + (double)a.cg[n] * (a2 - a1);
+            if (cnew < a.epsc) cnew = 0.0;
+            else if (cnew > 1.0 - a.epsc) cnew = 1.0;
+        }
+        int8_t fl;
+        if (cnew <= a.epsc) { fl = 0; cnew = 0.0; }
+        else if (cnew >= 1.0 - a.epsc) { fl = 1; cnew = 1.0; }
+        else fl = 2;
+        a.cn[n] = cnew;
+        a.flag[n] = fl;
+    }
+}
+
+// ghost cells of the new cvof and flags: SetVOFBC on walls (orientations
+// x- y- z- x+ y+ z+ in that order, the last one writing a cell wins; 'outflow'
+// copies the boundary cell as it stood after the earlier orientations), then
+// the periodic wrap of do_all_ghost, then get_flags_and_clip.
+__device__ bool ghost_cell_v(const Layout L, long t, int& i, int& j, int& k);
+
+__global__ void k_vof_ghosts(double* __restrict__ c, int8_t* __restrict__ flag, const Layout L, const Bnd B,
+                             long G, double epsc) {
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= G) return;
+    int i, j, k;
+    if (!ghost_cell_v(L, t, i, j, k)) return;
+    int s[3] = {i, j, k};
+    for (int d = 0; d < 3; d++)
+        if (B.per[d]) {
+            if (s[d] < 0) s[d] += L.n[d];
+            else if (s[d] >= L.n[d]) s[d] -= L.n[d];
+        }
+    double val = 0.0;
+    bool fixed = false;
+    for (int o = 5; o >= 0 && !fixed; o--) {
+        int d = o % 3;
+        bool lo = o < 3;
+        if (B.per[d]) continue;
+        bool out = lo ? s[d] < 0 : s[d] >= L.n[d];
+        if (!out) continue;
+        int cond = B.vofbc[o];
+        if (cond == PARIS_VOFBC_DRY) { val = 0.0; fixed = true; }
+        else if (cond == PARIS_VOFBC_WET) { val = 1.0; fixed = true; }
+        else s[d] = lo ? 0 : L.n[d] - 1;   // outflow
+    }
+    if (!fixed) val = c[lidx(L, s[0], s[1], s[2])];
+    int8_t fl;
+    if (val <= epsc) { fl = 0; val = 0.0; }
+    else if (val >= 1.0 - epsc) { fl = 1; val = 1.0; }
+    else fl = 2;
+    long n = lidx(L, i, j, k);
+    c[n] = val;
+    flag[n] = fl;
+}
+
+// same enumeration of ghost cells as the generic ghost fill
+__device__ bool ghost_cell_v(const Layout L, long t, int& i, int& j, int& k) {
+    const int g = L.ng;
+    const int ty = L.n[1] + 2 * g, tz = L.n[2] + 2 * g;
+    long rx = 2L * g * ty * tz, ry = (long)L.n[0] * 2 * g * tz, rz = (long)L.n[0] * L.n[1] * 2 * g;
+    if (t < rx) {
+        int a = (int)(t % (2 * g)); long r = t / (2 * g);
+        j = (int)(r % ty) - g; k = (int)(r / ty) - g;
+        i = a < g ? a - g : L.n[0] + (a - g);
+        return true;
+    }
+    t -= rx;
+    if (t < ry) {
+        i = (int)(t % L.n[0]); long r = t / L.n[0];
+        int a = (int)(r % (2 * g)); k = (int)(r / (2 * g)) - g;
+        j = a < g ? a - g : L.n[1] + (a - g);
+        return true;
+    }
+    t -= ry;
+    if (t < rz) {
+        i = (int)(t % L.n[0]); long r = t / L.n[0];
+        j = (int)(r % L.n[1]); int a = (int)(r / L.n[1]);
+        k = a < g ? a - g : L.n[2] + (a - g);
+        return true;
+    }
+    return false;
+}
+
+static long ghost_total(const Layout& L) {
+    const int g = L.ng;
+    long ty = L.n[1] + 2 * g, tz = L.n[2] + 2 * g;
+    return 2L * g * ty * tz + (long)L.n[0] * 2 * g * tz + (long)L.n[0] * L.n[1] * 2 * g;
+}
+
+// c_mask(cvof, cbinary), vofmodules.f90:1295-1305 (whole ghosted array)
+__global__ void k_c_mask(const double* __restrict__ c, uint8_t* __restrict__ cg, long total) {
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t < total) cg[t] = c[t] > 0.5 ? 1 : 0;
+}
+
+static int sweep(paris_ctx* c, int d, double dt) {
+    SweepArgs a;
+    a.c = c->fld[PARIS_FIELD_CVOF];
+    a.cn = c->c2;
+    a.flag = c->flag;
+    a.us = c->fld[PARIS_FIELD_U + d];
+    a.cg = c->cg;
+    a.L = c->L;
+    a.d = d;
+    a.wy = c->d.vof_advect == PARIS_ADVECT_WY;
+    a.dt = dt;
+    a.dxyz = c->h_dxh[c->d.ng];
+    a.epsc = c->d.epsc;
+    int tx, ty, tz;
+    tile_shape(d, tx, ty, tz);
+    dim3 grid(div_up(c->L.n[0], tx), div_up(c->L.n[1], ty), div_up(c->L.n[2], tz));
+    PARIS_LAUNCH(c, k_vof_sweep, grid, kSweepThreads, 0, a);
+    long G = ghost_total(c->L);
+    PARIS_LAUNCH(c, k_vof_ghosts, div_up(G, 256), 256, 0, c->c2, c->flag, c->L, c->bnd, G, c->d.epsc);
+    double* t = c->fld[PARIS_FIELD_CVOF];
+    c->fld[PARIS_FIELD_CVOF] = c->c2;
+    c->c2 = t;
+    return PARIS_OK;
+}
+
+// test_cell_size (vofmodules.f90:1827-1834): VOF needs cubic cells
+static bool cubic_cells(const paris_ctx* c) {
+    int g = c->d.ng;
+    double hx = c->h_dxh[g], hy = c->h_dyh[g], hz = c->h_dzh[g];
+    return !(fabs(hy - hx) * 1e12 / hx > 1.0 || fabs(hz - hx) * 1e12 / hx > 1.0);
+}
+
+extern "C" int paris_vof_sweeps(paris_handle_t c, int32_t tswap, double dt) {
+    if (!c) return PARIS_BAD_ARGS;
+    if (!cubic_cells(c)) {
+        ctx_set_error(c, "non-cubic cells");
+        return PARIS_BAD_ARGS;
+    }
+    cudaSetDevice(c->dev);
+    if (c->d.vof_advect == PARIS_ADVECT_WY) {
+        if (!c->cg) PARIS_CUDA_TRY(c, cudaMalloc(&c->cg, c->L.total));
+        PARIS_LAUNCH(c, k_c_mask, div_up(c->L.total, 256), 256, 0, c->fld[PARIS_FIELD_CVOF], c->cg, c->L.total);
+    }
+    int order[3];
+    int m = ((tswap % 3) + 3) % 3;
+    if (m == 0) { order[0] = 2; order[1] = 0; order[2] = 1; }        // z, x, y
+    else if (m == 1) { order[0] = 1; order[1] = 2; order[2] = 0; }   // y, z, x
+    else { order[0] = 0; order[1] = 1; order[2] = 2; }               // x, y, z
+    for (int s = 0; s < 3; s++) PARIS_CHECK(sweep(c, order[s], dt));
+    return PARIS_OK;
+}
+
+// linfunc(field,a1,a2,MeanFlag), vofmodules.f90:171-218, over every cell of
+// the ghosted array (the 27-point filter where all neighbours exist), then
+// do_all_ghost.  b1..b4 of initialize_linfunc (vofmodules.f90:133-147).
+__global__ void k_linfunc(const double* __restrict__ c, double* __restrict__ f, const Layout L, double a1,
+                          double a2, int harm, int filt) {
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const int g = L.ng, tx = L.n[0] + 2 * g, ty = L.n[1] + 2 * g, tz = L.n[2] + 2 * g;
+    if (t >= (long)tx * ty * tz) return;
+    int ii = (int)(t % tx), jj = (int)((t / tx) % ty), kk = (int)(t / ((long)tx * ty));
+    int i = ii - g, j = jj - g, k = kk - g;
+    long n = lidx(L, i, j, k);
+    double cf;
+    if (filt && ii > 0 && ii < tx - 1 && jj > 0 && jj < ty - 1 && kk > 0 && kk < tz - 1) {
+        const double b1 = 8.0 / 64, b2 = 4.0 / 64, b3 = 2.0 / 64, b4 = 1.0 / 64;
+        long sy = L.pitch, sz = L.plane;
+        cf = b1 * c[n] + b2 * (c[n - 1] + c[n - sy] + c[n - sz] + c[n + 1] + c[n + sy] + c[n + sz]) +
+             b3 * (c[n + 1 + sy] + c[n + 1 - sy] + c[n - 1 + sy] + c[n - 1 - sy] + c[n + 1 + sz] + c[n + 1 - sz] +
+                   c[n - 1 + sz] + c[n - 1 - sz] + c[n + sy + sz] + c[n + sy - sz] + c[n - sy + sz] + c[n - sy - sz]) +
+             b4 * (c[n + 1 + sy + sz] + c[n + 1 + sy - sz] + c[n + 1 - sy + sz] + c[n + 1 - sy - sz] +
+                   c[n - 1 + sy + sz] + c[n - 1 + sy - sz] + c[n - 1 - sy + sz] + c[n - 1 - sy - sz]);
+    } else {
+        cf = c[n];
+    }
+    if (!harm) {
+        f[n] = cf * (a2 - a1) + a1;
+    } else {
+        double inva1 = 1.0 / (a1 + 1.e-50), inva2 = 1.0 / (a2 + 1.e-50);
+        f[n] = 1.0 / (cf * (inva2 - inva1) + inva1);
+    }
+}
+
+extern "C" int paris_linfunc(paris_handle_t c, int32_t which) {
+    if (!c || (which != PARIS_FIELD_RHO && which != PARIS_FIELD_MU)) return PARIS_BAD_ARGS;
+    cudaSetDevice(c->dev);
+    PARIS_CHECK(ctx_alloc_field(c, which));
+    double a1 = which == PARIS_FIELD_RHO ? c->d.rho1 : c->d.mu1;
+    double a2 = which == PARIS_FIELD_RHO ? c->d.rho2 : c->d.mu2;
+    int mean = which == PARIS_FIELD_RHO ? c->d.dens_mean : c->d.visc_mean;
+    int harm = mean == PARIS_MEAN_HARM;
+    long tot = (long)(c->d.nx + 4) * (c->d.ny + 4) * (c->d.nz + 4);
+    PARIS_LAUNCH(c, k_linfunc, div_up(tot, 256), 256, 0, c->fld[PARIS_FIELD_CVOF], c->fld[which], c->L, a1, a2,
+                 harm, c->d.nfilter > 0 ? 1 : 0);
+    PARIS_CHECK(ctx_ghost_fill(c, c->fld[which]));
+    return PARIS_OK;
+}
+
+// ---- initial condition: spheres by ls2vof_refined -----------------------------
+struct Spheres {
+    const double *xc, *yc, *zc, *rad;
+    int nb;
+};
+
+static constexpr int kMaxCand = 16;
+
+// shapes2ls (vofmodules.f90:973-993) restricted to the bubbles that can be the
+// max in the cell's stencil region (all bubbles when there are too many).
+__device__ inline double shapes2ls(const Spheres& S, const int* cand, int nc, double xx, double yy, double zz) {
+    double r = -2.0e6;
+    for (int q = 0; q < nc; q++) {
+        int ib = cand ? cand[q] : q;
+        double dx = xx - S.xc[ib], dy = yy - S.yc[ib], dz = zz - S.zc[ib];
+        double v = S.rad[ib] * S.rad[ib] - (1.0 * (dx * dx) + 1.0 * (dy * dy) + 1.0 * (dz * dz));
+        r = r > v ? r : v;
+    }
+    return r;
+}
+
+// ls2vof_in_cell, vofnonmodule.f90:1142-1190
+__device__ inline double ls2vof_in_cell(const double st[27], int& nflag) {
+    double m[3], zero[3] = {0.0, 0.0, 0.0}, one[3] = {1.0, 1.0, 1.0};
+    plic::fd32(st, m);
+    m[0] = fabs(m[0]); m[1] = fabs(m[1]); m[2] = fabs(m[2]);
+    double norml1 = m[0] + m[1] + m[2];
+    m[0] = m[0] / norml1; m[1] = m[1] / norml1; m[2] = m[2] / norml1;
+    double alpha = 32.0 * st[13] / norml1;
+    alpha = alpha + 0.5;
+    if (alpha >= 1.0) { nflag = 1; return 1.0; }
+    if (alpha <= 0.0) { nflag = 0; return 0.0; }
+    nflag = 2;
+    return plic::fl3d(m, alpha, zero, one);
+}
+
+// One pass of ls2vof_refined over the interior.  pass 2 (n1 > 1) refines the
+// cells whose 3x3x3 flag neighbourhood (flags of pass 1) is not isolated
+// (notisolated, vofmodules.f90:1126-1150) and writes into cout/fout.
+__global__ void k_ls2vof(const Spheres S, const Layout L, const double* __restrict__ xc, const double* __restrict__ yc,
+                         const double* __restrict__ zc, const double* __restrict__ dxa, const double* __restrict__ dya,
+                         const double* __restrict__ dza, int n1, const int8_t* __restrict__ fin,
+                         const double* __restrict__ cin, double* __restrict__ cout, int8_t* __restrict__ fout) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= L.n[0]) return;
+    const int g = L.ng;
+    long n = lidx(L, i, j, k);
+    if (n1 > 1) {
+        int nfrac = 0, nfull = 0, ncells = 0;
+        for (int i0 = -1; i0 <= 1; i0++)
+            for (int j0 = -1; j0 <= 1; j0++)
+                for (int k0 = -1; k0 <= 1; k0++) {
+                    int f = fin[n + i0 + j0 * L.pitch + k0 * L.plane];
+                    nfrac += f / 2; nfull += f % 2; ncells++;
+                }
+        bool refine = !(nfrac == 0 && (nfull == 0 || nfull == ncells));
+        if (!refine) {
+            cout[n] = cin[n];
+            fout[n] = fin[n];
+            return;
+        }
+    }
+    double x = xc[i + g], y = yc[j + g], z = zc[k + g];
+    double dxc = dxa[i + g], dyc = dya[j + g], dzc = dza[k + g];
+    double dx1 = dxc / n1, dy1 = dyc / n1, dz1 = dzc / n1;
+    // candidate bubbles: upper bound of rad^2 - d^2 over the region reaches the
+    // best lower bound (region radius generous; any superset gives the same max)
+    int cand[kMaxCand];
+    int nc = 0;
+    bool all = false;
+    {
+        double hx = 0.5 * dxc + dx1, hy = 0.5 * dyc + dy1, hz = 0.5 * dzc + dz1;
+        double R = 1.01 * sqrt(hx * hx + hy * hy + hz * hz);
+        double lbmax = -1e300;
+        for (int ib = 0; ib < S.nb; ib++) {
+            double ddx = x - S.xc[ib], ddy = y - S.yc[ib], ddz = z - S.zc[ib];
+            double D = sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+            double lb = S.rad[ib] * S.rad[ib] - (D + R) * (D + R);
+            lbmax = lb > lbmax ? lb : lbmax;
+        }
+        for (int ib = 0; ib < S.nb; ib++) {
+            double ddx = x - S.xc[ib], ddy = y - S.yc[ib], ddz = z - S.zc[ib];
+            double D = sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+            double dn = D - R > 0.0 ? D - R : 0.0;
+            double ub = S.rad[ib] * S.rad[ib] - dn * dn;
+            if (ub >= lbmax - 1e-9 * (fabs(lbmax) + 1.0)) {
+                if (nc < kMaxCand) cand[nc++] = ib;
+                else all = true;
+            }
+        }
+    }
+    const int* cp = all ? nullptr : cand;
+    int ncu = all ? S.nb : nc;
+    int nfrac = 0, nfull = 0;
+    double b = 0.0;
+    for (int l = 0; l < n1; l++)
+        for (int m = 0; m < n1; m++)
+            for (int q = 0; q < n1; q++) {
+                double x0 = x - 0.5 * dxc + 0.5 * dx1 + dx1 * l;
+                double y0 = y - 0.5 * dyc + 0.5 * dy1 + dy1 * m;
+                double z0 = z - 0.5 * dzc + 0.5 * dz1 + dz1 * q;
+                double st[27];
+                for (int i0 = -1; i0 <= 1; i0++)
+                    for (int j0 = -1; j0 <= 1; j0++)
+                        for (int k0 = -1; k0 <= 1; k0++)
+                            st[(i0 + 1) + 3 * (j0 + 1) + 9 * (k0 + 1)] =
+                                shapes2ls(S, cp, ncu, x0 + i0 * dx1, y0 + j0 * dy1, z0 + k0 * dz1);
+                int nflag;
+                double a = ls2vof_in_cell(st, nflag);
+                if (nflag == 2) nfrac++;
+                else if (nflag == 1) nfull++;
+                b = b + a;
+            }
+    double cv = b / (double)(n1 * n1 * n1);
+    int8_t fl;
+    if (nfrac > 0) fl = 2;
+    else if (nfull == n1 * n1 * n1) { fl = 1; cv = 1.0; }
+    else if (nfull == 0) { fl = 0; cv = 0.0; }
+    else fl = 2;
+    cout[n] = cv;
+    fout[n] = fl;
+}
+
+// walls of the initial field: SetVOFBC without the clipping of the sweeps
+__global__ void k_init_ghosts(double* __restrict__ c, int8_t* __restrict__ flag, const Layout L, const Bnd B, long G) {
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= G) return;
+    int i, j, k;
+    if (!ghost_cell_v(L, t, i, j, k)) return;
+    int s[3] = {i, j, k};
+    for (int d = 0; d < 3; d++)
+        if (B.per[d]) {
+            if (s[d] < 0) s[d] += L.n[d];
+            else if (s[d] >= L.n[d]) s[d] -= L.n[d];
+        }
+    double val = 0.0;
+    int8_t fl = 0;
+    bool fixed = false;
+    for (int o = 5; o >= 0 && !fixed; o--) {
+        int d = o % 3;
+        bool lo = o < 3;
+        if (B.per[d]) continue;
+        bool out = lo ? s[d] < 0 : s[d] >= L.n[d];
+        if (!out) continue;
+        int cond = B.vofbc[o];
+        if (cond == PARIS_VOFBC_DRY) { val = 0.0; fl = 0; fixed = true; }
+        else if (cond == PARIS_VOFBC_WET) { val = 1.0; fl = 1; fixed = true; }
+        else s[d] = lo ? 0 : L.n[d] - 1;
+    }
+    if (!fixed) {
+        long src = lidx(L, s[0], s[1], s[2]);
+        val = c[src];
+        fl = flag[src];
+    }
+    long n = lidx(L, i, j, k);
+    c[n] = val;
+    flag[n] = fl;
+}
+
+extern "C" int paris_init_spheres(paris_handle_t c, int32_t nb, const double* xc, const double* yc, const double* zc,
+                                  const double* rad, int32_t refinement) {
+    if (!c || nb <= 0 || !xc || !yc || !zc || !rad || refinement < 1) return PARIS_BAD_ARGS;
+    cudaSetDevice(c->dev);
+    double* dbuf = nullptr;
+    PARIS_CUDA_TRY(c, cudaMalloc(&dbuf, 4L * nb * sizeof(double)));
+    const double* src[4] = {xc, yc, zc, rad};
+    for (int q = 0; q < 4; q++)
+        PARIS_CUDA_TRY(c, cudaMemcpyAsync(dbuf + q * nb, src[q], nb * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    Spheres S{dbuf, dbuf + nb, dbuf + 2 * nb, dbuf + 3 * nb, nb};
+    int8_t* f2 = nullptr;
+    PARIS_CUDA_TRY(c, cudaMalloc(&f2, c->L.total));
+    PARIS_CUDA_TRY(c, cudaMemsetAsync(f2, 0, c->L.total, c->stream));
+    dim3 grid(div_up(c->L.n[0], 64), c->L.n[1], c->L.n[2]);
+    long G = ghost_total(c->L);
+    double* cv = c->fld[PARIS_FIELD_CVOF];
+    // pass 1 (n1 = 1) into c2/f2, ghosts, then pass 2 into cvof/flag
+    PARIS_LAUNCH(c, k_ls2vof, grid, 64, 0, S, c->L, c->xc, c->yc, c->zc, c->dx, c->dy, c->dz, 1, (const int8_t*)nullptr,
+                 (const double*)nullptr, c->c2, f2);
+    PARIS_LAUNCH(c, k_init_ghosts, div_up(G, 256), 256, 0, c->c2, f2, c->L, c->bnd, G);
+    PARIS_LAUNCH(c, k_ls2vof, grid, 64, 0, S, c->L, c->xc, c->yc, c->zc, c->dx, c->dy, c->dz, refinement, f2, c->c2,
+                 cv, c->flag);
+    PARIS_LAUNCH(c, k_init_ghosts, div_up(G, 256), 256, 0, cv, c->flag, c->L, c->bnd, G);
+    PARIS_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    cudaFree(dbuf);
+    cudaFree(f2);
+    return PARIS_OK;
+}

@@ -1,0 +1,178 @@
+"""Host-side mirror of the reference's grid-core subroutines over the C-ABI.
+
+Each method keeps the name and argument meaning of the PARIS subroutine it
+replaces (vofsweeps, linfunc, get_all_heights, get_all_curvatures,
+surfaceForce, SetupPoisson, NewSolver, project_velocity, calcResiduals,
+Setup_testMG, get_MGtest_err).  Arrays are numpy arrays in the reference
+layout: float64 (Nz+2Ng, Ny+2Ng, Nx+2Ng) with ghosts, i fastest; A is
+(8, Nz, Ny, Nx) = A(is:ie,js:je,ks:ke,8).  Errors raise ParisError; a solver
+that reaches maxit returns it = maxit+1 and warns, as NewSolverMG does
+(MGsolver.f90:402).
+"""
+import ctypes
+import warnings
+
+import numpy as np
+
+from . import capi
+
+
+class ParisError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{capi.STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class ParisGpu:
+    """Device-resident grid core for one grid (one CUDA device, no MPI split)."""
+
+    def __init__(self, desc, lib=None):
+        self.lib = lib or capi.load_library()
+        self.desc = desc
+        h = ctypes.c_void_p()
+        st = self.lib.paris_gpu_init(ctypes.byref(desc), ctypes.byref(h))
+        if st != capi.OK:
+            raise ParisError(st, "paris_gpu_init failed")
+        self.h = h
+        g = desc.ng
+        self.shape = (desc.nz + 2 * g, desc.ny + 2 * g, desc.nx + 2 * g)
+        self.n = (desc.nx, desc.ny, desc.nz)
+
+    # -- life cycle ---------------------------------------------------------
+    def close(self):
+        if self.h:
+            self.lib.paris_gpu_finalize(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, what):
+        if st != capi.OK:
+            err = self.lib.paris_gpu_last_error(self.h)
+            raise ParisError(st, f"{what}: {err.decode() if err else ''}")
+
+    # -- transfers ----------------------------------------------------------
+    def upload(self, field, arr):
+        if field in (capi.F_VOF_FLAG,):
+            a = np.ascontiguousarray(arr, dtype=np.int32)
+            assert a.shape == self.shape
+        elif field == capi.F_A:
+            a = np.ascontiguousarray(arr, dtype=np.float64)
+            assert a.shape == (8, self.desc.nz, self.desc.ny, self.desc.nx)
+        elif field == capi.F_HEIGHT:
+            a = np.ascontiguousarray(arr, dtype=np.float64)
+            assert a.shape == (6,) + self.shape
+        else:
+            a = np.ascontiguousarray(arr, dtype=np.float64)
+            assert a.shape == self.shape, (a.shape, self.shape)
+        self._check(self.lib.paris_gpu_upload(self.h, field, _ptr(a)), "upload")
+
+    def download(self, field):
+        if field in (capi.F_VOF_FLAG, capi.F_VOF_PHASE):
+            a = np.empty(self.shape, dtype=np.int32)
+        elif field == capi.F_A:
+            a = np.empty((8, self.desc.nz, self.desc.ny, self.desc.nx))
+        elif field == capi.F_HEIGHT:
+            a = np.empty((6,) + self.shape)
+        else:
+            a = np.empty(self.shape)
+        self._check(self.lib.paris_gpu_download(self.h, field, _ptr(a)), "download")
+        return a
+
+    def sync(self):
+        self._check(self.lib.paris_gpu_sync(self.h), "sync")
+
+    def stream(self):
+        return self.lib.paris_gpu_stream(self.h)
+
+    def field_ptr(self, field):
+        return self.lib.paris_gpu_field_ptr(self.h, field)
+
+    def launch_count(self):
+        return self.lib.paris_gpu_launch_count(self.h)
+
+    # -- VOF ----------------------------------------------------------------
+    def vof_sweeps(self, tswap, dt):
+        """vofsweeps(tswap), vofmodules.f90:1340."""
+        self._check(self.lib.paris_vof_sweeps(self.h, int(tswap), float(dt)), "vofsweeps")
+
+    vofsweeps = vof_sweeps
+
+    def linfunc(self, which=capi.F_RHO):
+        """linfunc(rho,rho1,rho2,DensMean) or (mu,...), vofmodules.f90:171."""
+        self._check(self.lib.paris_linfunc(self.h, which), "linfunc")
+
+    def init_spheres(self, centers, radii, refinement=8):
+        c = np.ascontiguousarray(np.asarray(centers, dtype=np.float64).reshape(-1, 3))
+        r = np.ascontiguousarray(np.asarray(radii, dtype=np.float64).reshape(-1))
+        xs = [np.ascontiguousarray(c[:, a]) for a in range(3)]
+        self._check(self.lib.paris_init_spheres(self.h, len(r), _ptr(xs[0]), _ptr(xs[1]), _ptr(xs[2]),
+                                                _ptr(r), int(refinement)), "init_spheres")
+
+    # -- surface tension ------------------------------------------------------
+    def get_all_heights(self):
+        self._check(self.lib.paris_get_all_heights(self.h), "get_all_heights")
+
+    def get_all_curvatures(self):
+        kappa = np.empty(self.shape)
+        self._check(self.lib.paris_get_all_curvatures(self.h, _ptr(kappa)), "get_all_curvatures")
+        return kappa
+
+    def surface_force(self):
+        self._check(self.lib.paris_surface_force(self.h), "surfaceForce")
+
+    surfaceForce = surface_force
+
+    # -- projection -------------------------------------------------------------
+    def setup_poisson(self, dt, volume_source=0.0):
+        """SetPressureBC + SetupPoisson(u,v,w,umask,vmask,wmask,rho,dt,A,tmp,VolumeSource)."""
+        self._check(self.lib.paris_setup_poisson(self.h, float(dt), float(volume_source)), "SetupPoisson")
+
+    SetupPoisson = setup_poisson
+
+    def setup_test_mg(self):
+        self._check(self.lib.paris_setup_test_mg(self.h), "Setup_testMG")
+
+    def new_solver(self, max_error, beta=1.0, maxit=100, norm=2, mode=capi.MG_MIXED, rel_tol=0.0,
+                   nu1=2, nu2=2, pcg=0):
+        """NewSolver(A,p,maxError,beta,maxit,it,ierr,norm); returns the SolveResult."""
+        o = capi.SolveOpts()
+        o.max_error, o.rel_tol, o.beta = float(max_error), float(rel_tol), float(beta)
+        o.maxit, o.norm, o.mode, o.nu1, o.nu2, o.pcg = int(maxit), int(norm), int(mode), nu1, nu2, int(pcg)
+        r = capi.SolveResult()
+        st = self.lib.paris_new_solver(self.h, ctypes.byref(o), ctypes.byref(r))
+        if st == capi.NOT_CONVERGED:
+            warnings.warn(f"Warning: LinearSolver reached maxit: ||res||: {r.res}")
+        else:
+            self._check(st, "NewSolver")
+        return r
+
+    NewSolver = new_solver
+
+    def calc_residuals(self):
+        out = np.zeros(3)
+        self._check(self.lib.paris_calc_residuals(self.h, _ptr(out)), "calcResiduals")
+        return out
+
+    def mg_test_err(self):
+        e = ctypes.c_double()
+        self._check(self.lib.paris_mg_test_err(self.h, ctypes.byref(e)), "get_MGtest_err")
+        return e.value
+
+    def project_velocity(self, dt):
+        """project_velocity(), paris.f90:882."""
+        self._check(self.lib.paris_project_velocity(self.h, float(dt)), "project_velocity")

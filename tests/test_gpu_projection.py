@@ -1,0 +1,160 @@
+"""Parity of the pressure projection on the GPU against the FP64 oracle.
+
+SetupPoisson and project_velocity must match bit for bit (same operation
+order, no FMA); the reference multigrid must reproduce the oracle's iterates;
+the B200 multigrid (FP64 and mixed) must converge to the oracle's solution
+within the residual tolerance.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def drop_problem(capi, orc, workloads, n, bc="periodic", ndrops=6, seed=0, ratio=1000.0):
+    desc = capi.make_desc((n, n, n), bc=bc, rho1=1.0, rho2=ratio)
+    cen, rad = workloads.drop_layout(ndrops, rmin=0.1, rmax=0.2, seed=seed, h=1.0 / n)
+    cvof, flag, _ = orc.init_spheres(desc, cen, rad, refinement=4)
+    rho = orc.linfunc(desc, cvof, desc.rho1, desc.rho2, capi.MEAN_ARITH)
+    rng = np.random.default_rng(seed + 7)
+    vel = []
+    for _ in range(3):
+        f = orc.zeros(desc)
+        orc.interior(desc, f)[...] = rng.standard_normal((n, n, n))
+        if bc == "periodic":
+            orc.fill_ghosts(desc, f)
+        vel.append(f)
+    if bc == "wall":
+        # no flow through the walls: u(is-1) = u(ie) = 0 etc.
+        g = desc.ng
+        vel[0][:, :, g - 1] = 0.0
+        vel[0][:, :, g + n - 1] = 0.0
+        vel[1][:, g - 1, :] = 0.0
+        vel[1][:, g + n - 1, :] = 0.0
+        vel[2][g - 1, :, :] = 0.0
+        vel[2][g + n - 1, :, :] = 0.0
+    return desc, cvof, rho, vel
+
+
+def upload_state(gpu, capi, cvof, rho, vel, p=None):
+    gpu.upload(capi.F_CVOF, cvof)
+    gpu.upload(capi.F_RHO, rho)
+    for f, a in zip((capi.F_U, capi.F_V, capi.F_W), vel):
+        gpu.upload(f, a)
+    gpu.upload(capi.F_P, p if p is not None else np.zeros_like(cvof))
+
+
+@pytest.mark.parametrize("bc", ["periodic", "wall"])
+def test_setup_poisson_bitwise(gpu_lib, capi, runtime, orc, workloads, bc):
+    desc, cvof, rho, vel = drop_problem(capi, orc, workloads, 16, bc=bc)
+    dt = 1e-3
+    st, A_ref = orc.setup_poisson(desc, *vel, rho, dt)
+    assert st == 0
+    with runtime.ParisGpu(desc) as gpu:
+        upload_state(gpu, capi, cvof, rho, vel)
+        gpu.setup_poisson(dt)
+        A = gpu.download(capi.F_A)
+    assert np.array_equal(A, A_ref)
+
+
+def test_linfunc_bitwise(gpu_lib, capi, runtime, orc, workloads):
+    desc, cvof, rho_ref, vel = drop_problem(capi, orc, workloads, 16)
+    with runtime.ParisGpu(desc) as gpu:
+        gpu.upload(capi.F_CVOF, cvof)
+        gpu.linfunc(capi.F_RHO)
+        rho = gpu.download(capi.F_RHO)
+    assert np.array_equal(rho, rho_ref)
+
+
+def test_poissonmg_known_answer(gpu_lib, capi, runtime, orc):
+    """Tests/PoissonMG: 32x16x16 periodic, XLENGTH=2, 20 V-cycles; residual
+    < 1e-8 and L1 error < 0.1 (Tests/PoissonMG/run.sh:13), same iterates as
+    the oracle."""
+    desc = capi.make_desc((32, 16, 16), length=(2.0, 1.0, 1.0), rho1=1.0, rho2=1e5)
+    rho = orc.zeros(desc) + 1.0
+    A = orc.setup_testmg(desc, rho)
+    p_ref = orc.zeros(desc)
+    st, it, tres_ref, hist = orc.new_solver_mg(desc, A, p_ref, 1e-300, beta=1.0, maxit=20, norm=2)
+    with runtime.ParisGpu(desc) as gpu:
+        gpu.upload(capi.F_RHO, rho)
+        gpu.setup_test_mg()
+        A_gpu = gpu.download(capi.F_A)
+        # A1..A7 bit for bit; the sin() of the right-hand side may differ by
+        # an ulp between the device and glibc
+        assert np.array_equal(A_gpu[:7], A[:7])
+        assert np.abs(A_gpu[7] - A[7]).max() <= 1e-14 * np.abs(A[7]).max()
+        gpu.upload(capi.F_P, orc.zeros(desc))
+        with pytest.warns(UserWarning):
+            r = gpu.new_solver(1e-300, beta=1.0, maxit=20, norm=2, mode=capi.MG_REFERENCE)
+        p = gpu.download(capi.F_P)
+        err = gpu.mg_test_err()
+    assert r.it == 21
+    assert r.res < 1e-8 and err < 0.1
+    assert abs(r.res - tres_ref) <= 1e-6 * tres_ref
+    assert np.abs(orc.interior(desc, p) - orc.interior(desc, p_ref)).max() <= 1e-12
+
+
+@pytest.mark.parametrize("bc", ["periodic", "wall"])
+def test_reference_mg_iterates(gpu_lib, capi, runtime, orc, workloads, bc):
+    desc, cvof, rho, vel = drop_problem(capi, orc, workloads, 16, bc=bc)
+    dt = 1e-3
+    st, A = orc.setup_poisson(desc, *vel, rho, dt)
+    p_ref = orc.zeros(desc)
+    orc.new_solver_mg(desc, A, p_ref, 1e-300, beta=1.0, maxit=5, norm=2)
+    with runtime.ParisGpu(desc) as gpu:
+        upload_state(gpu, capi, cvof, rho, vel)
+        gpu.setup_poisson(dt)
+        with pytest.warns(UserWarning):
+            gpu.new_solver(1e-300, beta=1.0, maxit=5, norm=2, mode=capi.MG_REFERENCE)
+        p = gpu.download(capi.F_P)
+    scale = np.abs(orc.interior(desc, p_ref)).max()
+    assert np.abs(orc.interior(desc, p) - orc.interior(desc, p_ref)).max() <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("mode,pcg", [(2, 0), (1, 0), (2, 1), (1, 1)])
+@pytest.mark.parametrize("bc", ["periodic", "wall"])
+def test_fast_mg_converges_to_oracle(gpu_lib, capi, runtime, orc, workloads, mode, pcg, bc):
+    """The B200 multigrid reaches ||r||/||b|| < 1e-10; its pressure agrees with
+    the oracle's FP64 solution of the same system (up to the constant of the
+    singular periodic/closed problem) to the tolerance amplified by the
+    condition of the operator."""
+    n = 32
+    desc, cvof, rho, vel = drop_problem(capi, orc, workloads, n, bc=bc)
+    dt = 1e-3
+    st, A = orc.setup_poisson(desc, *vel, rho, dt)
+    p_ref, it_ref, _ = orc.fastmg_solve(desc, A, np.zeros((n, n, n)), 1e-12, maxit=100, mixed=False, pcg=True)
+    with runtime.ParisGpu(desc) as gpu:
+        upload_state(gpu, capi, cvof, rho, vel)
+        gpu.setup_poisson(dt)
+        r = gpu.new_solver(0.0, maxit=60, mode=mode, rel_tol=1e-10, pcg=pcg)
+        p = orc.interior(desc, gpu.download(capi.F_P))
+        assert r.rel_res < 1e-10
+        assert r.it <= 25
+        # the residual computed independently in FP64 on the device
+        L1, L2, Linf = gpu.calc_residuals()
+    b = A[7]
+    assert L2 * np.sqrt(b.size) / np.sqrt((b ** 2).sum()) < 2e-10
+    d = (p - p.mean()) - (p_ref - p_ref.mean())
+    assert np.abs(d).max() <= 1e-7 * np.abs(p_ref - p_ref.mean()).max()
+
+
+@pytest.mark.parametrize("bc", ["periodic", "wall"])
+def test_project_velocity_bitwise(gpu_lib, capi, runtime, orc, workloads, bc):
+    desc, cvof, rho, vel = drop_problem(capi, orc, workloads, 16, bc=bc)
+    dt = 1e-3
+    rng = np.random.default_rng(5)
+    p = orc.zeros(desc)
+    orc.interior(desc, p)[...] = rng.standard_normal((16, 16, 16))
+    if bc == "periodic":
+        orc.fill_ghosts(desc, p)
+    ref = [v.copy() for v in vel]
+    orc.project_velocity(desc, *ref, p, rho, dt)
+    for v in ref:
+        if bc == "periodic":
+            orc.fill_ghosts(desc, v)
+    with runtime.ParisGpu(desc) as gpu:
+        upload_state(gpu, capi, cvof, rho, vel, p)
+        gpu.project_velocity(dt)
+        out = [gpu.download(f) for f in (capi.F_U, capi.F_V, capi.F_W)]
+    for a, b in zip(out, ref):
+        assert np.array_equal(a, b)

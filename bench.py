@@ -1,0 +1,456 @@
+#!/usr/bin/env python
+"""Throughput of the PARIS per-timestep grid core on B200.
+
+One step = vofsweeps (CIAM, three split sweeps) -> linfunc(rho) -> the
+predicted velocity u* into u (stand-in for the momentum predictor, which is
+outside this path) -> SetupPoisson -> NewSolver to ||r||_2/||b||_2 < 1e-10
+from p = 0 -> project_velocity, on the 256^3 periodic unit cube with 64 drops
+of radius U[0.03,0.08] at density ratio 1000 and a seeded Gaussian u*
+(unit variance, 3 Jacobi smoothing sweeps).  `value` uses the mixed-precision
+multigrid (FP32 V(2,2) cycles in an FP64 defect-correction loop) with inputs
+resident in HBM; `fp64_steps_per_s` the same algorithm all in FP64; `e2e`
+the same step through the C-ABI with host buffers (u* uploaded, u,v,w,cvof
+downloaded every step).  `--impl reference` times the reference algorithm
+(the CPU restatement in oracle/) on the host cores.
+
+Prints one JSON line (rank 0).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "steps/s @256³ VOF+MG projection, mixed vs FP64 MG at 1e-10 residual"
+REL_TOL = 1e-10
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=256, help="cells per direction of the workload")
+    ap.add_argument("--pcg", type=int, default=0, help="1: V-cycle preconditioned CG outer loop")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-only", action="store_true", help="a few profiled steps, no JSON timing")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+class Dist:
+    """One process per GPU; replicas only (the grid core does not shard)."""
+
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v):
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([float(v)], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+def load_pkg():
+    import __graft_entry__
+    return __graft_entry__.load_package()
+
+
+def smoothed_faces(n, seed=1, sweeps=3, ng=2):
+    """u*, v*, w*: i.i.d. N(0,1) per face, `sweeps` Jacobi sweeps
+    u <- (u + 6 face neighbours)/7 on the periodic grid; ghosted arrays."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(3):
+        u = rng.standard_normal((n, n, n))
+        for _ in range(sweeps):
+            p = np.pad(u, 1, mode="wrap")
+            u = (p[1:-1, 1:-1, 1:-1] + p[:-2, 1:-1, 1:-1] + p[2:, 1:-1, 1:-1] + p[1:-1, :-2, 1:-1]
+                 + p[1:-1, 2:, 1:-1] + p[1:-1, 1:-1, :-2] + p[1:-1, 1:-1, 2:]) / 7.0
+        a = np.pad(u, ng, mode="wrap")
+        out.append(np.ascontiguousarray(a))
+    return out
+
+
+def workload(pkg, n, device=0):
+    capi, wl = pkg.capi, pkg.workloads
+    desc = capi.make_desc((n, n, n), rho1=1.0, rho2=1000.0, device=device)
+    cen, rad = wl.drop_layout(64, rmin=0.03, rmax=0.08, seed=0, h=1.0 / n)
+    us = smoothed_faces(n, seed=1)
+    umax = max(float(np.abs(a).max()) for a in us)
+    dt = 0.25 * (1.0 / n) / umax
+    return desc, cen, rad, us, dt
+
+
+# algorithmic HBM bytes per cell of each labelled kernel (cells as recorded
+# by the profiler: the grid cells the launch processes)
+ALGO_BYTES = {
+    "mg_smooth_f32": 12.0,        # half of a red-black sweep: (p 4 + 3 faces 12 + rhs 4 + p write 4)/2
+    "mg_smooth_f64": 24.0,
+    "mg_restrict_f32": 20.5,      # x 4 + b 4 + 3 faces 12 + coarse rhs 4/8
+    "mg_restrict_f64": 41.0,
+    "mg_prolong_f32": 8.5,        # x read+write 8 + coarse 4/8
+    "mg_prolong_f64": 17.0,
+    "mg_residual_fp64(r32)": 44.0,  # 3 faces + rhs 32 + p 8 + r (FP32) 4
+    "mg_residual_fp64(r64)": 48.0,
+    "mg_correct_f32": 20.0,       # p read+write 16 + correction 4
+    "mg_correct_f64": 24.0,
+    "mg_coef0": 36.0,             # FP64 faces 24 -> FP32 faces 12
+    "vof_sweep": 25.0,            # c 8 + u_d 8 + new c 8 + flag 1
+    "setup_poisson": 64.0,        # u,v,w,rho 32 + 3 faces + rhs 32
+    "project_velocity": 64.0,     # p,rho 16 + u,v,w read+write 48
+    "linfunc": 16.0,              # cvof 8 + rho 8 (ghosted cells)
+}
+
+
+def gpu_step(gpu, capi, k, dt, mode, pcg):
+    gpu.vof_sweeps(k, dt)
+    gpu.linfunc(capi.F_RHO)
+    for dst, src in ((capi.F_U, capi.F_USTAR), (capi.F_V, capi.F_VSTAR), (capi.F_W, capi.F_WSTAR)):
+        gpu.copy_field(dst, src)
+    gpu.setup_poisson(dt)
+    gpu.fill_field(capi.F_P, 0.0)
+    r = gpu.new_solver(0.0, maxit=200, mode=mode, rel_tol=REL_TOL, pcg=pcg)
+    gpu.project_velocity(dt)
+    return r
+
+
+def roofline(report, peak):
+    rows = []
+    for name, (n, ms, cells) in report.items():
+        b = ALGO_BYTES.get(name)
+        gbs = b * cells / (ms * 1e-3) / 1e9 if (b and ms > 0) else None
+        rows.append({"kernel": name, "launches": n, "ms": round(ms, 4),
+                     "algo_bytes_per_launch": (b * cells / n) if b else None,
+                     "gbs": round(gbs, 1) if gbs else None,
+                     "frac": round(gbs / peak, 3) if gbs else None})
+    rows.sort(key=lambda r: -r["ms"])
+    return rows
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+class CpuReference:
+    """The reference algorithm on the host cores (the FP64 restatement in
+    oracle/, OpenMP over k): vofsweeps, linfunc, SetupPoisson, the reference
+    V-cycles (MGsolver.f90) and project_velocity.  The reference multigrid
+    needs hundreds of cycles at density ratio 1000, so a sample step runs
+    `cycles` V-cycles and the time to 1e-10 is extrapolated with the
+    asymptotic convergence rate measured once over `rate_cycles` cycles."""
+
+    def __init__(self, pkg, desc, us, dt, cvof=None, flag=None, cen=None, rad=None, cycles=2, rate_cycles=8):
+        from oracle import pyoracle as orc
+        self.orc, self.capi, self.desc, self.dt = orc, pkg.capi, desc, dt
+        self.us = us
+        if cvof is None:
+            cvof, flag, _ = orc.init_spheres(desc, cen, rad, refinement=8)
+        self.c, self.f = cvof.copy(), flag.copy()
+        self.u = [a.copy() for a in us]
+        self.cycles, self.rate_cycles = cycles, rate_cycles
+        self.rate = None
+        self.cores = len(os.sched_getaffinity(0))
+
+    def _pre(self, k):
+        orc, d = self.orc, self.desc
+        orc.vofsweeps(d, k, self.dt, self.c, self.f, *self.u)
+        rho = orc.linfunc(d, self.c, d.rho1, d.rho2, self.capi.MEAN_ARITH)
+        self.u = [a.copy() for a in self.us]
+        st, A = orc.setup_poisson(d, *self.u, rho, self.dt)
+        return rho, A
+
+    def measure_rate(self, k=0):
+        rho, A = self._pre(k)
+        p = self.orc.zeros(self.desc)
+        _, _, _, h = self.orc.new_solver_mg(self.desc, A, p, 0.0, beta=1.0, maxit=self.rate_cycles, norm=2)
+        self.rate = float((h[-1] / h[-4]) ** (1.0 / 3.0))
+        self.rms_b = float(np.sqrt(np.mean(A[7] ** 2)))
+        self.orc.project_velocity(self.desc, *self.u, p, rho, self.dt)
+        return self.rate
+
+    def step(self, k):
+        """Returns (seconds of the sample, extrapolated seconds to 1e-10)."""
+        t0 = time.perf_counter()
+        rho, A = self._pre(k)
+        t1 = time.perf_counter()
+        p = self.orc.zeros(self.desc)
+        _, _, _, h = self.orc.new_solver_mg(self.desc, A, p, 0.0, beta=1.0, maxit=self.cycles, norm=2)
+        t2 = time.perf_counter()
+        self.orc.project_velocity(self.desc, *self.u, p, rho, self.dt)
+        t3 = time.perf_counter()
+        rms_b = float(np.sqrt(np.mean(A[7] ** 2)))
+        target = REL_TOL * rms_b
+        more = max(0.0, np.log(target / h[-1]) / np.log(self.rate)) if h[-1] > target else 0.0
+        n_needed = self.cycles + int(np.ceil(more))
+        t_cycle = (t2 - t1) / self.cycles
+        self.n_needed = n_needed
+        return t3 - t0, (t1 - t0) + (t3 - t2) + n_needed * t_cycle
+
+
+def run_reference(args, dist):
+    pkg = load_pkg()
+    if dist.rank != 0:
+        return 0
+    n = args.n
+    desc, cen, rad, us, dt = workload(pkg, n)
+    ref = CpuReference(pkg, desc, us, dt, cen=cen, rad=rad)
+    ref.measure_rate()
+    for k in range(args.warmup):
+        ref.step(k)
+    samples, est = [], []
+    for k in range(args.steps):
+        s, e = ref.step(args.warmup + k)
+        samples.append(s)
+        est.append(e)
+    t_est = float(np.mean(est))
+    v = 1.0 / t_est
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_est * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{n}^3 periodic unit cube, 64 drops r~U[0.03,0.08], rho ratio 1000, "
+                               "smoothed Gaussian u*, CIAM VOF + reference MG V-cycles to rel. residual 1e-10",
+                   "cells": n ** 3, "solver": "reference MG (MGsolver.f90), FP64, nrelax=3",
+                   "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": v, "unit": "steps/s", "cores": ref.cores, "kind": "port",
+                         "sample": f"each step: VOF+linfunc+SetupPoisson+project and {ref.cycles} reference "
+                                   f"V-cycles at {n}^3; time to 1e-10 extrapolated with the measured "
+                                   f"asymptotic rate {ref.rate:.4f}/cycle ({ref.n_needed} cycles); "
+                                   f"sample wall {np.mean(samples):.1f} s"},
+        "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "mg_cycles_to_tol": ref.n_needed,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def run_b200(args, dist):
+    import torch
+    pkg = load_pkg()
+    capi, runtime = pkg.capi, pkg.runtime
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    n = args.n
+    desc, cen, rad, us, dt = workload(pkg, n, device=dev)
+    gpu = runtime.ParisGpu(desc)
+    gpu.init_spheres(cen, rad, refinement=8)
+    for f, a in zip((capi.F_USTAR, capi.F_VSTAR, capi.F_WSTAR), us):
+        gpu.upload(f, a)
+    for dst, src in ((capi.F_U, capi.F_USTAR), (capi.F_V, capi.F_VSTAR), (capi.F_W, capi.F_WSTAR)):
+        gpu.copy_field(dst, src)
+    # initial projection gives the divergence-free velocity the first sweep uses
+    gpu.linfunc(capi.F_RHO)
+    gpu.setup_poisson(dt)
+    gpu.fill_field(capi.F_P, 0.0)
+    gpu.new_solver(0.0, maxit=200, mode=capi.MG_MIXED, rel_tol=REL_TOL, pcg=args.pcg)
+    gpu.project_velocity(dt)
+    cvof0 = gpu.download(capi.F_CVOF) if (dist.rank == 0 and not args.no_cpu_baseline) else None
+    flag0 = gpu.download(capi.F_VOF_FLAG) if cvof0 is not None else None
+    stream = torch.cuda.ExternalStream(gpu.stream())
+    peak, peak_kind = measured_peak()
+
+    if args.profile_only:
+        gpu.profile(True)
+        for k in range(max(1, args.steps)):
+            gpu_step(gpu, capi, k, dt, capi.MG_MIXED, args.pcg)
+        gpu.profile(False)
+        rep = gpu.profile_report()
+        if dist.rank == 0:
+            print(json.dumps({"profile": roofline(rep, peak)}), flush=True)
+        gpu.close()
+        return 0
+
+    def timed(mode, steps, k0):
+        for k in range(args.warmup):
+            gpu_step(gpu, capi, k0 + k, dt, mode, args.pcg)
+        gpu.sync()
+        dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        its = []
+        l0 = gpu.launch_count()
+        e0.record(stream)
+        for k in range(steps):
+            r = gpu_step(gpu, capi, k0 + args.warmup + k, dt, mode, args.pcg)
+            its.append(r.it)
+        e1.record(stream)
+        e1.synchronize()
+        gpu.sync()
+        launches = gpu.launch_count() - l0
+        ms = dist.max(e0.elapsed_time(e1))
+        dist.barrier()
+        return ms, its, launches
+
+    clocks = Clocks(dev)
+    clocks.start()
+    ms, its, launches = timed(capi.MG_MIXED, args.steps, 0)
+    clk = clocks.stop()
+    ms64, its64, _ = timed(capi.MG_FP64, args.steps, 1000)
+
+    # per-kernel CUDA-event profile of the same step (separate, after timing)
+    gpu.profile(True)
+    for k in range(2):
+        gpu_step(gpu, capi, 2000 + k, dt, capi.MG_MIXED, args.pcg)
+    gpu.profile(False)
+    rows = roofline(gpu.profile_report(), peak)
+    top = rows[0]
+
+    # end to end through the C-ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        shape = us[0].shape
+        h_in = [torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
+        for h, a in zip(h_in, us):
+            h[...] = a
+        h_out = [torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy() for _ in range(4)]
+        e_steps = max(1, args.steps)
+        gpu.sync()
+        dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        for k in range(e_steps):
+            for f, h in zip((capi.F_USTAR, capi.F_VSTAR, capi.F_WSTAR), h_in):
+                gpu.upload_from(f, h)
+            gpu_step(gpu, capi, 3000 + k, dt, capi.MG_MIXED, args.pcg)
+            for f, h in zip((capi.F_U, capi.F_V, capi.F_W, capi.F_CVOF), h_out):
+                gpu.download_into(f, h)
+        e1.record(stream)
+        e1.synchronize()
+        wall = time.perf_counter() - t0
+        ems = dist.max(e0.elapsed_time(e1))
+        dist.barrier()
+        nb = int(np.prod(shape)) * 8
+        e2e = {"value": dist.world * e_steps / (ems / 1e3), "unit": "steps/s", "h2d_bytes_per_step": 3 * nb,
+               "d2h_bytes_per_step": 4 * nb, "steps": e_steps, "host_wall_s": round(wall, 3)}
+
+    cpu = None
+    if dist.rank == 0 and not args.no_cpu_baseline:
+        ref = CpuReference(pkg, desc, us, dt, cvof=cvof0, flag=flag0)
+        ref.measure_rate()
+        s, est = ref.step(0)
+        cpu = {"value": 1.0 / est, "unit": "steps/s", "cores": ref.cores, "kind": "port",
+               "sample": f"one step at {n}^3 (VOF+linfunc+SetupPoisson+project and {ref.cycles} reference "
+                         f"V-cycles, {s:.1f} s wall); time to 1e-10 extrapolated with the measured rate "
+                         f"{ref.rate:.4f}/cycle over {ref.n_needed} cycles"}
+    gpu.close()
+    if dist.rank != 0:
+        return 0
+    value = dist.world * args.steps / (ms / 1e3)
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+        "config": {"workload": f"{n}^3 periodic unit cube, 64 drops r~U[0.03,0.08] (seed 0), rho 1000/1, "
+                               "smoothed Gaussian u* (seed 1), CIAM VOF + B200 MG to ||r||/||b|| < 1e-10 from p=0",
+                   "cells": n ** 3, "solver": ("mixed FP32 V(2,2) in FP64 " + ("PCG" if args.pcg else
+                                                                                 "defect correction")),
+                   "parallelism": f"replicas x{dist.world}", "l2": "inputs larger than L2 (141 MB per field)"},
+        "fp64_steps_per_s": dist.world * args.steps / (ms64 / 1e3),
+        "mg_iterations": {"mixed": its, "fp64": its64},
+        "mcell_updates_per_s": value * n ** 3 / 1e6,
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": top["kernel"], "achieved": top["gbs"], "peak": peak,
+                     "unit": "GB/s", "frac": top["frac"], "traffic": None,
+                     "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                     "algo_bytes_per_launch": top["algo_bytes_per_launch"]},
+        "kernels": rows[:12],
+        "clocks": clk,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    dist = Dist()
+    try:
+        rc = run_reference(args, dist) if args.impl == "reference" else run_b200(args, dist)
+    finally:
+        dist.close()
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -93,7 +93,10 @@ typedef struct paris_ctx* paris_handle_t;
 #define PARIS_FIELD_A        12   /* A(is:ie,js:je,ks:ke,8), no ghosts */
 #define PARIS_FIELD_HEIGHT   13   /* height(imin:imax,...,6) */
 #define PARIS_FIELD_VOF_PHASE 14  /* integer vof_phase (host int32) */
-#define PARIS_NFIELDS        15
+#define PARIS_FIELD_USTAR    15   /* caller scratch face fields, e.g. the predicted  */
+#define PARIS_FIELD_VSTAR    16   /* velocity u* kept on the device between steps    */
+#define PARIS_FIELD_WSTAR    17
+#define PARIS_NFIELDS        18
 
 /* ---- life cycle (replaces the allocations of initialize/initialize_VOF,
  *      paris.f90:3016-3031 and init_MG, MGsolver.f90:34-65) --------------- */
@@ -105,6 +108,10 @@ int paris_gpu_finalize(paris_handle_t h);
  * take int32 arrays, every other field real(8).                           */
 int paris_gpu_upload(paris_handle_t h, int32_t field, const void* host);
 int paris_gpu_download(paris_handle_t h, int32_t field, void* host);
+/* Device-to-device copy of one real(8) field into another (ghosts included). */
+int paris_gpu_copy_field(paris_handle_t h, int32_t dst_field, int32_t src_field);
+/* Set every element of a real(8) field (ghosts included) to value. */
+int paris_gpu_fill_field(paris_handle_t h, int32_t field, double value);
 /* Block until all work queued on the handle's stream has finished. */
 int paris_gpu_sync(paris_handle_t h);
 /* The cudaStream_t the handle issues all work on (as void*). */
@@ -115,6 +122,14 @@ void* paris_gpu_field_ptr(paris_handle_t h, int32_t field);
 const char* paris_gpu_last_error(paris_handle_t h);
 /* Number of kernels this handle launched since creation (launch counter). */
 int64_t paris_gpu_launch_count(paris_handle_t h);
+/* Per-kernel timing with CUDA events on the handle's stream: enable = 1
+ * clears the table and brackets every following launch with two events,
+ * enable = 0 stops.  The report is one line per kernel,
+ * "name<TAB>launches<TAB>total_ms<TAB>cells", cells being the sum over the
+ * launches of the grid cells each launch processed.  Returns the bytes
+ * needed (including the terminating 0); writes at most len bytes.          */
+int paris_gpu_profile(paris_handle_t h, int32_t enable);
+int64_t paris_gpu_profile_report(paris_handle_t h, char* buf, int64_t len);
 
 /* ---- VOF (replaces vofsweeps, vofmodules.f90:1340-1361, with
  *      swp/swpz/swpr, vofnonmodule.f90:27-48,126-237,664-754) ------------ */

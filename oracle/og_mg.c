@@ -36,6 +36,7 @@ int og_setup_poisson(const paris_grid_desc* desc, const double* u, const double*
     long N = (long)nx * ny * nz;
     long sy = g->sy, sz = g->sz;
     int status = 0;
+#pragma omp parallel for schedule(static)
     for (int k = ng; k < ng + nz; k++)
         for (int j = ng; j < ng + ny; j++)
             for (int i = ng; i < ng + nx; i++) {
@@ -226,6 +227,7 @@ static double og_get_residual(const og_mg* mg, const og_level* l, double* A, con
     int ng = mg->g->ng;
     long N = l->N;
     double en = 0.0;
+#pragma omp parallel for reduction(+ : en) schedule(static)
     for (int k = 0; k < l->n[2]; k++)
         for (int j = 0; j < l->n[1]; j++)
             for (int i = 0; i < l->n[0]; i++) {
@@ -246,6 +248,7 @@ static double og_compute_residual(const og_grid* g, const double* A, const doubl
     int ng = g->ng, nx = g->nx, ny = g->ny, nz = g->nz;
     long N = (long)nx * ny * nz;
     double en = 0.0;
+#pragma omp parallel for reduction(+ : en) schedule(static)
     for (int k = 0; k < nz; k++)
         for (int j = 0; j < ny; j++)
             for (int i = 0; i < nx; i++) {
@@ -265,6 +268,7 @@ static double og_compute_residual(const og_grid* g, const double* A, const doubl
  * (1,1,0),(1,0,1),(1,1,1) in (di,dj,dk). */
 static void og_fill_coefficients(const og_level* f, og_level* c) {
     static const int ord[8][3] = {{0,0,0},{0,1,0},{0,0,1},{0,1,1},{1,0,0},{1,1,0},{1,0,1},{1,1,1}};
+#pragma omp parallel for collapse(2) schedule(static)
     for (int comp = 0; comp < 8; comp++)
         for (int k = 0; k < c->n[2]; k++)
             for (int j = 0; j < c->n[1]; j++)
@@ -282,6 +286,7 @@ static void og_fill_coefficients(const og_level* f, og_level* c) {
 /* coarse_from_fine, MGsolver.f90:185-201: Ac8 = 0; Ac8 += Af8*0.125 over
  * i1,j1,k1 = 0..1 with k1 fastest */
 static void og_coarse_from_fine(const og_level* f, og_level* c) {
+#pragma omp parallel for schedule(static)
     for (int k = 0; k < c->n[2]; k++)
         for (int j = 0; j < c->n[1]; j++)
             for (int i = 0; i < c->n[0]; i++) {
@@ -300,6 +305,7 @@ static void og_coarse_from_fine(const og_level* f, og_level* c) {
  * sym_MG weights the 8 children by |pf| (pf was just zeroed by the caller). */
 static void og_coarse_fine_interp(const og_mg* mg, og_level* f, const og_level* c, int sym) {
     int ng = mg->g->ng;
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < c->n[0]; i++)
         for (int j = 0; j < c->n[1]; j++)
             for (int k = 0; k < c->n[2]; k++) {
@@ -343,12 +349,14 @@ static void og_mg_iteration(og_mg* mg, double beta, int norm) {
         og_coarse_fine_interp(mg, l, &mg->lev[L - 1], mg->sym);
         og_apply_bc_mg(mg, l, l->e);
         og_get_residual(mg, l, l->K, l->e, norm);
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < l->ntot; q++) l->p[q] = l->p[q] + l->e[q];
         memset(l->e, 0, l->ntot * sizeof(double));
         for (int r = 0; r < mg->nrelax; r++) {
             og_rb_relax(mg, l, l->K, l->e, beta);
             og_apply_bc_mg(mg, l, l->e);
         }
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < l->ntot; q++) l->p[q] = l->p[q] + l->e[q];
         og_get_residual(mg, l, l->K, l->e, norm);
     }
@@ -447,18 +455,21 @@ int og_project_velocity(const paris_grid_desc* desc, double* u, double* v, doubl
     if (g->d.bdry_cond[0] != PARIS_BC_PERIODIC) ieu--;
     if (g->d.bdry_cond[1] != PARIS_BC_PERIODIC) jev--;
     if (g->d.bdry_cond[2] != PARIS_BC_PERIODIC) kew--;
+#pragma omp parallel for schedule(static)
     for (int k = ng; k < ng + g->nz; k++)
         for (int j = ng; j < ng + g->ny; j++)
             for (int i = ng; i <= ieu; i++) {
                 long n = OG_IX(g, i, j, k);
                 u[n] = u[n] - dt * (2.0 * og_mask(g, 0, i) / g->dxh[i]) * (p[n + 1] - p[n]) / (rho[n + 1] + rho[n]);
             }
+#pragma omp parallel for schedule(static)
     for (int k = ng; k < ng + g->nz; k++)
         for (int j = ng; j <= jev; j++)
             for (int i = ng; i < ng + g->nx; i++) {
                 long n = OG_IX(g, i, j, k);
                 v[n] = v[n] - dt * (2.0 * og_mask(g, 1, j) / g->dyh[j]) * (p[n + sy] - p[n]) / (rho[n + sy] + rho[n]);
             }
+#pragma omp parallel for schedule(static)
     for (int k = ng; k <= kew; k++)
         for (int j = ng; j < ng + g->ny; j++)
             for (int i = ng; i < ng + g->nx; i++) {

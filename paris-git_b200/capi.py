@@ -23,7 +23,7 @@ MEAN_ARITH, MEAN_HARM = 101, 102
 
 # fields
 (F_CVOF, F_U, F_V, F_W, F_RHO, F_P, F_DU, F_DV, F_DW, F_KAPPA, F_MU, F_VOF_FLAG,
- F_A, F_HEIGHT, F_VOF_PHASE) = range(15)
+ F_A, F_HEIGHT, F_VOF_PHASE, F_USTAR, F_VSTAR, F_WSTAR) = range(18)
 
 # solver modes
 MG_REFERENCE, MG_FP64, MG_MIXED = 0, 1, 2
@@ -122,6 +122,10 @@ _PROTOS = {
     "paris_gpu_upload": (_I, [_P, _I, _P]),
     "paris_gpu_download": (_I, [_P, _I, _P]),
     "paris_gpu_sync": (_I, [_P]),
+    "paris_gpu_copy_field": (_I, [_P, _I, _I]),
+    "paris_gpu_fill_field": (_I, [_P, _I, _D]),
+    "paris_gpu_profile": (_I, [_P, _I]),
+    "paris_gpu_profile_report": (ctypes.c_int64, [_P, ctypes.c_char_p, ctypes.c_int64]),
     "paris_gpu_stream": (_P, [_P]),
     "paris_gpu_field_ptr": (_P, [_P, _I]),
     "paris_gpu_last_error": (ctypes.c_char_p, [_P]),

@@ -67,11 +67,20 @@ void ctx_set_error(paris_ctx* c, const char* fmt, ...);
         }                                                                           \
     } while (0)
 
+// Optional per-kernel CUDA-event timing (paris_gpu_profile).
+void prof_begin(paris_ctx* c, const char* name, long cells);
+void prof_end(paris_ctx* c);
+int prof_enabled(const paris_ctx* c);
+
 // Launch with bookkeeping: counts every kernel the handle issues and checks
-// the launch.  Use inside functions returning int.
-#define PARIS_LAUNCH(ctx, kernel, grid, block, smem, ...)                           \
+// the launch; `name` and `cells` label the launch in the profile.  Use inside
+// functions returning int.
+#define PARIS_LAUNCH_N(ctx, name, cells, kernel, grid, block, smem, ...)            \
     do {                                                                            \
+        bool _prof = prof_enabled(ctx);                                             \
+        if (_prof) prof_begin((ctx), (name), (cells));                              \
         kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);            \
+        if (_prof) prof_end(ctx);                                                   \
         (ctx)->launches++;                                                          \
         cudaError_t _e = cudaGetLastError();                                        \
         if (_e != cudaSuccess) {                                                    \
@@ -80,6 +89,9 @@ void ctx_set_error(paris_ctx* c, const char* fmt, ...);
             return PARIS_CUDA_ERROR;                                                \
         }                                                                           \
     } while (0)
+
+#define PARIS_LAUNCH(ctx, kernel, grid, block, smem, ...) \
+    PARIS_LAUNCH_N(ctx, #kernel, 0L, kernel, grid, block, smem, __VA_ARGS__)
 
 #define PARIS_CHECK(expr)                       \
     do {                                        \

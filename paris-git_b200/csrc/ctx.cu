@@ -269,6 +269,7 @@ extern "C" int paris_gpu_finalize(paris_handle_t c) {
     for (auto& l : c->fl32) { free_ptr(l.cx); free_ptr(l.cy); free_ptr(l.cz); free_ptr(l.b); free_ptr(l.x); }
     for (auto& l : c->fl64) { free_ptr(l.cx); free_ptr(l.cy); free_ptr(l.cz); free_ptr(l.b); free_ptr(l.x); }
     if (c->red_host) cudaFreeHost(c->red_host);
+    for (auto e : c->evpool) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PARIS_OK;
@@ -367,6 +368,33 @@ extern "C" int paris_gpu_download(paris_handle_t c, int32_t field, void* host) {
     return PARIS_OK;
 }
 
+static bool real_field(int f) {
+    return f >= 0 && f < PARIS_NFIELDS && f != PARIS_FIELD_VOF_FLAG && f != PARIS_FIELD_A &&
+           f != PARIS_FIELD_HEIGHT && f != PARIS_FIELD_VOF_PHASE;
+}
+
+extern "C" int paris_gpu_copy_field(paris_handle_t c, int32_t dst, int32_t src) {
+    if (!c || !real_field(dst) || !real_field(src) || !c->fld[src]) return PARIS_BAD_ARGS;
+    cudaSetDevice(c->dev);
+    PARIS_CHECK(ctx_alloc_field(c, dst));
+    PARIS_CUDA_TRY(c, cudaMemcpyAsync(c->fld[dst], c->fld[src], c->L.total * sizeof(double), cudaMemcpyDeviceToDevice,
+                                      c->stream));
+    return PARIS_OK;
+}
+
+__global__ void k_fill(double* __restrict__ f, double v, long n) {
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t < n) f[t] = v;
+}
+
+extern "C" int paris_gpu_fill_field(paris_handle_t c, int32_t field, double value) {
+    if (!c || !real_field(field)) return PARIS_BAD_ARGS;
+    cudaSetDevice(c->dev);
+    PARIS_CHECK(ctx_alloc_field(c, field));
+    PARIS_LAUNCH(c, k_fill, div_up(c->L.total, 256), 256, 0, c->fld[field], value, c->L.total);
+    return PARIS_OK;
+}
+
 extern "C" int paris_gpu_sync(paris_handle_t c) {
     if (!c) return PARIS_BAD_ARGS;
     PARIS_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -387,6 +415,64 @@ extern "C" void* paris_gpu_field_ptr(paris_handle_t c, int32_t field) {
 extern "C" const char* paris_gpu_last_error(paris_handle_t c) { return c ? c->err : "null handle"; }
 
 extern "C" int64_t paris_gpu_launch_count(paris_handle_t c) { return c ? c->launches : 0; }
+
+// ---- per-kernel event timing --------------------------------------------------
+int prof_enabled(const paris_ctx* c) { return c->prof_on; }
+
+void prof_begin(paris_ctx* c, const char* name, long cells) {
+    size_t need = 2 * (c->prof.size() + 1);
+    while (c->evpool.size() < need) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) { c->prof_on = 0; return; }
+        c->evpool.push_back(e);
+    }
+    int ev = (int)(2 * c->prof.size());
+    c->prof.push_back(paris_ctx::ProfRec{name, cells, ev});
+    cudaEventRecord(c->evpool[ev], c->stream);
+}
+
+void prof_end(paris_ctx* c) {
+    if (c->prof.empty()) return;
+    cudaEventRecord(c->evpool[c->prof.back().ev + 1], c->stream);
+}
+
+extern "C" int paris_gpu_profile(paris_handle_t c, int32_t enable) {
+    if (!c) return PARIS_BAD_ARGS;
+    if (enable) c->prof.clear();
+    c->prof_on = enable ? 1 : 0;
+    return PARIS_OK;
+}
+
+extern "C" int64_t paris_gpu_profile_report(paris_handle_t c, char* buf, int64_t len) {
+    if (!c) return -1;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return -1;
+    struct Acc { std::string name; long n; double ms; double cells; };
+    std::vector<Acc> acc;
+    for (const auto& r : c->prof) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->evpool[r.ev], c->evpool[r.ev + 1]);
+        Acc* a = nullptr;
+        for (auto& x : acc)
+            if (x.name == r.name) { a = &x; break; }
+        if (!a) { acc.push_back(Acc{r.name, 0, 0.0, 0.0}); a = &acc.back(); }
+        a->n++;
+        a->ms += ms;
+        a->cells += (double)r.cells;
+    }
+    std::string out;
+    char line[512];
+    for (const auto& a : acc) {
+        snprintf(line, sizeof(line), "%s\t%ld\t%.6f\t%.0f\n", a.name.c_str(), a.n, a.ms, a.cells);
+        out += line;
+    }
+    int64_t need = (int64_t)out.size() + 1;
+    if (buf && len > 0) {
+        int64_t m = need < len ? need : len;
+        memcpy(buf, out.c_str(), m - 1);
+        buf[m - 1] = 0;
+    }
+    return need;
+}
 
 int ctx_ensure_matrix(paris_ctx* c) {
     if (!c->cx) {

@@ -68,6 +68,15 @@ struct paris_ctx {
     double* fast_zold64 = nullptr;
     int64_t launches = 0;
     char err[512] = {0};
+    // per-kernel event timing
+    struct ProfRec {
+        const char* name;
+        long cells;
+        int ev;   // index of the start event in evpool (stop = ev + 1)
+    };
+    int prof_on = 0;
+    std::vector<ProfRec> prof;
+    std::vector<cudaEvent_t> evpool;
 };
 
 static constexpr int kRedBlocks = 1184;   // 148 SMs x 8

@@ -9,6 +9,7 @@
 // The inner cycle runs in T = float (mixed) or double; the outer loop is FP64:
 // defect correction p += V(b - A p), or CG preconditioned by the V-cycle.
 // Levels at or below kCoarseCells cells run in one single-block kernel.
+#include <string.h>
 #include "ctx.cuh"
 
 static constexpr long kCoarseCells = 4096;   // 16^3
@@ -323,6 +324,29 @@ __global__ void k_pcg_dir(double* __restrict__ d, const double* __restrict__ z, 
 }
 
 // ---- host side ---------------------------------------------------------------
+// profile label of a kernel instantiated for T (stable strings)
+template <typename T>
+static const char* kname(const char* base);
+template <>
+const char* kname<float>(const char* base) {
+    static const char* names[] = {"mg_smooth_f32", "mg_restrict_f32", "mg_prolong_f32", "mg_coarse_cycle_f32",
+                                  "mg_correct_f32", "mg_residual_fp64(r32)"};
+    static const char* keys[] = {"mg_smooth", "mg_restrict", "mg_prolong", "mg_coarse_cycle", "mg_correct",
+                                 "mg_residual_fp64"};
+    for (int q = 0; q < 6; q++)
+        if (!strcmp(base, keys[q])) return names[q];
+    return base;
+}
+template <>
+const char* kname<double>(const char* base) {
+    static const char* names[] = {"mg_smooth_f64", "mg_restrict_f64", "mg_prolong_f64", "mg_coarse_cycle_f64",
+                                  "mg_correct_f64", "mg_residual_fp64(r64)"};
+    static const char* keys[] = {"mg_smooth", "mg_restrict", "mg_prolong", "mg_coarse_cycle", "mg_correct",
+                                 "mg_residual_fp64"};
+    for (int q = 0; q < 6; q++)
+        if (!strcmp(base, keys[q])) return names[q];
+    return base;
+}
 template <typename T>
 static std::vector<FastLevel<T>>& levels(paris_ctx* c);
 template <>
@@ -369,10 +393,10 @@ static LV<T> view(const FastLevel<T>& l) {
 template <typename T>
 static int fast_coefs(paris_ctx* c) {
     auto& lv = levels<T>(c);
-    PARIS_LAUNCH(c, k_fast_coef0<T>, div_up(c->N, 256), 256, 0, c->cx, c->cy, c->cz, lv[0].cx, lv[0].cy, lv[0].cz,
+    PARIS_LAUNCH_N(c, "mg_coef0", c->N, k_fast_coef0<T>, div_up(c->N, 256), 256, 0, c->cx, c->cy, c->cz, lv[0].cx, lv[0].cy, lv[0].cz,
                  c->N);
     for (int L = 1; L < (int)lv.size(); L++)
-        PARIS_LAUNCH(c, k_fast_coarsen<T>, div_up(lv[L].N, 256), 256, 0, view(lv[L - 1]), view(lv[L]), lv[L].cx,
+        PARIS_LAUNCH_N(c, "mg_coarsen", lv[L].N, k_fast_coarsen<T>, div_up(lv[L].N, 256), 256, 0, view(lv[L - 1]), view(lv[L]), lv[L].cx,
                      lv[L].cy, lv[L].cz);
     return PARIS_OK;
 }
@@ -389,23 +413,23 @@ static int vcycle(paris_ctx* c, int nu1, int nu2) {
         LV<T> v = view(lv[L]);
         long nh = (long)((v.n0 + 1) / 2) * v.n1 * v.n2;
         for (int s = 0; s < nu1; s++) {
-            PARIS_LAUNCH(c, k_fast_smooth<T>, div_up(nh, 256), 256, 0, v, c->bnd, 0);
-            PARIS_LAUNCH(c, k_fast_smooth<T>, div_up(nh, 256), 256, 0, v, c->bnd, 1);
+            PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, div_up(nh, 256), 256, 0, v, c->bnd, 0);
+            PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, div_up(nh, 256), 256, 0, v, c->bnd, 1);
         }
         LV<T> cv = view(lv[L + 1]);
-        PARIS_LAUNCH(c, k_fast_restrict<T>, div_up(cv.N, 256), 256, 0, v, cv, c->bnd);
+        PARIS_LAUNCH_N(c, kname<T>("mg_restrict"), v.N, k_fast_restrict<T>, div_up(cv.N, 256), 256, 0, v, cv, c->bnd);
         if (L + 1 < Lc) PARIS_CUDA_TRY(c, cudaMemsetAsync(lv[L + 1].x, 0, lv[L + 1].N * sizeof(T), c->stream));
     }
     LVSet<T> S;
     for (int L = 0; L < nl; L++) S.l[L] = view(lv[L]);
-    PARIS_LAUNCH(c, k_fast_coarse_cycle<T>, 1, 1024, 0, S, Lc, nl, c->bnd, nu1, nu2);
+    PARIS_LAUNCH_N(c, kname<T>("mg_coarse_cycle"), lv[Lc].N, k_fast_coarse_cycle<T>, 1, 1024, 0, S, Lc, nl, c->bnd, nu1, nu2);
     for (int L = Lc - 1; L >= 0; L--) {
         LV<T> v = view(lv[L]);
-        PARIS_LAUNCH(c, k_fast_prolong<T>, div_up(v.N, 256), 256, 0, v, view(lv[L + 1]));
+        PARIS_LAUNCH_N(c, kname<T>("mg_prolong"), v.N, k_fast_prolong<T>, div_up(v.N, 256), 256, 0, v, view(lv[L + 1]));
         long nh = (long)((v.n0 + 1) / 2) * v.n1 * v.n2;
         for (int s = 0; s < nu2; s++) {
-            PARIS_LAUNCH(c, k_fast_smooth<T>, div_up(nh, 256), 256, 0, v, c->bnd, 1);
-            PARIS_LAUNCH(c, k_fast_smooth<T>, div_up(nh, 256), 256, 0, v, c->bnd, 0);
+            PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, div_up(nh, 256), 256, 0, v, c->bnd, 1);
+            PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, div_up(nh, 256), 256, 0, v, c->bnd, 0);
         }
     }
     return PARIS_OK;
@@ -425,7 +449,7 @@ static int solve_dc(paris_ctx* c, const paris_solve_opts* o, paris_solve_result*
     Mat64 A{c->cx, c->cy, c->cz, c->rhs};
     double* p = c->fld[PARIS_FIELD_P];
     double s[3], tres, rel;
-    PARIS_LAUNCH(c, k_fast_residual64<T>, kRedBlocks, 256, 0, A, p, c->L, c->bnd, lv[0].b, (double*)nullptr,
+    PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>, kRedBlocks, 256, 0, A, p, c->L, c->bnd, lv[0].b, (double*)nullptr,
                  c->red_part);
     PARIS_CHECK(ctx_reduce_finish(c, 3, s));
     double bn2 = s[2];
@@ -435,8 +459,8 @@ static int solve_dc(paris_ctx* c, const paris_solve_opts* o, paris_solve_result*
     int nu1 = o->nu1 > 0 ? o->nu1 : 2, nu2 = o->nu2 > 0 ? o->nu2 : 2;
     while (!done && it < o->maxit) {
         PARIS_CHECK(vcycle<T>(c, nu1, nu2));
-        PARIS_LAUNCH(c, k_fast_correct<T>, div_up(c->N, 256), 256, 0, p, lv[0].x, c->L, 1.0);
-        PARIS_LAUNCH(c, k_fast_residual64<T>, kRedBlocks, 256, 0, A, p, c->L, c->bnd, lv[0].b, (double*)nullptr,
+        PARIS_LAUNCH_N(c, kname<T>("mg_correct"), c->N, k_fast_correct<T>, div_up(c->N, 256), 256, 0, p, lv[0].x, c->L, 1.0);
+        PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>, kRedBlocks, 256, 0, A, p, c->L, c->bnd, lv[0].b, (double*)nullptr,
                      c->red_part);
         PARIS_CHECK(ctx_reduce_finish(c, 3, s));
         it++;
@@ -479,7 +503,7 @@ static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result
     Mat64 A{c->cx, c->cy, c->cz, c->rhs};
     double* p = c->fld[PARIS_FIELD_P];
     double s[3], tres, rel;
-    PARIS_LAUNCH(c, k_fast_residual64<T>, kRedBlocks, 256, 0, A, p, c->L, c->bnd, (T*)nullptr, c->fast_r64,
+    PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>, kRedBlocks, 256, 0, A, p, c->L, c->bnd, (T*)nullptr, c->fast_r64,
                  c->red_part);
     PARIS_CHECK(ctx_reduce_finish(c, 3, s));
     double bn2 = s[2];

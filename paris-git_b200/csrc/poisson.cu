@@ -117,7 +117,7 @@ extern "C" int paris_setup_poisson(paris_handle_t c, double dt, double volume_so
     if (!(dt > 0.0)) return PARIS_BAD_ARGS;
     cudaSetDevice(c->dev);
     PARIS_CHECK(ctx_ensure_matrix(c));
-    PARIS_LAUNCH(c, k_setup_poisson, kRedBlocks, 256, 0, c->fld[PARIS_FIELD_U], c->fld[PARIS_FIELD_V],
+    PARIS_LAUNCH_N(c, "setup_poisson", c->N, k_setup_poisson, kRedBlocks, 256, 0, c->fld[PARIS_FIELD_U], c->fld[PARIS_FIELD_V],
                  c->fld[PARIS_FIELD_W], c->fld[PARIS_FIELD_RHO], c->cx, c->cy, c->cz, c->rhs, c->L, c->bnd,
                  metric(c), dt, volume_source, c->red_part);
     double out[2];
@@ -264,7 +264,7 @@ __global__ void k_project(double* __restrict__ u, double* __restrict__ v, double
 extern "C" int paris_project_velocity(paris_handle_t c, double dt) {
     if (!c) return PARIS_BAD_ARGS;
     cudaSetDevice(c->dev);
-    PARIS_LAUNCH(c, k_project, cell_grid(c->L), cell_block(), 0, c->fld[PARIS_FIELD_U], c->fld[PARIS_FIELD_V],
+    PARIS_LAUNCH_N(c, "project_velocity", c->N, k_project, cell_grid(c->L), cell_block(), 0, c->fld[PARIS_FIELD_U], c->fld[PARIS_FIELD_V],
                  c->fld[PARIS_FIELD_W], c->fld[PARIS_FIELD_P], c->fld[PARIS_FIELD_RHO], c->L, c->bnd, metric(c), dt);
     // SetVelocityBC + do_ghost_vector follow the projection (paris.f90:590-591)
     PARIS_CHECK(ctx_ghost_fill(c, c->fld[PARIS_FIELD_U]));

@@ -254,9 +254,9 @@ static int sweep(paris_ctx* c, int d, double dt) {
     int tx, ty, tz;
     tile_shape(d, tx, ty, tz);
     dim3 grid(div_up(c->L.n[0], tx), div_up(c->L.n[1], ty), div_up(c->L.n[2], tz));
-    PARIS_LAUNCH(c, k_vof_sweep, grid, kSweepThreads, 0, a);
+    PARIS_LAUNCH_N(c, "vof_sweep", c->N, k_vof_sweep, grid, kSweepThreads, 0, a);
     long G = ghost_total(c->L);
-    PARIS_LAUNCH(c, k_vof_ghosts, div_up(G, 256), 256, 0, c->c2, c->flag, c->L, c->bnd, G, c->d.epsc);
+    PARIS_LAUNCH_N(c, "vof_ghosts", G, k_vof_ghosts, div_up(G, 256), 256, 0, c->c2, c->flag, c->L, c->bnd, G, c->d.epsc);
     double* t = c->fld[PARIS_FIELD_CVOF];
     c->fld[PARIS_FIELD_CVOF] = c->c2;
     c->c2 = t;
@@ -330,7 +330,7 @@ extern "C" int paris_linfunc(paris_handle_t c, int32_t which) {
     int mean = which == PARIS_FIELD_RHO ? c->d.dens_mean : c->d.visc_mean;
     int harm = mean == PARIS_MEAN_HARM;
     long tot = (long)(c->d.nx + 4) * (c->d.ny + 4) * (c->d.nz + 4);
-    PARIS_LAUNCH(c, k_linfunc, div_up(tot, 256), 256, 0, c->fld[PARIS_FIELD_CVOF], c->fld[which], c->L, a1, a2,
+    PARIS_LAUNCH_N(c, "linfunc", tot, k_linfunc, div_up(tot, 256), 256, 0, c->fld[PARIS_FIELD_CVOF], c->fld[which], c->L, a1, a2,
                  harm, c->d.nfilter > 0 ? 1 : 0);
     PARIS_CHECK(ctx_ghost_fill(c, c->fld[which]));
     return PARIS_OK;

@@ -93,6 +93,36 @@ class ParisGpu:
         self._check(self.lib.paris_gpu_download(self.h, field, _ptr(a)), "download")
         return a
 
+    def download_into(self, field, out):
+        """Download a real(8) field into a caller-owned (e.g. pinned) array."""
+        assert out.dtype == np.float64 and out.shape == self.shape and out.flags.c_contiguous
+        self._check(self.lib.paris_gpu_download(self.h, field, _ptr(out)), "download")
+
+    def upload_from(self, field, arr):
+        """Upload without a copy: arr must already be contiguous float64."""
+        assert arr.dtype == np.float64 and arr.shape == self.shape and arr.flags.c_contiguous
+        self._check(self.lib.paris_gpu_upload(self.h, field, _ptr(arr)), "upload")
+
+    def copy_field(self, dst, src):
+        self._check(self.lib.paris_gpu_copy_field(self.h, dst, src), "copy_field")
+
+    def fill_field(self, field, value):
+        self._check(self.lib.paris_gpu_fill_field(self.h, field, float(value)), "fill_field")
+
+    def profile(self, enable):
+        self._check(self.lib.paris_gpu_profile(self.h, 1 if enable else 0), "profile")
+
+    def profile_report(self):
+        """{kernel: (launches, total_ms, cells)} of the events recorded so far."""
+        need = self.lib.paris_gpu_profile_report(self.h, None, 0)
+        buf = ctypes.create_string_buffer(int(need) + 1)
+        self.lib.paris_gpu_profile_report(self.h, buf, len(buf))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, n, ms, cells = line.split("\t")
+            out[name] = (int(n), float(ms), float(cells))
+        return out
+
     def sync(self):
         self._check(self.lib.paris_gpu_sync(self.h), "sync")
 

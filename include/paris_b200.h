@@ -192,6 +192,21 @@ int paris_mg_test_err(paris_handle_t h, double* err);
 /* project_velocity, paris.f90:882-909 */
 int paris_project_velocity(paris_handle_t h, double dt);
 
+/* calcResiduals without any device allocation.  No counterpart in the
+ * reference: it serves callers that cannot allocate device memory, e.g. a
+ * driver whose device memory is all owned by its own pool or by another
+ * runtime, or one held to a fixed memory budget.  A_dev: A(is:ie,js:je,ks:ke,8)
+ * and p_dev: p(imin:imax,jmin:jmax,kmin:kmax) (ng ghost layers), both already
+ * on the current device in the reference layout; out3 (host) receives L1, L2,
+ * Linf as calcResiduals.  stream: a cudaStream_t or NULL.  Scratch is a fixed
+ * 1.5 MiB device array held by every GPU that loads the library: grids above
+ * 16,777,216 interior cells are rejected (PARIS_BAD_ARGS).  All calls share
+ * that array, so calls that overlap on the GPU race.  The first call on a
+ * device looks up the array's device address; make it before any stream
+ * capture. */
+int paris_calc_residuals_noalloc(int32_t nx, int32_t ny, int32_t nz, int32_t ng, const double* A_dev,
+                                 const double* p_dev, double* out3, void* stream);
+
 /* ---- projection adjoint (no counterpart in the reference: the transpose of
  *      SetupPoisson modules.f90:2735-2745 + solve + project_velocity
  *      paris.f90:898-909).  With u = u* - dt*B*G*p and A(B) p = -D u*,

@@ -25,6 +25,7 @@ SOURCES = {
     "solver.cu": True,
     "vof.cu": True,
     "stubs.cu": True,
+    "noalloc.cu": True,
 }
 
 

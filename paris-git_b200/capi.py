@@ -142,6 +142,7 @@ _PROTOS = {
     "paris_calc_residuals": (_I, [_P, _P]),
     "paris_mg_test_err": (_I, [_P, _P]),
     "paris_project_velocity": (_I, [_P, _D]),
+    "paris_calc_residuals_noalloc": (_I, [_I, _I, _I, _I, _P, _P, _P, _P]),
     "paris_projection_adjoint": (_I, [_P, _D, _P, _P, _P, _P, _P, _P, _P, _P, _P,
                                       ctypes.POINTER(SolveOpts)]),
 }

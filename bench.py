@@ -40,7 +40,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=256, help="cells per direction of the workload")
-    ap.add_argument("--pcg", type=int, default=0, help="1: V-cycle preconditioned CG outer loop")
+    ap.add_argument("--pcg", type=int, default=1, help="1: FP64 flexible CG preconditioned by the V-cycle, 0: defect correction")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="a few profiled steps, no JSON timing")
@@ -340,9 +340,9 @@ def run_b200(args, dist):
         gpu.close()
         return 0
 
-    def timed(mode, steps, k0):
+    def timed(mode, steps, k0, pcg=args.pcg):
         for k in range(args.warmup):
-            gpu_step(gpu, capi, k0 + k, dt, mode, args.pcg)
+            gpu_step(gpu, capi, k0 + k, dt, mode, pcg)
         gpu.sync()
         dist.barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -350,7 +350,7 @@ def run_b200(args, dist):
         l0 = gpu.launch_count()
         e0.record(stream)
         for k in range(steps):
-            r = gpu_step(gpu, capi, k0 + args.warmup + k, dt, mode, args.pcg)
+            r = gpu_step(gpu, capi, k0 + args.warmup + k, dt, mode, pcg)
             its.append(r.it)
         e1.record(stream)
         e1.synchronize()
@@ -365,6 +365,7 @@ def run_b200(args, dist):
     ms, its, launches = timed(capi.MG_MIXED, args.steps, 0)
     clk = clocks.stop()
     ms64, its64, _ = timed(capi.MG_FP64, args.steps, 1000)
+    msdc, itsdc, _ = timed(capi.MG_MIXED, args.steps, 4000, pcg=1 - args.pcg)
 
     # per-kernel CUDA-event profile of the same step (separate, after timing)
     gpu.profile(True)
@@ -422,11 +423,12 @@ def run_b200(args, dist):
         "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
         "config": {"workload": f"{n}^3 periodic unit cube, 64 drops r~U[0.03,0.08] (seed 0), rho 1000/1, "
                                "smoothed Gaussian u* (seed 1), CIAM VOF + B200 MG to ||r||/||b|| < 1e-10 from p=0",
-                   "cells": n ** 3, "solver": ("mixed FP32 V(2,2) in FP64 " + ("PCG" if args.pcg else
-                                                                                 "defect correction")),
+                   "cells": n ** 3, "solver": ("FP32 red-black V(2,2) cycles in an FP64 " +
+                                              ("flexible-CG (preconditioner) loop" if args.pcg else "defect-correction loop")),
                    "parallelism": f"replicas x{dist.world}", "l2": "inputs larger than L2 (141 MB per field)"},
         "fp64_steps_per_s": dist.world * args.steps / (ms64 / 1e3),
-        "mg_iterations": {"mixed": its, "fp64": its64},
+        ("mixed_dc_steps_per_s" if args.pcg else "mixed_pcg_steps_per_s"): dist.world * args.steps / (msdc / 1e3),
+        "mg_iterations": {"mixed": its, "fp64": its64, ("mixed_dc" if args.pcg else "mixed_pcg"): itsdc},
         "mcell_updates_per_s": value * n ** 3 / 1e6,
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": top["kernel"], "achieved": top["gbs"], "peak": peak,

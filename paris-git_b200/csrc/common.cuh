@@ -7,32 +7,28 @@
 #include "../../include/paris_b200.h"
 
 // ---------------------------------------------------------------------------
-// Field layout in HBM.  A field with ghost layers keeps the reference's shape
-// (Nx+2Ng)(Ny+2Ng)(Nz+2Ng), i fastest, but each x-row is padded so that the
-// first interior cell of every row sits on a 128-byte boundary:
-//   row  = [pad | Ng ghosts | Nx interior | Ng ghosts | pad]
+// Field layout in HBM: exactly the reference's array
+// F(imin:imax,jmin:jmax,kmin:kmax) with Ng ghost layers, i fastest, so a
+// Fortran array moves to and from the device as one contiguous copy.
 //   elem(i,j,k) = base[off + i + pitch*j + plane*k], i,j,k interior-relative
 //   (-Ng .. N+Ng-1).
 // ---------------------------------------------------------------------------
 struct Layout {
     int n[3];      // interior cells
     int ng;
-    long pitch;    // elements per row
+    long pitch;    // elements per row (Nx + 2 Ng)
     long plane;    // elements per plane
     long off;      // offset of interior (0,0,0)
-    long total;    // elements to allocate
+    long total;    // elements of the array
 };
-
-static constexpr int kRowLead = 16;   // elements before interior i = 0
 
 inline Layout make_layout(int nx, int ny, int nz, int ng) {
     Layout L;
     L.n[0] = nx; L.n[1] = ny; L.n[2] = nz; L.ng = ng;
-    long need = kRowLead + nx + ng;
-    L.pitch = (need + 15) / 16 * 16;
+    L.pitch = nx + 2 * ng;
     L.plane = L.pitch * (ny + 2 * ng);
-    L.off = kRowLead + L.pitch * ng + L.plane * ng;
-    L.total = L.plane * (nz + 2 * ng) + 16;
+    L.off = ng + L.pitch * ng + L.plane * ng;
+    L.total = L.plane * (nz + 2 * ng);
     return L;
 }
 
@@ -102,10 +98,13 @@ int prof_enabled(const paris_ctx* c);
 inline unsigned div_up(long a, long b) { return (unsigned)((a + b - 1) / b); }
 
 // Deterministic block reduction of a double (fixed tree order).
+__device__ inline int linear_tid() { return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z); }
+
 template <int BLOCK>
 __device__ inline double block_sum(double v, double* sh) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int tid = linear_tid();
+    int lane = tid & 31, w = tid >> 5;
     if (lane == 0) sh[w] = v;
     __syncthreads();
     v = 0.0;
@@ -114,13 +113,14 @@ __device__ inline double block_sum(double v, double* sh) {
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     }
     __syncthreads();
-    return v;   // valid in thread 0
+    return v;   // valid in the first thread
 }
 
 template <int BLOCK>
 __device__ inline double block_max(double v, double* sh) {
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int tid = linear_tid();
+    int lane = tid & 31, w = tid >> 5;
     if (lane == 0) sh[w] = v;
     __syncthreads();
     v = 0.0;
@@ -131,3 +131,16 @@ __device__ inline double block_max(double v, double* sh) {
     __syncthreads();
     return v;
 }
+
+// Loops over the interior cells of an n0 x n1 x n2 box with blocks of
+// (bx, by) threads: threadIdx.x runs along i, (blockIdx.x, threadIdx.y) over
+// the rows (j,k) with a grid stride; no 64-bit divisions per cell.
+#define ROWS_BEGIN(n0, n1, n2)                                                             \
+    for (int _row = blockIdx.x * blockDim.y + threadIdx.y; _row < (n1) * (n2);             \
+         _row += gridDim.x * blockDim.y) {                                                 \
+        const int j = _row % (n1), k = _row / (n1);                                        \
+        for (int i = threadIdx.x; i < (n0); i += blockDim.x) {
+#define ROWS_END \
+        }        \
+    }
+static const dim3 kRowBlock(128, 2, 1);

@@ -129,11 +129,11 @@ int ctx_ghost_fill_i8(paris_ctx* c, int8_t* f) {
 
 // ---- reductions -----------------------------------------------------------
 // Kernels write kRedBlocks partials per slot; this sums them in a fixed order.
-__global__ void k_reduce_slots(const double* __restrict__ part, double* out, int op_max) {
+__global__ void k_reduce_slots(const double* __restrict__ part, double* out, int op_max, int nb) {
     __shared__ double sh[32];
     int slot = blockIdx.x;
     double v = 0.0;
-    for (int b = threadIdx.x; b < kRedBlocks; b += blockDim.x) {
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
         double x = part[(long)slot * kRedBlocks + b];
         v = op_max ? fmax(v, x) : v + x;
     }
@@ -142,7 +142,7 @@ __global__ void k_reduce_slots(const double* __restrict__ part, double* out, int
 }
 
 int ctx_reduce_finish(paris_ctx* c, int nslots, double* out_host, int op_max) {
-    PARIS_LAUNCH(c, k_reduce_slots, nslots, 256, 0, c->red_part, c->red_out, op_max);
+    PARIS_LAUNCH(c, k_reduce_slots, nslots, 256, 0, c->red_part, c->red_out, op_max, c->red_nb);
     PARIS_CUDA_TRY(c, cudaMemcpyAsync(c->red_host, c->red_out, nslots * sizeof(double),
                                       cudaMemcpyDeviceToHost, c->stream));
     PARIS_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -208,6 +208,7 @@ extern "C" int paris_gpu_init(const paris_grid_desc* desc, paris_handle_t* out) 
     if (c->d.epsc <= 0.0) c->d.epsc = 1e-12;
     if (c->d.nrelax <= 0) c->d.nrelax = 3;
     c->dev = desc->device;
+    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev);
     if (cudaSetDevice(c->dev) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
         return PARIS_CUDA_ERROR;
@@ -263,7 +264,8 @@ extern "C" int paris_gpu_finalize(paris_handle_t c) {
                     (void*)c->xc, (void*)c->yc, (void*)c->zc, (void*)c->c2, (void*)c->flag, (void*)c->cg,
                     (void*)c->height, (void*)c->i32stage, (void*)c->cx, (void*)c->cy, (void*)c->cz,
                     (void*)c->rhs, (void*)c->A, (void*)c->red_part, (void*)c->red_out, (void*)c->fast_r64,
-                    (void*)c->fast_d64, (void*)c->fast_q64, (void*)c->fast_z64, (void*)c->fast_zold64})
+                    (void*)c->fast_d64, (void*)c->fast_q64, (void*)c->fast_z64, (void*)c->fast_zold64,
+                    (void*)c->vflux, (void*)c->mixlist, (void*)c->mixcount})
         free_ptr(p);
     for (auto& l : c->ref) { free_ptr(l.K); free_ptr(l.p); free_ptr(l.e); }
     for (auto& l : c->fl32) { free_ptr(l.cx); free_ptr(l.cy); free_ptr(l.cz); free_ptr(l.b); free_ptr(l.x); }
@@ -287,23 +289,13 @@ static long ghosted_cells(const paris_ctx* c) {
     return (long)(c->d.nx + 2 * c->d.ng) * (c->d.ny + 2 * c->d.ng) * (c->d.nz + 2 * c->d.ng);
 }
 
-// device pointer of the first element (ghost corner) of a ghosted field
-template <typename T>
-static T* corner(const paris_ctx* c, T* base) {
-    return base + (c->L.off - c->L.ng - c->L.pitch * c->L.ng - c->L.plane * c->L.ng);
-}
-
+// one contiguous copy: the device array has the Fortran layout
 int copy_ghosted(paris_ctx* c, double* dev, const double* host, bool to_dev) {
-    const int g = c->d.ng;
-    size_t w = (size_t)(c->d.nx + 2 * g) * sizeof(double);
-    size_t rows = (size_t)(c->d.ny + 2 * g) * (c->d.nz + 2 * g);
-    double* d0 = corner(c, dev);
+    size_t bytes = (size_t)c->L.total * sizeof(double);
     if (to_dev)
-        PARIS_CUDA_TRY(c, cudaMemcpy2DAsync(d0, c->L.pitch * sizeof(double), host, w, w, rows,
-                                            cudaMemcpyHostToDevice, c->stream));
+        PARIS_CUDA_TRY(c, cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, c->stream));
     else
-        PARIS_CUDA_TRY(c, cudaMemcpy2DAsync((void*)host, w, d0, c->L.pitch * sizeof(double), w, rows,
-                                            cudaMemcpyDeviceToHost, c->stream));
+        PARIS_CUDA_TRY(c, cudaMemcpyAsync((void*)host, dev, bytes, cudaMemcpyDeviceToHost, c->stream));
     return PARIS_OK;
 }
 

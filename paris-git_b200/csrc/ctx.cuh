@@ -4,6 +4,8 @@
 #include <vector>
 #include "common.cuh"
 
+static constexpr int kRedBlocks = 1184;   // 148 SMs x 8: capacity of the partial-sum slots
+
 // One level of the reference multigrid (DataMG/pMG/EMG of MGsolver.f90:26-30),
 // interior-only arrays; the one-layer halo is resolved in the kernels
 // (periodic wrap, zero at walls where ghost_MG_* never writes).
@@ -42,6 +44,9 @@ struct paris_ctx {
     double* c2 = nullptr;          // second cvof buffer of the sweeps
     int8_t* flag = nullptr;        // vof_flag (ghosted)
     uint8_t* cg = nullptr;         // c_mask of the Weymouth-Yue sweeps
+    double* vflux = nullptr;       // vof1/vof2/vof3 of the mixed cells (3 ghosted arrays)
+    long* mixlist = nullptr;       // mixed flux cells of the current sweep
+    int* mixcount = nullptr;
     double* height = nullptr;      // 6 ghosted fields
     int32_t* i32stage = nullptr;   // staging for int32 host transfers
     // pressure equation, compact interior arrays (N each)
@@ -55,6 +60,9 @@ struct paris_ctx {
     double* red_part = nullptr;    // kRedBlocks partials * 4 slots
     double* red_out = nullptr;     // device scalars
     double* red_host = nullptr;    // pinned
+    int red_nb = kRedBlocks;       // blocks of the last reduction launch
+    int nsm = 148;
+    std::vector<std::pair<const void*, int>> red_occ;   // kernel -> resident blocks per SM
     // multigrid hierarchies
     int ref_lmg = 0;
     std::vector<RefLevel> ref;     // index 1..LMG
@@ -79,7 +87,24 @@ struct paris_ctx {
     std::vector<cudaEvent_t> evpool;
 };
 
-static constexpr int kRedBlocks = 1184;   // 148 SMs x 8
+
+// Grid of a reduction kernel: one wave of resident blocks (at most
+// kRedBlocks); records the block count for ctx_reduce_finish.
+template <typename K>
+unsigned red_grid(paris_ctx* c, K kernel, int threads) {
+    const void* key = (const void*)kernel;
+    int per = 0;
+    for (auto& e : c->red_occ)
+        if (e.first == key) per = e.second;
+    if (!per) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0) != cudaSuccess || per < 1) per = 1;
+        c->red_occ.push_back({key, per});
+    }
+    int g = per * c->nsm;
+    if (g > kRedBlocks) g = kRedBlocks;
+    c->red_nb = g;
+    return (unsigned)g;
+}
 
 // internal API (ctx.cu)
 int ctx_alloc_field(paris_ctx* c, int field);

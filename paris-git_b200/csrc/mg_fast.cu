@@ -82,31 +82,28 @@ __device__ inline void restrict_cell(const LV<T>& f, const LV<T>& c, const Bnd& 
     c.b[cidx(c.n0, c.n1, i, j, k)] = (T)0.125 * s;
 }
 
+// grid (ceil(n/128), n1, n2), block 128: one thread per cell of the colour
 template <typename T>
 __global__ void k_fast_smooth(const LV<T> v, const Bnd B, int color) {
-    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    int h0 = (v.n0 + 1) >> 1;
-    if (t >= (long)h0 * v.n1 * v.n2) return;
-    int ih = (int)(t % h0), j = (int)((t / h0) % v.n1), k = (int)(t / ((long)h0 * v.n1));
+    int ih = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
     int i = 2 * ih + ((j + k + color) & 1);
     if (i < v.n0) smooth_cell(v, B, i, j, k);
 }
 
 template <typename T>
 __global__ void k_fast_restrict(const LV<T> f, const LV<T> c, const Bnd B) {
-    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (t >= c.N) return;
-    int i = (int)(t % c.n0), j = (int)((t / c.n0) % c.n1), k = (int)(t / ((long)c.n0 * c.n1));
-    restrict_cell(f, c, B, i, j, k);
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i < c.n0) restrict_cell(f, c, B, i, j, k);
 }
 
 template <typename T>
 __global__ void k_fast_prolong(const LV<T> f, const LV<T> c) {
-    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (t >= f.N) return;
-    int i = (int)(t % f.n0), j = (int)((t / f.n0) % f.n1), k = (int)(t / ((long)f.n0 * f.n1));
-    f.x[t] += c.x[cidx(c.n0, c.n1, i >> 1, j >> 1, k >> 1)];
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= f.n0) return;
+    f.x[cidx(f.n0, f.n1, i, j, k)] += c.x[cidx(c.n0, c.n1, i >> 1, j >> 1, k >> 1)];
 }
+
+static inline dim3 row_grid(long n0, int n1, int n2) { return dim3(div_up(n0, 128), n1, n2); }
 
 // The V-cycle from level L0 down to the coarsest, in one block.
 template <typename T>
@@ -209,9 +206,8 @@ __global__ void k_fast_residual64(const Mat64 A, const double* __restrict__ p, c
                                   T* __restrict__ rT, double* __restrict__ r64, double* part) {
     __shared__ double sh[32];
     double s2 = 0.0, s1 = 0.0, sb = 0.0;
-    long N = (long)L.n[0] * L.n[1] * L.n[2];
-    for (long m = blockIdx.x * (long)blockDim.x + threadIdx.x; m < N; m += (long)gridDim.x * blockDim.x) {
-        int i = (int)(m % L.n[0]), j = (int)((m / L.n[0]) % L.n[1]), k = (int)(m / ((long)L.n[0] * L.n[1]));
+    ROWS_BEGIN(L.n[0], L.n[1], L.n[2])
+        long m = cidx(L.n[0], L.n[1], i, j, k);
         double a1 = i > 0 ? A.cx[m - 1] : (B.per[0] ? A.cx[m + L.n[0] - 1] : 0.0);
         double a3 = j > 0 ? A.cy[m - L.n[0]] : (B.per[1] ? A.cy[m + (long)L.n[0] * (L.n[1] - 1)] : 0.0);
         long sz = (long)L.n[0] * L.n[1];
@@ -228,11 +224,11 @@ __global__ void k_fast_residual64(const Mat64 A, const double* __restrict__ p, c
         s2 += r * r;
         s1 += fabs(r);
         sb += b * b;
-    }
+    ROWS_END
     s2 = block_sum<256>(s2, sh);
     s1 = block_sum<256>(s1, sh);
     sb = block_sum<256>(sb, sh);
-    if (threadIdx.x == 0) {
+    if (linear_tid() == 0) {
         part[blockIdx.x] = s2;
         part[kRedBlocks + blockIdx.x] = s1;
         part[2 * kRedBlocks + blockIdx.x] = sb;
@@ -242,12 +238,10 @@ __global__ void k_fast_residual64(const Mat64 A, const double* __restrict__ p, c
 // p += x (the level-0 correction) on the ghosted field
 template <typename T>
 __global__ void k_fast_correct(double* __restrict__ p, const T* __restrict__ x, const Layout L, double alpha) {
-    long m = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    long N = (long)L.n[0] * L.n[1] * L.n[2];
-    if (m >= N) return;
-    int i = (int)(m % L.n[0]), j = (int)((m / L.n[0]) % L.n[1]), k = (int)(m / ((long)L.n[0] * L.n[1]));
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= L.n[0]) return;
     long n = lidx(L, i, j, k);
-    p[n] = p[n] + alpha * (double)x[m];
+    p[n] = p[n] + alpha * (double)x[cidx(L.n[0], L.n[1], i, j, k)];
 }
 
 // ---- PCG helpers (FP64 compact vectors) --------------------------------------
@@ -256,15 +250,14 @@ __global__ void k_pcg_matvec(const Mat64 A, const double* __restrict__ d, double
                              const Bnd B, double* part) {
     __shared__ double sh[32];
     double s = 0.0;
-    long N = (long)L.n[0] * L.n[1] * L.n[2];
-    for (long m = blockIdx.x * (long)blockDim.x + threadIdx.x; m < N; m += (long)gridDim.x * blockDim.x) {
-        int i = (int)(m % L.n[0]), j = (int)((m / L.n[0]) % L.n[1]), k = (int)(m / ((long)L.n[0] * L.n[1]));
+    ROWS_BEGIN(L.n[0], L.n[1], L.n[2])
+        long m = cidx(L.n[0], L.n[1], i, j, k);
         double v = ax_compact(A, d, L, B, i, j, k, m);
         q[m] = v;
         s += d[m] * v;
-    }
+    ROWS_END
     s = block_sum<256>(s, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = s;
+    if (linear_tid() == 0) part[blockIdx.x] = s;
 }
 
 // p += alpha d (ghosted p), r -= alpha q ; slots 0 = r.r, 1 = sum |r|
@@ -272,19 +265,18 @@ __global__ void k_pcg_update(double* __restrict__ p, double* __restrict__ r, con
                              const double* __restrict__ q, double alpha, const Layout L, double* part) {
     __shared__ double sh[32];
     double s2 = 0.0, s1 = 0.0;
-    long N = (long)L.n[0] * L.n[1] * L.n[2];
-    for (long m = blockIdx.x * (long)blockDim.x + threadIdx.x; m < N; m += (long)gridDim.x * blockDim.x) {
-        int i = (int)(m % L.n[0]), j = (int)((m / L.n[0]) % L.n[1]), k = (int)(m / ((long)L.n[0] * L.n[1]));
+    ROWS_BEGIN(L.n[0], L.n[1], L.n[2])
+        long m = cidx(L.n[0], L.n[1], i, j, k);
         long n = lidx(L, i, j, k);
         p[n] = p[n] + alpha * d[m];
         double rr = r[m] - alpha * q[m];
         r[m] = rr;
         s2 += rr * rr;
         s1 += fabs(rr);
-    }
+    ROWS_END
     s2 = block_sum<256>(s2, sh);
     s1 = block_sum<256>(s1, sh);
-    if (threadIdx.x == 0) {
+    if (linear_tid() == 0) {
         part[blockIdx.x] = s2;
         part[kRedBlocks + blockIdx.x] = s1;
     }
@@ -411,13 +403,12 @@ static int vcycle(paris_ctx* c, int nu1, int nu2) {
     if (Lc > 0) PARIS_CUDA_TRY(c, cudaMemsetAsync(lv[0].x, 0, lv[0].N * sizeof(T), c->stream));
     for (int L = 0; L < Lc; L++) {
         LV<T> v = view(lv[L]);
-        long nh = (long)((v.n0 + 1) / 2) * v.n1 * v.n2;
         for (int s = 0; s < nu1; s++) {
-            PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, div_up(nh, 256), 256, 0, v, c->bnd, 0);
-            PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, div_up(nh, 256), 256, 0, v, c->bnd, 1);
+            PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, row_grid((v.n0 + 1) / 2, v.n1, v.n2), 128, 0, v, c->bnd, 0);
+            PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, row_grid((v.n0 + 1) / 2, v.n1, v.n2), 128, 0, v, c->bnd, 1);
         }
         LV<T> cv = view(lv[L + 1]);
-        PARIS_LAUNCH_N(c, kname<T>("mg_restrict"), v.N, k_fast_restrict<T>, div_up(cv.N, 256), 256, 0, v, cv, c->bnd);
+        PARIS_LAUNCH_N(c, kname<T>("mg_restrict"), v.N, k_fast_restrict<T>, row_grid(cv.n0, cv.n1, cv.n2), 128, 0, v, cv, c->bnd);
         if (L + 1 < Lc) PARIS_CUDA_TRY(c, cudaMemsetAsync(lv[L + 1].x, 0, lv[L + 1].N * sizeof(T), c->stream));
     }
     LVSet<T> S;
@@ -425,11 +416,10 @@ static int vcycle(paris_ctx* c, int nu1, int nu2) {
     PARIS_LAUNCH_N(c, kname<T>("mg_coarse_cycle"), lv[Lc].N, k_fast_coarse_cycle<T>, 1, 1024, 0, S, Lc, nl, c->bnd, nu1, nu2);
     for (int L = Lc - 1; L >= 0; L--) {
         LV<T> v = view(lv[L]);
-        PARIS_LAUNCH_N(c, kname<T>("mg_prolong"), v.N, k_fast_prolong<T>, div_up(v.N, 256), 256, 0, v, view(lv[L + 1]));
-        long nh = (long)((v.n0 + 1) / 2) * v.n1 * v.n2;
+        PARIS_LAUNCH_N(c, kname<T>("mg_prolong"), v.N, k_fast_prolong<T>, row_grid(v.n0, v.n1, v.n2), 128, 0, v, view(lv[L + 1]));
         for (int s = 0; s < nu2; s++) {
-            PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, div_up(nh, 256), 256, 0, v, c->bnd, 1);
-            PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, div_up(nh, 256), 256, 0, v, c->bnd, 0);
+            PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, row_grid((v.n0 + 1) / 2, v.n1, v.n2), 128, 0, v, c->bnd, 1);
+            PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, row_grid((v.n0 + 1) / 2, v.n1, v.n2), 128, 0, v, c->bnd, 0);
         }
     }
     return PARIS_OK;
@@ -449,7 +439,7 @@ static int solve_dc(paris_ctx* c, const paris_solve_opts* o, paris_solve_result*
     Mat64 A{c->cx, c->cy, c->cz, c->rhs};
     double* p = c->fld[PARIS_FIELD_P];
     double s[3], tres, rel;
-    PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>, kRedBlocks, 256, 0, A, p, c->L, c->bnd, lv[0].b, (double*)nullptr,
+    PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>, red_grid(c, k_fast_residual64<T>, 256), kRowBlock, 0, A, p, c->L, c->bnd, lv[0].b, (double*)nullptr,
                  c->red_part);
     PARIS_CHECK(ctx_reduce_finish(c, 3, s));
     double bn2 = s[2];
@@ -459,8 +449,8 @@ static int solve_dc(paris_ctx* c, const paris_solve_opts* o, paris_solve_result*
     int nu1 = o->nu1 > 0 ? o->nu1 : 2, nu2 = o->nu2 > 0 ? o->nu2 : 2;
     while (!done && it < o->maxit) {
         PARIS_CHECK(vcycle<T>(c, nu1, nu2));
-        PARIS_LAUNCH_N(c, kname<T>("mg_correct"), c->N, k_fast_correct<T>, div_up(c->N, 256), 256, 0, p, lv[0].x, c->L, 1.0);
-        PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>, kRedBlocks, 256, 0, A, p, c->L, c->bnd, lv[0].b, (double*)nullptr,
+        PARIS_LAUNCH_N(c, kname<T>("mg_correct"), c->N, k_fast_correct<T>, row_grid(c->d.nx, c->d.ny, c->d.nz), 128, 0, p, lv[0].x, c->L, 1.0);
+        PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>, red_grid(c, k_fast_residual64<T>, 256), kRowBlock, 0, A, p, c->L, c->bnd, lv[0].b, (double*)nullptr,
                      c->red_part);
         PARIS_CHECK(ctx_reduce_finish(c, 3, s));
         it++;
@@ -487,7 +477,7 @@ static int precondition(paris_ctx* c, int nu1, int nu2, double* rz, double* rzol
     auto& lv = levels<T>(c);
     PARIS_LAUNCH(c, k_to_T<T>, div_up(c->N, 256), 256, 0, c->fast_r64, lv[0].b, c->N);
     PARIS_CHECK(vcycle<T>(c, nu1, nu2));
-    PARIS_LAUNCH(c, k_pcg_takez<T>, kRedBlocks, 256, 0, lv[0].x, c->fast_z64, c->fast_zold64, c->fast_r64, c->N,
+    PARIS_LAUNCH(c, k_pcg_takez<T>, red_grid(c, k_pcg_takez<T>, 256), 256, 0, lv[0].x, c->fast_z64, c->fast_zold64, c->fast_r64, c->N,
                  c->red_part);
     double s[2];
     PARIS_CHECK(ctx_reduce_finish(c, 2, s));
@@ -503,7 +493,7 @@ static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result
     Mat64 A{c->cx, c->cy, c->cz, c->rhs};
     double* p = c->fld[PARIS_FIELD_P];
     double s[3], tres, rel;
-    PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>, kRedBlocks, 256, 0, A, p, c->L, c->bnd, (T*)nullptr, c->fast_r64,
+    PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>, red_grid(c, k_fast_residual64<T>, 256), kRowBlock, 0, A, p, c->L, c->bnd, (T*)nullptr, c->fast_r64,
                  c->red_part);
     PARIS_CHECK(ctx_reduce_finish(c, 3, s));
     double bn2 = s[2];
@@ -520,11 +510,11 @@ static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result
     }
     while (!done && it < o->maxit) {
         double dq;
-        PARIS_LAUNCH(c, k_pcg_matvec, kRedBlocks, 256, 0, A, c->fast_d64, c->fast_q64, c->L, c->bnd, c->red_part);
+        PARIS_LAUNCH_N(c, "pcg_matvec_fp64", c->N, k_pcg_matvec, red_grid(c, k_pcg_matvec, 256), kRowBlock, 0, A, c->fast_d64, c->fast_q64, c->L, c->bnd, c->red_part);
         PARIS_CHECK(ctx_reduce_finish(c, 1, &dq));
         if (!(dq > 0.0)) break;
         double alpha = rz / dq;
-        PARIS_LAUNCH(c, k_pcg_update, kRedBlocks, 256, 0, p, c->fast_r64, c->fast_d64, c->fast_q64, alpha, c->L,
+        PARIS_LAUNCH_N(c, "pcg_update_fp64", c->N, k_pcg_update, red_grid(c, k_pcg_update, 256), kRowBlock, 0, p, c->fast_r64, c->fast_d64, c->fast_q64, alpha, c->L,
                      c->red_part);
         PARIS_CHECK(ctx_reduce_finish(c, 2, s));
         it++;

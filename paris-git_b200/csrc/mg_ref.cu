@@ -235,7 +235,7 @@ int mg_ref_solve(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* re
                      c->ref[L].K, dims(c->ref[L]));
     double* p = c->fld[PARIS_FIELD_P];
     PARIS_LAUNCH(c, k_ref_field_io, div_up(lf.N, 256), 256, 0, p, lf.p, c->L, 0);
-    PARIS_LAUNCH(c, k_ref_get_residual, kRedBlocks, 256, 0, lf.K, lf.p, dims(lf), c->bnd, o->norm, c->red_part);
+    PARIS_LAUNCH(c, k_ref_get_residual, red_grid(c, k_ref_get_residual, 256), 256, 0, lf.K, lf.p, dims(lf), c->bnd, o->norm, c->red_part);
     double s;
     PARIS_CHECK(ctx_reduce_finish(c, 1, &s));
     double nxyz = (double)c->d.nx * (double)c->d.ny * (double)c->d.nz;
@@ -248,7 +248,7 @@ int mg_ref_solve(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* re
         PARIS_CHECK(mg_iteration(c, o->beta, nrelax, c->d.sym_mg));
         PARIS_LAUNCH(c, k_ref_field_io, div_up(lf.N, 256), 256, 0, p, lf.p, c->L, 1);
         PARIS_CHECK(ctx_ghost_fill(c, p));
-        PARIS_LAUNCH(c, k_ref_compute_residual, kRedBlocks, 256, 0, c->A, p, c->L, o->norm, c->red_part);
+        PARIS_LAUNCH(c, k_ref_compute_residual, red_grid(c, k_ref_compute_residual, 256), 256, 0, c->A, p, c->L, o->norm, c->red_part);
         PARIS_CHECK(ctx_reduce_finish(c, 1, &s));
         tres2 = s / nxyz;
         if (o->norm == 2) tres2 = sqrt(tres2);

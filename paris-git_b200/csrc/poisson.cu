@@ -43,9 +43,8 @@ __global__ void k_setup_poisson(const double* __restrict__ u, const double* __re
     __shared__ double sh[32];
     double s_rhs = 0.0, s_bad = 0.0;
     const int g = L.ng;
-    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < (long)L.n[0] * L.n[1] * L.n[2];
-         t += (long)gridDim.x * blockDim.x) {
-        int i = (int)(t % L.n[0]), j = (int)((t / L.n[0]) % L.n[1]), k = (int)(t / ((long)L.n[0] * L.n[1]));
+    ROWS_BEGIN(L.n[0], L.n[1], L.n[2])
+        long t = cidx(L.n[0], L.n[1], i, j, k);
         long n = lidx(L, i, j, k);
         double r0 = rho[n];
         double a1 = 2.0 * dt * face_mask(B, L, 0, i - 1) / (M.dx[i + g] * M.dxh[i - 1 + g] * (rho[n - 1] + r0));
@@ -62,10 +61,10 @@ __global__ void k_setup_poisson(const double* __restrict__ u, const double* __re
         if (a7 < 1e-50) bad = true;   // no solid cells on this grid: A7 tiny is an error
         s_rhs += a8;
         s_bad += bad ? 1.0 : 0.0;
-    }
+    ROWS_END
     s_rhs = block_sum<256>(s_rhs, sh);
     s_bad = block_sum<256>(s_bad, sh);
-    if (threadIdx.x == 0) {
+    if (linear_tid() == 0) {
         part[blockIdx.x] = s_rhs;
         part[kRedBlocks + blockIdx.x] = s_bad;
     }
@@ -117,7 +116,7 @@ extern "C" int paris_setup_poisson(paris_handle_t c, double dt, double volume_so
     if (!(dt > 0.0)) return PARIS_BAD_ARGS;
     cudaSetDevice(c->dev);
     PARIS_CHECK(ctx_ensure_matrix(c));
-    PARIS_LAUNCH_N(c, "setup_poisson", c->N, k_setup_poisson, kRedBlocks, 256, 0, c->fld[PARIS_FIELD_U], c->fld[PARIS_FIELD_V],
+    PARIS_LAUNCH_N(c, "setup_poisson", c->N, k_setup_poisson, red_grid(c, k_setup_poisson, 256), kRowBlock, 0, c->fld[PARIS_FIELD_U], c->fld[PARIS_FIELD_V],
                  c->fld[PARIS_FIELD_W], c->fld[PARIS_FIELD_RHO], c->cx, c->cy, c->cz, c->rhs, c->L, c->bnd,
                  metric(c), dt, volume_source, c->red_part);
     double out[2];
@@ -174,8 +173,8 @@ __global__ void k_calc_residuals(const double* __restrict__ A, const double* __r
     __shared__ double sh[32];
     long N = (long)L.n[0] * L.n[1] * L.n[2];
     double s1 = 0.0, s2 = 0.0, smax = 0.0;
-    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < N; t += (long)gridDim.x * blockDim.x) {
-        int i = (int)(t % L.n[0]), j = (int)((t / L.n[0]) % L.n[1]), k = (int)(t / ((long)L.n[0] * L.n[1]));
+    ROWS_BEGIN(L.n[0], L.n[1], L.n[2])
+        long t = cidx(L.n[0], L.n[1], i, j, k);
         long n = lidx(L, i, j, k);
         double r = fabs(-p[n] * A[6 * N + t] + A[0 * N + t] * p[n - 1] + A[1 * N + t] * p[n + 1] +
                         A[2 * N + t] * p[n - L.pitch] + A[3 * N + t] * p[n + L.pitch] +
@@ -183,11 +182,11 @@ __global__ void k_calc_residuals(const double* __restrict__ A, const double* __r
         s1 += r;
         s2 += r * r;
         smax = fmax(smax, r);
-    }
+    ROWS_END
     s1 = block_sum<256>(s1, sh);
     s2 = block_sum<256>(s2, sh);
     smax = block_max<256>(smax, sh);
-    if (threadIdx.x == 0) {
+    if (linear_tid() == 0) {
         part[blockIdx.x] = s1;
         part[kRedBlocks + blockIdx.x] = s2;
         part[2 * kRedBlocks + blockIdx.x] = smax;
@@ -198,7 +197,7 @@ extern "C" int paris_calc_residuals(paris_handle_t c, double* out3) {
     if (!c || !out3 || !c->have_matrix) return PARIS_BAD_ARGS;
     cudaSetDevice(c->dev);
     if (!c->A_valid) PARIS_CHECK(poisson_build_full_A(c));
-    PARIS_LAUNCH(c, k_calc_residuals, kRedBlocks, 256, 0, c->A, c->fld[PARIS_FIELD_P], c->L, c->red_part);
+    PARIS_LAUNCH(c, k_calc_residuals, red_grid(c, k_calc_residuals, 256), kRowBlock, 0, c->A, c->fld[PARIS_FIELD_P], c->L, c->red_part);
     double s[2], mx[1];
     PARIS_CHECK(ctx_reduce_finish(c, 2, s));
     // the max slot is reduced separately
@@ -237,7 +236,7 @@ __global__ void k_mgtest_err(const double* __restrict__ p, const Layout L, const
 extern "C" int paris_mg_test_err(paris_handle_t c, double* err) {
     if (!c || !err) return PARIS_BAD_ARGS;
     cudaSetDevice(c->dev);
-    PARIS_LAUNCH(c, k_mgtest_err, kRedBlocks, 256, 0, c->fld[PARIS_FIELD_P], c->L, c->xc, c->yc, c->zc, c->red_part);
+    PARIS_LAUNCH(c, k_mgtest_err, red_grid(c, k_mgtest_err, 256), 256, 0, c->fld[PARIS_FIELD_P], c->L, c->xc, c->yc, c->zc, c->red_part);
     double s[2];
     PARIS_CHECK(ctx_reduce_finish(c, 2, s));
     *err = s[0] / s[1];

@@ -15,15 +15,16 @@
 #include "ctx.cuh"
 #include "plic.cuh"
 
-static constexpr int kSweepThreads = 256;
-static constexpr int kMaxFlux = 320;    // (32+2)*8 or 32*(8+2)
-
 struct SweepArgs {
     const double* c;     // old cvof (ghosted)
     double* cn;          // new cvof (ghosted)
     int8_t* flag;        // new flags
     const double* us;    // face velocity of the sweep direction
     const uint8_t* cg;   // c_mask (WY)
+    double *v1, *v2, *v3;   // fluxes of the mixed cells (ghosted arrays, sparse)
+    long* list;          // layout indices of the mixed flux cells
+    int* count;
+    long cap;
     Layout L;
     int d;               // 0,1,2
     int wy;              // 1: swpr
@@ -31,73 +32,61 @@ struct SweepArgs {
     double epsc;
 };
 
-// tile shape (cells) of a sweep along d
-__host__ __device__ inline void tile_shape(int d, int& tx, int& ty, int& tz) {
-    tx = 32;
-    ty = d == 2 ? 1 : 8;
-    tz = d == 2 ? 8 : 1;
+// The flux cells of a sweep along d are the interior in the other two
+// directions and -1..n along d (vofnonmodule.f90:143-145 loops over is-1..ie+1;
+// only the d-neighbours of interior cells are used).
+__device__ inline bool flux_cell(const SweepArgs& a, int& i, int& j, int& k) {
+    i = blockIdx.x * blockDim.x + threadIdx.x;
+    j = blockIdx.y;
+    k = blockIdx.z;
+    if (a.d == 0) i -= 1; else if (a.d == 1) j -= 1; else k -= 1;
+    return i >= -1 && j >= -1 && k >= -1 && i <= a.L.n[0] && j <= a.L.n[1] && k <= a.L.n[2] &&
+           (a.d == 0 || i < a.L.n[0]) && (a.d == 1 || j < a.L.n[1]) && (a.d == 2 || k < a.L.n[2]);
 }
 
-__global__ void __launch_bounds__(kSweepThreads) k_vof_sweep(const SweepArgs a) {
-    __shared__ double v1[kMaxFlux], v2[kMaxFlux], v3[kMaxFlux];
-    __shared__ int queue[kMaxFlux];
-    __shared__ int nq;
-    const Layout& L = a.L;
-    int tx, ty, tz;
-    tile_shape(a.d, tx, ty, tz);
-    const int i0 = blockIdx.x * tx, j0 = blockIdx.y * ty, k0 = blockIdx.z * tz;
-    // extended tile along d
-    int ex = tx + (a.d == 0 ? 2 : 0), ey = ty + (a.d == 1 ? 2 : 0), ez = tz + (a.d == 2 ? 2 : 0);
-    int ox = a.d == 0 ? -1 : 0, oy = a.d == 1 ? -1 : 0, oz = a.d == 2 ? -1 : 0;
-    const int nflux = ex * ey * ez;
-    const long od = a.d == 0 ? 1 : (a.d == 1 ? L.pitch : L.plane);
-    if (threadIdx.x == 0) nq = 0;
-    __syncthreads();
-    // phase 1: closed-form fluxes, queue the mixed cells
-    for (int e = threadIdx.x; e < nflux; e += blockDim.x) {
-        int li = e % ex, lj = (e / ex) % ey, lk = e / (ex * ey);
-        int i = i0 + ox + li, j = j0 + oy + lj, k = k0 + oz + lk;
-        double f1 = 0.0, f2 = 0.0, f3 = 0.0;
-        bool in = i >= -1 && i <= L.n[0] && j >= -1 && j <= L.n[1] && k >= -1 && k <= L.n[2];
-        if (in) {
-            long n = lidx(L, i, j, k);
-            double cc = a.c[n];
-            double a2 = a.us[n] * a.dt / a.dxyz;
-            double a1 = a.us[n - od] * a.dt / a.dxyz;
-            if (cc == 1.0) {
-                f1 = plic::dmax1(-a1, 0.0);
-                f2 = a.wy ? 0.0 : 1.0 - plic::dmax1(a1, 0.0) + plic::dmin1(a2, 0.0);
-                f3 = plic::dmax1(a2, 0.0);
-            } else if (cc > 0.0) {
-                int q = atomicAdd(&nq, 1);
-                queue[q] = e;
-            }
-        }
-        v1[e] = f1; v2[e] = f2; v3[e] = f3;
+// 1. list of the mixed flux cells (0 < c < 1), warp-aggregated append
+__global__ void k_vof_mixed_list(const SweepArgs a) {
+    int i, j, k;
+    bool in = flux_cell(a, i, j, k);
+    long n = in ? lidx(a.L, i, j, k) : 0;
+    bool mixed = in && a.c[n] > 0.0 && a.c[n] != 1.0;
+    unsigned m = __ballot_sync(0xffffffffu, mixed);
+    if (!m) return;
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(a.count, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (mixed) {
+        int q = base + __popc(m & ((1u << lane) - 1u));
+        if (q < a.cap) a.list[q] = n;
     }
-    __syncthreads();
-    // phase 1b: PLIC fluxes of the mixed cells
-    for (int q = threadIdx.x; q < nq; q += blockDim.x) {
-        int e = queue[q];
-        int li = e % ex, lj = (e / ex) % ey, lk = e / (ex * ey);
-        int i = i0 + ox + li, j = j0 + oy + lj, k = k0 + oz + lk;
-        long n = lidx(L, i, j, k);
+}
+
+// 2. PLIC fluxes of the listed cells: fit_plane_new + three FL3D for swpz,
+// mycs + AL3D + two FL3D for swpr
+__global__ void __launch_bounds__(128) k_vof_mixed_flux(const SweepArgs a) {
+    const Layout& L = a.L;
+    const long od = a.d == 0 ? 1 : (a.d == 1 ? L.pitch : L.plane);
+    int cnt = *a.count;
+    if (cnt > a.cap) cnt = (int)a.cap;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt; q += gridDim.x * blockDim.x) {
+        long n = a.list[q];
         double cc = a.c[n];
         double a2 = a.us[n] * a.dt / a.dxyz;
         double a1 = a.us[n - od] * a.dt / a.dxyz;
         double st[27];
 #pragma unroll
-        for (int i1 = -1; i1 <= 1; i1++)
+        for (int k1 = -1; k1 <= 1; k1++)
 #pragma unroll
             for (int j1 = -1; j1 <= 1; j1++)
 #pragma unroll
-                for (int k1 = -1; k1 <= 1; k1++)
+                for (int i1 = -1; i1 <= 1; i1++)
                     st[(i1 + 1) + 3 * (j1 + 1) + 9 * (k1 + 1)] = a.c[n + i1 + j1 * L.pitch + k1 * L.plane];
         double m[3], x0[3] = {0.0, 0.0, 0.0}, dx[3] = {1.0, 1.0, 1.0};
         plic::mycs(st, m);
         double f1 = 0.0, f2 = 0.0, f3 = 0.0;
         if (!a.wy) {
-            // fit_plane_new (vofnonmodule.f90:633-655) and the three fluxes of swpz
             if (!(m[0] == 0.0 && m[1] == 0.0 && m[2] == 0.0)) {
                 double alpha = plic::al3d(m, cc);
                 m[a.d] = m[a.d] / (1.0 - a1 + a2);
@@ -126,35 +115,51 @@ __global__ void __launch_bounds__(kSweepThreads) k_vof_sweep(const SweepArgs a) 
                 f3 = plic::fl3d(m, alpha, x0, dx);
             }
         }
-        v1[e] = f1; v2[e] = f2; v3[e] = f3;
+        a.v1[n] = f1; a.v2[n] = f2; a.v3[n] = f3;
     }
-    __syncthreads();
-    // phase 2: the update of the tile's cells, clipping and flags
-    const int eo = a.d == 0 ? 1 : (a.d == 1 ? ex : ex * ey);   // flux-tile stride along d
-    for (int e = threadIdx.x; e < tx * ty * tz; e += blockDim.x) {
-        int li = e % tx, lj = (e / tx) % ty, lk = e / (tx * ty);
-        int i = i0 + li, j = j0 + lj, k = k0 + lk;
-        if (i >= L.n[0] || j >= L.n[1] || k >= L.n[2]) continue;
-        int f = (li - ox) + ex * ((lj - oy) + ey * (lk - oz));
-        long n = lidx(L, i, j, k);
-        double cnew;
-        if (!a.wy) {
-            cnew = v3[f - eo] + v2[f] + v1[f + eo];
-            cnew = plic::dmax1(0.0, plic::dmin1(1.0, cnew));
-        } else {
-            double a2 = a.us[n] * a.dt / a.dxyz;
-            double a1 = a.us[n - od] * a.dt / a.dxyz;
-            cnew = a.c[n] - (v3[f] - v1[f + eo]) + (v3[f - eo] - v1[f]) + (double)a.cg[n] * (a2 - a1);
-            if (cnew < a.epsc) cnew = 0.0;
-            else if (cnew > 1.0 - a.epsc) cnew = 1.0;
-        }
-        int8_t fl;
-        if (cnew <= a.epsc) { fl = 0; cnew = 0.0; }
-        else if (cnew >= 1.0 - a.epsc) { fl = 1; cnew = 1.0; }
-        else fl = 2;
-        a.cn[n] = cnew;
-        a.flag[n] = fl;
+}
+
+// vof1/vof2/vof3 of one flux cell: closed form for c == 1 (and 0 for c <= 0),
+// the stored PLIC flux for a mixed cell (vofnonmodule.f90:155-186, :700-727)
+__device__ inline double cell_flux(const SweepArgs& a, long n, long od, int which) {
+    double cc = a.c[n];
+    if (cc == 1.0) {
+        double a2 = a.us[n] * a.dt / a.dxyz;
+        double a1 = a.us[n - od] * a.dt / a.dxyz;
+        if (which == 1) return plic::dmax1(-a1, 0.0);
+        if (which == 3) return plic::dmax1(a2, 0.0);
+        return 1.0 - plic::dmax1(a1, 0.0) + plic::dmin1(a2, 0.0);
     }
+    if (cc > 0.0) return which == 1 ? a.v1[n] : (which == 2 ? a.v2[n] : a.v3[n]);
+    return 0.0;
+}
+
+// 3. the update of the interior: new c, clipping (swpz :224-230 / swpr
+// :731-745 and get_flags_and_clip) and the flag, into the second buffer
+__global__ void k_vof_update(const SweepArgs a) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    const Layout& L = a.L;
+    if (i >= L.n[0]) return;
+    const long od = a.d == 0 ? 1 : (a.d == 1 ? L.pitch : L.plane);
+    long n = lidx(L, i, j, k);
+    double cnew;
+    if (!a.wy) {
+        cnew = cell_flux(a, n - od, od, 3) + cell_flux(a, n, od, 2) + cell_flux(a, n + od, od, 1);
+        cnew = plic::dmax1(0.0, plic::dmin1(1.0, cnew));
+    } else {
+        double a2 = a.us[n] * a.dt / a.dxyz;
+        double a1 = a.us[n - od] * a.dt / a.dxyz;
+        cnew = a.c[n] - (cell_flux(a, n, od, 3) - cell_flux(a, n + od, od, 1)) +
+               (cell_flux(a, n - od, od, 3) - cell_flux(a, n, od, 1)) + (double)a.cg[n] * (a2 - a1);
+        if (cnew < a.epsc) cnew = 0.0;
+        else if (cnew > 1.0 - a.epsc) cnew = 1.0;
+    }
+    int8_t fl;
+    if (cnew <= a.epsc) { fl = 0; cnew = 0.0; }
+    else if (cnew >= 1.0 - a.epsc) { fl = 1; cnew = 1.0; }
+    else fl = 2;
+    a.cn[n] = cnew;
+    a.flag[n] = fl;
 }
 
 // ghost cells of the new cvof and flags: SetVOFBC on walls (orientations
@@ -239,24 +244,40 @@ __global__ void k_c_mask(const double* __restrict__ c, uint8_t* __restrict__ cg,
 }
 
 static int sweep(paris_ctx* c, int d, double dt) {
+    const Layout& L = c->L;
+    if (!c->vflux) {
+        PARIS_CUDA_TRY(c, cudaMalloc(&c->vflux, 3 * L.total * sizeof(double)));
+        PARIS_CUDA_TRY(c, cudaMalloc(&c->mixlist, L.total * sizeof(long)));
+        PARIS_CUDA_TRY(c, cudaMalloc(&c->mixcount, sizeof(int)));
+    }
     SweepArgs a;
     a.c = c->fld[PARIS_FIELD_CVOF];
     a.cn = c->c2;
     a.flag = c->flag;
     a.us = c->fld[PARIS_FIELD_U + d];
     a.cg = c->cg;
-    a.L = c->L;
+    a.v1 = c->vflux;
+    a.v2 = c->vflux + L.total;
+    a.v3 = c->vflux + 2 * L.total;
+    a.list = c->mixlist;
+    a.count = c->mixcount;
+    a.cap = L.total;
+    a.L = L;
     a.d = d;
     a.wy = c->d.vof_advect == PARIS_ADVECT_WY;
     a.dt = dt;
     a.dxyz = c->h_dxh[c->d.ng];
     a.epsc = c->d.epsc;
-    int tx, ty, tz;
-    tile_shape(d, tx, ty, tz);
-    dim3 grid(div_up(c->L.n[0], tx), div_up(c->L.n[1], ty), div_up(c->L.n[2], tz));
-    PARIS_LAUNCH_N(c, "vof_sweep", c->N, k_vof_sweep, grid, kSweepThreads, 0, a);
+    PARIS_CUDA_TRY(c, cudaMemsetAsync(c->mixcount, 0, sizeof(int), c->stream));
+    int ext[3] = {L.n[0], L.n[1], L.n[2]};
+    ext[d] += 2;
+    PARIS_LAUNCH_N(c, "vof_mixed_list", (long)ext[0] * ext[1] * ext[2], k_vof_mixed_list,
+                   dim3(div_up(ext[0], 128), ext[1], ext[2]), 128, 0, a);
+    PARIS_LAUNCH_N(c, "vof_mixed_flux", 0L, k_vof_mixed_flux, 148 * 16, 128, 0, a);
+    PARIS_LAUNCH_N(c, "vof_sweep", c->N, k_vof_update, dim3(div_up(L.n[0], 128), L.n[1], L.n[2]), 128, 0, a);
     long G = ghost_total(c->L);
-    PARIS_LAUNCH_N(c, "vof_ghosts", G, k_vof_ghosts, div_up(G, 256), 256, 0, c->c2, c->flag, c->L, c->bnd, G, c->d.epsc);
+    PARIS_LAUNCH_N(c, "vof_ghosts", G, k_vof_ghosts, div_up(G, 256), 256, 0, c->c2, c->flag, c->L, c->bnd, G,
+                   c->d.epsc);
     double* t = c->fld[PARIS_FIELD_CVOF];
     c->fld[PARIS_FIELD_CVOF] = c->c2;
     c->c2 = t;

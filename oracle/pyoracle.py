@@ -57,6 +57,9 @@ def lib():
             "og_linfunc": (I, [G, P, P, D, D, I]),
             "og_init_spheres": (I, [G, I, P, P, P, P, I, I, P, P, P]),
             "og_fastmg_solve": (I, [G, P, P, D, I, I, I, I, I, P]),
+            "og_get_all_heights": (I, [G, P, P, P]),
+            "og_get_all_curvatures": (I, [G, P, P, P, P, P, P]),
+            "og_surface_force": (I, [G, P, P, P, P, P, P]),
             "og_al3d": (D, [P, D]),
             "og_cc3d": (D, [P, D]),
             "og_fl3d": (D, [P, D, P, P]),
@@ -212,3 +215,26 @@ def fastmg_solve(desc, A, p_int, rel_tol, maxit=100, mixed=True, pcg=False, nu1=
     it = lib().og_fastmg_solve(ctypes.byref(desc), _p(np.ascontiguousarray(A)), _p(p), rel_tol, maxit,
                                1 if mixed else 0, 1 if pcg else 0, nu1, nu2, _p(hist))
     return p, it, hist[:it]
+
+
+def get_all_heights(desc, cvof, flag):
+    """get_all_heights: returns height (6, Nzt, Nyt, Nxt)."""
+    H = np.zeros((6,) + shape(desc))
+    lib().og_get_all_heights(ctypes.byref(desc), _p(np.ascontiguousarray(cvof)),
+                             _p(np.ascontiguousarray(flag, dtype=np.int32)), _p(H))
+    return H
+
+
+def get_all_curvatures(desc, cvof, flag, H):
+    """get_all_curvatures: returns (kappa, kappaflag, method_count)."""
+    kap = zeros(desc)
+    kf = zeros(desc, np.int32)
+    mc = np.zeros(5, dtype=np.int32)
+    lib().og_get_all_curvatures(ctypes.byref(desc), _p(np.ascontiguousarray(cvof)),
+                                _p(np.ascontiguousarray(flag, dtype=np.int32)), _p(np.ascontiguousarray(H)),
+                                _p(kap), _p(kf), _p(mc))
+    return kap, kf, mc
+
+
+def surface_force(desc, cvof, kappa, rho, du, dv, dw):
+    return lib().og_surface_force(ctypes.byref(desc), _p(cvof), _p(kappa), _p(rho), _p(du), _p(dv), _p(dw))

@@ -26,6 +26,7 @@ SOURCES = {
     "vof.cu": True,
     "stubs.cu": True,
     "noalloc.cu": True,
+    "st.cu": True,
 }
 
 

@@ -48,6 +48,9 @@ struct paris_ctx {
     long* mixlist = nullptr;       // mixed flux cells of the current sweep
     int* mixcount = nullptr;
     double* height = nullptr;      // 6 ghosted fields
+    int8_t* kflag = nullptr;       // kappaflag of the curvature passes
+    int* st_list = nullptr;        // interior mixed cells of the curvature passes
+    int* st_count = nullptr;
     int32_t* i32stage = nullptr;   // staging for int32 host transfers
     // pressure equation, compact interior arrays (N each)
     double *cx = nullptr, *cy = nullptr, *cz = nullptr, *rhs = nullptr;

@@ -2,18 +2,6 @@
 // this build yet; they fail loudly.
 #include "ctx.cuh"
 
-extern "C" int paris_get_all_heights(paris_handle_t c) {
-    if (c) ctx_set_error(c, "paris_get_all_heights: not implemented in this build");
-    return PARIS_BAD_ARGS;
-}
-extern "C" int paris_get_all_curvatures(paris_handle_t c, double*) {
-    if (c) ctx_set_error(c, "paris_get_all_curvatures: not implemented in this build");
-    return PARIS_BAD_ARGS;
-}
-extern "C" int paris_surface_force(paris_handle_t c) {
-    if (c) ctx_set_error(c, "paris_surface_force: not implemented in this build");
-    return PARIS_BAD_ARGS;
-}
 extern "C" int paris_projection_adjoint(paris_handle_t c, double, const double*, const double*, const double*, double*,
                                         double*, double*, double*, double*, double*, const paris_solve_opts*) {
     if (c) ctx_set_error(c, "paris_projection_adjoint: not implemented in this build");

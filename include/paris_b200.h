@@ -207,13 +207,23 @@ int paris_project_velocity(paris_handle_t h, double dt);
 int paris_calc_residuals_noalloc(int32_t nx, int32_t ny, int32_t nz, int32_t ng, const double* A_dev,
                                  const double* p_dev, double* out3, void* stream);
 
-/* ---- projection adjoint (no counterpart in the reference: the transpose of
- *      SetupPoisson modules.f90:2735-2745 + solve + project_velocity
- *      paris.f90:898-909).  With u = u* - dt*B*G*p and A(B) p = -D u*,
- *      given g_u = dL/du (three face fields, reference layout with ghosts),
- *      returns dL/du* (three face fields) and dL/dB, B being the face
- *      coefficient 2/(rho_c + rho_n) of each face (three face fields).
- *      The forward p (checkpointed on the device by the last solve) is used.  */
+/* ---- projection adjoint.  No counterpart in the reference: the transpose
+ *      of SetupPoisson (modules.f90:2722-2753) + NewSolver + project_velocity
+ *      (paris.f90:898-909).  With B_f = 2/(rho_L + rho_R) on every face,
+ *      A(B) p = -D u* and u = u* - dt*B*G*p, given gu, gv, gw = dL/du it
+ *      returns gus, gvs, gws = dL/du* and gbx, gby, gbz = dL/dB (six face
+ *      fields; all nine arrays in the reference layout with ghosts, host or
+ *      device memory).  Gradients live on the faces project_velocity updates
+ *      (all faces of a periodic direction, the interior faces of a wall-bounded
+ *      one); ghost entries of gu/gv/gw are ignored and those of the outputs
+ *      are zero (ghost faces are periodic images or boundary constants).
+ *      Uses the forward state on the device: RHO, the matrix of the last
+ *      paris_setup_poisson (dt must equal its dt) and P as left by the solve.
+ *      The transpose solve is the B200 multigrid (A is symmetric); opts as for
+ *      paris_new_solver with PARIS_MG_REFERENCE read as PARIS_MG_FP64, or NULL
+ *      for FP64 PCG to ||r||/||b|| < 1e-12.  Returns PARIS_NOT_CONVERGED (with
+ *      the outputs written) when that tolerance was not reached.  Any output
+ *      pointer may be NULL. */
 int paris_projection_adjoint(paris_handle_t h, double dt,
                              const double* gu, const double* gv, const double* gw,
                              double* gus, double* gvs, double* gws,

@@ -67,6 +67,9 @@ def lib():
             "og_area_centroid": (None, [P, D, P]),
             "og_mycs": (None, [P, P]),
             "og_fd32": (None, [P, P]),
+            "og_face_B": (None, [G, P, P, P, P]),
+            "og_projection_forward_B": (I, [G, D, P, P, P, P, P, P, P, P, P, P, D, I]),
+            "og_projection_adjoint": (I, [G, D, P, P, P, P, P, P, P, P, P, P, P, P, P, D, I]),
         }
         for name, (res, args) in protos.items():
             f = getattr(_lib, name)
@@ -238,3 +241,47 @@ def get_all_curvatures(desc, cvof, flag, H):
 
 def surface_force(desc, cvof, kappa, rho, du, dv, dw):
     return lib().og_surface_force(ctypes.byref(desc), _p(cvof), _p(kappa), _p(rho), _p(du), _p(dv), _p(dw))
+
+
+def face_B(desc, rho):
+    """B_f = 2/(rho_L + rho_R) on the faces project_velocity updates."""
+    B = [zeros(desc) for _ in range(3)]
+    lib().og_face_B(ctypes.byref(desc), _p(np.ascontiguousarray(rho)), *(_p(b) for b in B))
+    return B
+
+
+def projection_forward_B(desc, dt, B, ustar, rel_tol=1e-15, maxit=60):
+    """SetupPoisson + solve + project_velocity with the face coefficients B
+    as the parameters.  Returns ([u, v, w], p, cycles)."""
+    us = [np.ascontiguousarray(a, dtype=np.float64) for a in ustar]
+    out = [zeros(desc) for _ in range(3)]
+    p = zeros(desc)
+    it = lib().og_projection_forward_B(ctypes.byref(desc), dt, *(_p(np.ascontiguousarray(b)) for b in B),
+                                       *(_p(a) for a in us), *(_p(a) for a in out), _p(p), rel_tol, maxit)
+    return out, p, it
+
+
+def projection_adjoint(desc, dt, B, p, g, rel_tol=1e-15, maxit=60):
+    """dL/du* and dL/dB of the projection given g = dL/du.  Returns
+    ([gu*, gv*, gw*], [gBx, gBy, gBz], cycles)."""
+    gs = [zeros(desc) for _ in range(3)]
+    gb = [zeros(desc) for _ in range(3)]
+    gg = [np.ascontiguousarray(a, dtype=np.float64) for a in g]
+    it = lib().og_projection_adjoint(ctypes.byref(desc), dt, *(_p(np.ascontiguousarray(b)) for b in B),
+                                     _p(np.ascontiguousarray(p)), *(_p(a) for a in gg), *(_p(a) for a in gs),
+                                     *(_p(a) for a in gb), rel_tol, maxit)
+    return gs, gb, it
+
+
+def updated_faces(desc, d):
+    """Boolean mask (layout shape) of the faces of direction d (0=x) that
+    project_velocity updates."""
+    m = np.zeros(shape(desc), dtype=bool)
+    g = desc.ng
+    n = (desc.nx, desc.ny, desc.nz)
+    per = desc.bdry_cond[d] == 1
+    hi = [n[0], n[1], n[2]]
+    if not per:
+        hi[d] -= 1
+    m[g:g + hi[2], g:g + hi[1], g:g + hi[0]] = True
+    return m

@@ -24,7 +24,7 @@ SOURCES = {
     "mg_fast.cu": False,
     "solver.cu": True,
     "vof.cu": True,
-    "stubs.cu": True,
+    "adjoint.cu": True,
     "noalloc.cu": True,
     "st.cu": True,
 }

@@ -77,6 +77,7 @@ struct paris_ctx {
     double* fast_q64 = nullptr;
     double* fast_z64 = nullptr;
     double* fast_zold64 = nullptr;
+    double* adj = nullptr;         // projection adjoint: 10 ghosted fields + N (allocated on first use)
     int64_t launches = 0;
     char err[512] = {0};
     // per-kernel event timing
@@ -122,3 +123,4 @@ int poisson_build_full_A(paris_ctx* c);
 int mg_ref_solve(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* r);
 // mg_fast.cu
 int mg_fast_solve(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* r);
+int mg_fast_solve_into(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* r, const double* rhs, double* x);

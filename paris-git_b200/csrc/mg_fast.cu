@@ -434,10 +434,9 @@ static bool converged(const paris_solve_opts* o, double s2, double s1, double bn
 }
 
 template <typename T>
-static int solve_dc(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* res) {
+static int solve_dc(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* res, const double* rhs, double* p) {
     auto& lv = levels<T>(c);
-    Mat64 A{c->cx, c->cy, c->cz, c->rhs};
-    double* p = c->fld[PARIS_FIELD_P];
+    Mat64 A{c->cx, c->cy, c->cz, rhs};
     double s[3], tres, rel;
     PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>, red_grid(c, k_fast_residual64<T>, 256), kRowBlock, 0, A, p, c->L, c->bnd, lv[0].b, (double*)nullptr,
                  c->red_part);
@@ -487,11 +486,10 @@ static int precondition(paris_ctx* c, int nu1, int nu2, double* rz, double* rzol
 }
 
 template <typename T>
-static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* res) {
+static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* res, const double* rhs, double* p) {
     for (double** v : {&c->fast_r64, &c->fast_d64, &c->fast_q64, &c->fast_z64, &c->fast_zold64})
         PARIS_CHECK(alloc_vec(c, v));
-    Mat64 A{c->cx, c->cy, c->cz, c->rhs};
-    double* p = c->fld[PARIS_FIELD_P];
+    Mat64 A{c->cx, c->cy, c->cz, rhs};
     double s[3], tres, rel;
     PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>, red_grid(c, k_fast_residual64<T>, 256), kRowBlock, 0, A, p, c->L, c->bnd, (T*)nullptr, c->fast_r64,
                  c->red_part);
@@ -538,18 +536,23 @@ static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result
     return done ? PARIS_OK : PARIS_NOT_CONVERGED;
 }
 
-int mg_fast_solve(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* res) {
+int mg_fast_solve_into(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* res, const double* rhs,
+                       double* x) {
     if (!c->have_matrix) return PARIS_BAD_ARGS;
     int st;
     if (o->mode == PARIS_MG_MIXED) {
         PARIS_CHECK(fast_alloc<float>(c));
         PARIS_CHECK(fast_coefs<float>(c));
-        st = o->pcg ? solve_pcg<float>(c, o, res) : solve_dc<float>(c, o, res);
+        st = o->pcg ? solve_pcg<float>(c, o, res, rhs, x) : solve_dc<float>(c, o, res, rhs, x);
     } else {
         PARIS_CHECK(fast_alloc<double>(c));
         PARIS_CHECK(fast_coefs<double>(c));
-        st = o->pcg ? solve_pcg<double>(c, o, res) : solve_dc<double>(c, o, res);
+        st = o->pcg ? solve_pcg<double>(c, o, res, rhs, x) : solve_dc<double>(c, o, res, rhs, x);
     }
-    if (st == PARIS_OK || st == PARIS_NOT_CONVERGED) PARIS_CHECK(ctx_ghost_fill(c, c->fld[PARIS_FIELD_P]));
+    if (st == PARIS_OK || st == PARIS_NOT_CONVERGED) PARIS_CHECK(ctx_ghost_fill(c, x));
     return st;
+}
+
+int mg_fast_solve(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* res) {
+    return mg_fast_solve_into(c, o, res, c->rhs, c->fld[PARIS_FIELD_P]);
 }

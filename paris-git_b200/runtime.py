@@ -206,3 +206,27 @@ class ParisGpu:
     def project_velocity(self, dt):
         """project_velocity(), paris.f90:882."""
         self._check(self.lib.paris_project_velocity(self.h, float(dt)), "project_velocity")
+
+    def projection_adjoint(self, dt, g, rel_tol=1e-12, maxit=100, mode=capi.MG_FP64, pcg=1):
+        """Reverse mode of setup_poisson + new_solver + project_velocity.
+
+        g: dL/du, dL/dv, dL/dw (layout-shaped float64 arrays).  Returns
+        ([dL/du*, dL/dv*, dL/dw*], [dL/dBx, dL/dBy, dL/dBz]) with
+        B = 2/(rho_L + rho_R) the face coefficient; the forward state (RHO,
+        the SetupPoisson matrix, P) must still be on the device."""
+        o = capi.SolveOpts()
+        o.max_error, o.rel_tol, o.beta = 0.0, float(rel_tol), 1.0
+        o.maxit, o.norm, o.mode, o.nu1, o.nu2, o.pcg = int(maxit), 2, int(mode), 2, 2, int(pcg)
+        gg = [np.ascontiguousarray(a, dtype=np.float64) for a in g]
+        for a in gg:
+            if a.shape != self.shape:
+                raise ValueError("projection_adjoint: gradient arrays must have the layout's shape")
+        gs = [np.empty(self.shape) for _ in range(3)]
+        gb = [np.empty(self.shape) for _ in range(3)]
+        st = self.lib.paris_projection_adjoint(self.h, float(dt), *(_ptr(a) for a in gg), *(_ptr(a) for a in gs),
+                                               *(_ptr(a) for a in gb), ctypes.byref(o))
+        if st == capi.NOT_CONVERGED:
+            warnings.warn("projection_adjoint: transpose solve did not reach the tolerance")
+        else:
+            self._check(st, "projection_adjoint")
+        return gs, gb

@@ -36,7 +36,7 @@ def make_case(capi, orc, n, bc, seed, layout):
     return d, us, w, m, cen, rad
 
 
-def gpu_forward(gpu, capi, dt, us, p0=None, rel_tol=1e-14, maxit=60):
+def gpu_forward(gpu, capi, dt, us, p0=None, rel_tol=1e-14, maxit=60, project=True):
     for f, a in zip((capi.F_U, capi.F_V, capi.F_W), us):
         gpu.upload(f, a)
     gpu.setup_poisson(dt)
@@ -47,6 +47,8 @@ def gpu_forward(gpu, capi, dt, us, p0=None, rel_tol=1e-14, maxit=60):
     with warnings.catch_warnings():
         warnings.simplefilter("ignore")
         gpu.new_solver(0.0, maxit=maxit, mode=capi.MG_FP64, rel_tol=rel_tol, pcg=1)
+    if not project:
+        return None
     gpu.project_velocity(dt)
     return [gpu.download(f) for f in (capi.F_U, capi.F_V, capi.F_W)]
 
@@ -89,12 +91,17 @@ def test_adjoint_matches_oracle(gpu_lib, capi, runtime, orc, bc, n):
 
 
 def fd_forward(gpu, capi, dt, us, p0):
-    """A forward for differencing: from the unperturbed pressure, 12 PCG
-    cycles with no stopping test, which takes the residual of the +-eps
-    perturbation down to the FP64 floor of b - A p (the stopping test of
-    the base solve, relative to ||b||, would leave ~1e-5 of a 1e-6
-    perturbation's response unresolved at 128^3)."""
-    return gpu_forward(gpu, capi, dt, us, p0, rel_tol=1e-300, maxit=12)
+    """A forward for differencing, from the unperturbed pressure: FP64 PCG to
+    ||r||/||b|| < 1e-15, then four FP64 defect-correction cycles that take the
+    true residual b - A p to its FP64 floor (the base solve's 1e-14 would
+    leave ~1e-5 of the response to a 1e-6 perturbation unresolved at 128^3;
+    CG itself is not run below the floor, where its recurrences drift)."""
+    gpu_forward(gpu, capi, dt, us, p0, rel_tol=1e-15, maxit=60, project=False)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        gpu.new_solver(0.0, maxit=4, mode=capi.MG_FP64, rel_tol=1e-300, pcg=0)
+    gpu.project_velocity(dt)
+    return [gpu.download(f) for f in (capi.F_U, capi.F_V, capi.F_W)]
 
 
 def test_adjoint_finite_differences_128(gpu_lib, capi, runtime, orc):

@@ -158,6 +158,17 @@ def workload(pkg, n, device=0):
 # algorithmic HBM bytes per cell of each labelled kernel (cells as recorded
 # by the profiler: the grid cells the launch processes)
 ALGO_BYTES = {
+    "pcg_matvec_fp64": 40.0,      # d 8 + 3 faces 24 + q 8
+    "pcg_update_fp64(z32)": 56.0, # p r/w 16 + d 8 + r r/w 16 + q 8 + rhs (FP32) 4 + z (FP32) 4
+    "pcg_update_fp64(z64)": 64.0,
+    "pcg_rz(z32)": 12.0,          # r 8 + z 4
+    "pcg_rz(z64)": 16.0,
+    "pcg_dir(z32)": 20.0,         # z 4 + d r/w 16
+    "pcg_dir(z64)": 24.0,
+    "mg_sweep_f32": 24.0,         # fused red-black sweep: x in 4 + 3 faces 12 + rhs 4 + x out 4
+    "mg_sweep_f64": 48.0,
+    "mg_sweep_zero_f32": 20.0,    # first sweep from x = 0: no iterate read
+    "mg_sweep_zero_f64": 40.0,
     "mg_smooth_f32": 12.0,        # half of a red-black sweep: (p 4 + 3 faces 12 + rhs 4 + p write 4)/2
     "mg_smooth_f64": 24.0,
     "mg_restrict_f32": 20.5,      # x 4 + b 4 + 3 faces 12 + coarse rhs 4/8

@@ -264,13 +264,13 @@ extern "C" int paris_gpu_finalize(paris_handle_t c) {
                     (void*)c->xc, (void*)c->yc, (void*)c->zc, (void*)c->c2, (void*)c->flag, (void*)c->cg,
                     (void*)c->height, (void*)c->i32stage, (void*)c->cx, (void*)c->cy, (void*)c->cz,
                     (void*)c->rhs, (void*)c->A, (void*)c->red_part, (void*)c->red_out, (void*)c->fast_r64,
-                    (void*)c->fast_d64, (void*)c->fast_q64, (void*)c->fast_z64, (void*)c->fast_zold64,
+                    (void*)c->fast_d64, (void*)c->fast_q64,
                     (void*)c->vflux, (void*)c->mixlist, (void*)c->mixcount, (void*)c->kflag, (void*)c->st_list,
                     (void*)c->st_count, (void*)c->adj})
         free_ptr(p);
     for (auto& l : c->ref) { free_ptr(l.K); free_ptr(l.p); free_ptr(l.e); }
-    for (auto& l : c->fl32) { free_ptr(l.cx); free_ptr(l.cy); free_ptr(l.cz); free_ptr(l.b); free_ptr(l.x); }
-    for (auto& l : c->fl64) { free_ptr(l.cx); free_ptr(l.cy); free_ptr(l.cz); free_ptr(l.b); free_ptr(l.x); }
+    for (auto& l : c->fl32) { free_ptr(l.cx); free_ptr(l.cy); free_ptr(l.cz); free_ptr(l.b); free_ptr(l.x); free_ptr(l.x2); }
+    for (auto& l : c->fl64) { free_ptr(l.cx); free_ptr(l.cy); free_ptr(l.cz); free_ptr(l.b); free_ptr(l.x); free_ptr(l.x2); }
     if (c->red_host) cudaFreeHost(c->red_host);
     for (auto e : c->evpool) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);

@@ -26,6 +26,7 @@ struct FastLevel {
     long N;
     T *cx, *cy, *cz;
     T *b, *x;
+    T* x2;   // second iterate of the fused sweeps (they read one and write the other)
 };
 
 struct paris_ctx {
@@ -75,8 +76,6 @@ struct paris_ctx {
     double* fast_r64 = nullptr;    // PCG vectors (N each)
     double* fast_d64 = nullptr;
     double* fast_q64 = nullptr;
-    double* fast_z64 = nullptr;
-    double* fast_zold64 = nullptr;
     double* adj = nullptr;         // projection adjoint: 10 ghosted fields + N (allocated on first use)
     int64_t launches = 0;
     char err[512] = {0};

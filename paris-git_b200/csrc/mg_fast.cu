@@ -15,6 +15,7 @@
 static constexpr long kCoarseCells = 4096;   // 16^3
 static constexpr int kMaxLevels = 16;
 static constexpr int kCoarseSweeps = 8;
+static constexpr long kFusedCells = 1L << 18;   // levels of at least 64^3 cells use the fused sweep
 
 template <typename T>
 struct LV {
@@ -104,6 +105,8 @@ __global__ void k_fast_prolong(const LV<T> f, const LV<T> c) {
 }
 
 static inline dim3 row_grid(long n0, int n1, int n2) { return dim3(div_up(n0, 128), n1, n2); }
+
+#include "mg_sweep.cuh"
 
 // The V-cycle from level L0 down to the coarsest, in one block.
 template <typename T>
@@ -260,59 +263,52 @@ __global__ void k_pcg_matvec(const Mat64 A, const double* __restrict__ d, double
     if (linear_tid() == 0) part[blockIdx.x] = s;
 }
 
-// p += alpha d (ghosted p), r -= alpha q ; slots 0 = r.r, 1 = sum |r|
+// p += alpha d (ghosted p), r -= alpha q, and the right-hand side of the next
+// V-cycle rT = (T) r.  slots: 0 = r.r, 1 = sum |r|, 2 = r.zold (zold: the
+// last preconditioned residual, still in the V-cycle's output buffer)
+template <typename T>
 __global__ void k_pcg_update(double* __restrict__ p, double* __restrict__ r, const double* __restrict__ d,
-                             const double* __restrict__ q, double alpha, const Layout L, double* part) {
+                             const double* __restrict__ q, T* __restrict__ rT, const T* __restrict__ zold,
+                             double alpha, const Layout L, double* part) {
     __shared__ double sh[32];
-    double s2 = 0.0, s1 = 0.0;
+    double s2 = 0.0, s1 = 0.0, sz = 0.0;
     ROWS_BEGIN(L.n[0], L.n[1], L.n[2])
         long m = cidx(L.n[0], L.n[1], i, j, k);
         long n = lidx(L, i, j, k);
         p[n] = p[n] + alpha * d[m];
         double rr = r[m] - alpha * q[m];
         r[m] = rr;
+        rT[m] = (T)rr;
         s2 += rr * rr;
         s1 += fabs(rr);
+        sz += rr * (double)zold[m];
     ROWS_END
     s2 = block_sum<256>(s2, sh);
     s1 = block_sum<256>(s1, sh);
+    sz = block_sum<256>(sz, sh);
     if (linear_tid() == 0) {
         part[blockIdx.x] = s2;
         part[kRedBlocks + blockIdx.x] = s1;
+        part[2 * kRedBlocks + blockIdx.x] = sz;
     }
 }
 
+// slot 0 = r.z with z the V-cycle's output
 template <typename T>
-__global__ void k_to_T(const double* __restrict__ a, T* __restrict__ b, long N) {
-    long m = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (m < N) b[m] = (T)a[m];
-}
-
-// zold = z; z = x0 ; slots 0 = r.z, 1 = r.zold
-template <typename T>
-__global__ void k_pcg_takez(const T* __restrict__ x0, double* __restrict__ z, double* __restrict__ zold,
-                            const double* __restrict__ r, long N, double* part) {
+__global__ void k_pcg_rz(const T* __restrict__ z, const double* __restrict__ r, long N, double* part) {
     __shared__ double sh[32];
-    double s0 = 0.0, s1 = 0.0;
-    for (long m = blockIdx.x * (long)blockDim.x + threadIdx.x; m < N; m += (long)gridDim.x * blockDim.x) {
-        double zo = z[m];
-        double zn = (double)x0[m];
-        zold[m] = zo;
-        z[m] = zn;
-        s0 += r[m] * zn;
-        s1 += r[m] * zo;
-    }
+    double s0 = 0.0;
+    for (long m = blockIdx.x * (long)blockDim.x + threadIdx.x; m < N; m += (long)gridDim.x * blockDim.x)
+        s0 += r[m] * (double)z[m];
     s0 = block_sum<256>(s0, sh);
-    s1 = block_sum<256>(s1, sh);
-    if (threadIdx.x == 0) {
-        part[blockIdx.x] = s0;
-        part[kRedBlocks + blockIdx.x] = s1;
-    }
+    if (threadIdx.x == 0) part[blockIdx.x] = s0;
 }
 
-__global__ void k_pcg_dir(double* __restrict__ d, const double* __restrict__ z, double beta, long N) {
+// d = z + beta d
+template <typename T>
+__global__ void k_pcg_dir(double* __restrict__ d, const T* __restrict__ z, double beta, long N) {
     long m = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (m < N) d[m] = z[m] + beta * d[m];
+    if (m < N) d[m] = (double)z[m] + beta * d[m];
 }
 
 // ---- host side ---------------------------------------------------------------
@@ -322,20 +318,22 @@ static const char* kname(const char* base);
 template <>
 const char* kname<float>(const char* base) {
     static const char* names[] = {"mg_smooth_f32", "mg_restrict_f32", "mg_prolong_f32", "mg_coarse_cycle_f32",
-                                  "mg_correct_f32", "mg_residual_fp64(r32)"};
+                                  "mg_correct_f32", "mg_residual_fp64(r32)", "mg_sweep_f32", "mg_sweep_zero_f32",
+                                  "pcg_update_fp64(z32)", "pcg_rz(z32)", "pcg_dir(z32)"};
     static const char* keys[] = {"mg_smooth", "mg_restrict", "mg_prolong", "mg_coarse_cycle", "mg_correct",
-                                 "mg_residual_fp64"};
-    for (int q = 0; q < 6; q++)
+                                 "mg_residual_fp64", "mg_sweep", "mg_sweep_zero", "pcg_update", "pcg_rz", "pcg_dir"};
+    for (int q = 0; q < 11; q++)
         if (!strcmp(base, keys[q])) return names[q];
     return base;
 }
 template <>
 const char* kname<double>(const char* base) {
     static const char* names[] = {"mg_smooth_f64", "mg_restrict_f64", "mg_prolong_f64", "mg_coarse_cycle_f64",
-                                  "mg_correct_f64", "mg_residual_fp64(r64)"};
+                                  "mg_correct_f64", "mg_residual_fp64(r64)", "mg_sweep_f64", "mg_sweep_zero_f64",
+                                  "pcg_update_fp64(z64)", "pcg_rz(z64)", "pcg_dir(z64)"};
     static const char* keys[] = {"mg_smooth", "mg_restrict", "mg_prolong", "mg_coarse_cycle", "mg_correct",
-                                 "mg_residual_fp64"};
-    for (int q = 0; q < 6; q++)
+                                 "mg_residual_fp64", "mg_sweep", "mg_sweep_zero", "pcg_update", "pcg_rz", "pcg_dir"};
+    for (int q = 0; q < 11; q++)
         if (!strcmp(base, keys[q])) return names[q];
     return base;
 }
@@ -373,6 +371,11 @@ static int fast_alloc(paris_ctx* c) {
         l.n[0] = c->d.nx >> L; l.n[1] = c->d.ny >> L; l.n[2] = c->d.nz >> L;
         l.N = (long)l.n[0] * l.n[1] * l.n[2];
         for (T** p : {&l.cx, &l.cy, &l.cz, &l.b, &l.x}) PARIS_CUDA_TRY(c, cudaMalloc(p, l.N * sizeof(T)));
+        // the fused sweep stages 16-byte row chunks and pairs cells by parity
+        l.x2 = nullptr;
+        bool fusable = l.N >= kFusedCells && l.N > kCoarseCells && l.n[0] % 4 == 0 && l.n[1] % 2 == 0 &&
+                       l.n[2] % 2 == 0 && L < nl - 1;
+        if (fusable) PARIS_CUDA_TRY(c, cudaMalloc(&l.x2, l.N * sizeof(T)));
     }
     return PARIS_OK;
 }
@@ -393,35 +396,99 @@ static int fast_coefs(paris_ctx* c) {
     return PARIS_OK;
 }
 
-// one V(nu1,nu2) cycle on level 0 from x0 = 0 with the right-hand side in b0
+// Planes per block of the fused sweep: enough blocks for one wave of resident
+// blocks, at least 8 planes per block.
 template <typename T>
-static int vcycle(paris_ctx* c, int nu1, int nu2) {
+static int sweep_chunk(paris_ctx* c, const FastLevel<T>& l) {
+    static int per_sm = 0;   // resident blocks per SM (the same on every B200)
+    if (!per_sm) {
+        cudaFuncSetAttribute(k_rb_sweep<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<T>());
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rb_sweep<T>, kSwThreads, sweep_smem<T>()) !=
+                cudaSuccess || per_sm < 1)
+            per_sm = 1;
+    }
+    long tiles = (long)div_up(l.n[0], kSwTX) * div_up(l.n[1], kSwTY);
+    long nbz = (long)per_sm * c->nsm / tiles;
+    long cap = l.n[2] / 8;
+    if (nbz > cap) nbz = cap;
+    if (nbz < 1) nbz = 1;
+    return (int)div_up(l.n[2], nbz);
+}
+
+template <typename T>
+static int sweep_fused(paris_ctx* c, const FastLevel<T>& l, const T* xin, T* xout, const T* xc, int first) {
+    int zc = sweep_chunk<T>(c, l);
+    dim3 grid(div_up(l.n[0], kSwTX), div_up(l.n[1], kSwTY), div_up(l.n[2], zc));
+    PARIS_LAUNCH_N(c, kname<T>(xin ? "mg_sweep" : "mg_sweep_zero"), l.N, k_rb_sweep<T>, grid, kSwThreads,
+                   sweep_smem<T>(), view(l), xin, xout, xc, c->bnd, first, zc);
+    return PARIS_OK;
+}
+
+template <typename T>
+static LV<T> view_x(const FastLevel<T>& l, T* x) {
+    LV<T> v = view(l);
+    v.x = x;
+    return v;
+}
+
+// one V(nu1,nu2) cycle on level 0 from x0 = 0 with the right-hand side in b0;
+// *x0 receives the buffer holding the level-0 result (lv[0].x or lv[0].x2)
+template <typename T>
+static int vcycle(paris_ctx* c, int nu1, int nu2, T** x0) {
     auto& lv = levels<T>(c);
     int nl = (int)lv.size();
     int Lc = 0;
     while (Lc < nl - 1 && lv[Lc].N > kCoarseCells) Lc++;
-    if (Lc > 0) PARIS_CUDA_TRY(c, cudaMemsetAsync(lv[0].x, 0, lv[0].N * sizeof(T), c->stream));
+    T* cur[kMaxLevels];
     for (int L = 0; L < Lc; L++) {
-        LV<T> v = view(lv[L]);
-        for (int s = 0; s < nu1; s++) {
-            PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, row_grid((v.n0 + 1) / 2, v.n1, v.n2), 128, 0, v, c->bnd, 0);
-            PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, row_grid((v.n0 + 1) / 2, v.n1, v.n2), 128, 0, v, c->bnd, 1);
+        const FastLevel<T>& l = lv[L];
+        if (l.x2 && nu1 > 0) {
+            const T* in = nullptr;
+            T* out = l.x;
+            for (int s = 0; s < nu1; s++) {
+                PARIS_CHECK(sweep_fused<T>(c, l, in, out, nullptr, 0));
+                in = out;
+                out = out == l.x ? l.x2 : l.x;
+            }
+            cur[L] = (T*)in;
+        } else {
+            PARIS_CUDA_TRY(c, cudaMemsetAsync(l.x, 0, l.N * sizeof(T), c->stream));
+            LV<T> v = view(l);
+            for (int s = 0; s < nu1; s++) {
+                PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, row_grid((v.n0 + 1) / 2, v.n1, v.n2), 128, 0, v, c->bnd, 0);
+                PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, row_grid((v.n0 + 1) / 2, v.n1, v.n2), 128, 0, v, c->bnd, 1);
+            }
+            cur[L] = l.x;
         }
         LV<T> cv = view(lv[L + 1]);
-        PARIS_LAUNCH_N(c, kname<T>("mg_restrict"), v.N, k_fast_restrict<T>, row_grid(cv.n0, cv.n1, cv.n2), 128, 0, v, cv, c->bnd);
-        if (L + 1 < Lc) PARIS_CUDA_TRY(c, cudaMemsetAsync(lv[L + 1].x, 0, lv[L + 1].N * sizeof(T), c->stream));
+        PARIS_LAUNCH_N(c, kname<T>("mg_restrict"), l.N, k_fast_restrict<T>, row_grid(cv.n0, cv.n1, cv.n2), 128, 0,
+                       view_x(l, cur[L]), cv, c->bnd);
     }
     LVSet<T> S;
     for (int L = 0; L < nl; L++) S.l[L] = view(lv[L]);
     PARIS_LAUNCH_N(c, kname<T>("mg_coarse_cycle"), lv[Lc].N, k_fast_coarse_cycle<T>, 1, 1024, 0, S, Lc, nl, c->bnd, nu1, nu2);
+    cur[Lc] = lv[Lc].x;
     for (int L = Lc - 1; L >= 0; L--) {
-        LV<T> v = view(lv[L]);
-        PARIS_LAUNCH_N(c, kname<T>("mg_prolong"), v.N, k_fast_prolong<T>, row_grid(v.n0, v.n1, v.n2), 128, 0, v, view(lv[L + 1]));
-        for (int s = 0; s < nu2; s++) {
-            PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, row_grid((v.n0 + 1) / 2, v.n1, v.n2), 128, 0, v, c->bnd, 1);
-            PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, row_grid((v.n0 + 1) / 2, v.n1, v.n2), 128, 0, v, c->bnd, 0);
+        const FastLevel<T>& l = lv[L];
+        if (l.x2 && nu2 > 0) {
+            T* in = cur[L];
+            for (int s = 0; s < nu2; s++) {
+                T* out = in == l.x ? l.x2 : l.x;
+                PARIS_CHECK(sweep_fused<T>(c, l, in, out, s == 0 ? cur[L + 1] : nullptr, 1));
+                in = out;
+            }
+            cur[L] = in;
+        } else {
+            LV<T> v = view_x(l, cur[L]);
+            PARIS_LAUNCH_N(c, kname<T>("mg_prolong"), v.N, k_fast_prolong<T>, row_grid(v.n0, v.n1, v.n2), 128, 0, v,
+                           view_x(lv[L + 1], cur[L + 1]));
+            for (int s = 0; s < nu2; s++) {
+                PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, row_grid((v.n0 + 1) / 2, v.n1, v.n2), 128, 0, v, c->bnd, 1);
+                PARIS_LAUNCH_N(c, kname<T>("mg_smooth"), v.N, k_fast_smooth<T>, row_grid((v.n0 + 1) / 2, v.n1, v.n2), 128, 0, v, c->bnd, 0);
+            }
         }
     }
+    *x0 = cur[0];
     return PARIS_OK;
 }
 
@@ -447,8 +514,9 @@ static int solve_dc(paris_ctx* c, const paris_solve_opts* o, paris_solve_result*
     int it = 0;
     int nu1 = o->nu1 > 0 ? o->nu1 : 2, nu2 = o->nu2 > 0 ? o->nu2 : 2;
     while (!done && it < o->maxit) {
-        PARIS_CHECK(vcycle<T>(c, nu1, nu2));
-        PARIS_LAUNCH_N(c, kname<T>("mg_correct"), c->N, k_fast_correct<T>, row_grid(c->d.nx, c->d.ny, c->d.nz), 128, 0, p, lv[0].x, c->L, 1.0);
+        T* x0;
+        PARIS_CHECK(vcycle<T>(c, nu1, nu2, &x0));
+        PARIS_LAUNCH_N(c, kname<T>("mg_correct"), c->N, k_fast_correct<T>, row_grid(c->d.nx, c->d.ny, c->d.nz), 128, 0, p, x0, c->L, 1.0);
         PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>, red_grid(c, k_fast_residual64<T>, 256), kRowBlock, 0, A, p, c->L, c->bnd, lv[0].b, (double*)nullptr,
                      c->red_part);
         PARIS_CHECK(ctx_reduce_finish(c, 3, s));
@@ -471,27 +539,27 @@ static int alloc_vec(paris_ctx* c, double** p) {
     return PARIS_OK;
 }
 
+// z = V(rT): one V-cycle on the right-hand side already in lv[0].b; returns
+// the buffer holding z and r.z
 template <typename T>
-static int precondition(paris_ctx* c, int nu1, int nu2, double* rz, double* rzold) {
-    auto& lv = levels<T>(c);
-    PARIS_LAUNCH(c, k_to_T<T>, div_up(c->N, 256), 256, 0, c->fast_r64, lv[0].b, c->N);
-    PARIS_CHECK(vcycle<T>(c, nu1, nu2));
-    PARIS_LAUNCH(c, k_pcg_takez<T>, red_grid(c, k_pcg_takez<T>, 256), 256, 0, lv[0].x, c->fast_z64, c->fast_zold64, c->fast_r64, c->N,
-                 c->red_part);
-    double s[2];
-    PARIS_CHECK(ctx_reduce_finish(c, 2, s));
-    *rz = s[0];
-    *rzold = s[1];
+static int precondition(paris_ctx* c, int nu1, int nu2, T** z, double* rz) {
+    PARIS_CHECK(vcycle<T>(c, nu1, nu2, z));
+    PARIS_LAUNCH_N(c, kname<T>("pcg_rz"), c->N, k_pcg_rz<T>, red_grid(c, k_pcg_rz<T>, 256), 256, 0, *z, c->fast_r64,
+                   c->N, c->red_part);
+    PARIS_CHECK(ctx_reduce_finish(c, 1, rz));
     return PARIS_OK;
 }
 
+// Flexible CG (Polak-Ribiere beta) preconditioned by one V-cycle, in FP64.
+// z stays in the V-cycle's output buffer until the next V-cycle starts: the
+// update kernel forms r.zold before that.
 template <typename T>
 static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* res, const double* rhs, double* p) {
-    for (double** v : {&c->fast_r64, &c->fast_d64, &c->fast_q64, &c->fast_z64, &c->fast_zold64})
-        PARIS_CHECK(alloc_vec(c, v));
+    auto& lv = levels<T>(c);
+    for (double** v : {&c->fast_r64, &c->fast_d64, &c->fast_q64}) PARIS_CHECK(alloc_vec(c, v));
     Mat64 A{c->cx, c->cy, c->cz, rhs};
     double s[3], tres, rel;
-    PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>, red_grid(c, k_fast_residual64<T>, 256), kRowBlock, 0, A, p, c->L, c->bnd, (T*)nullptr, c->fast_r64,
+    PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>, red_grid(c, k_fast_residual64<T>, 256), kRowBlock, 0, A, p, c->L, c->bnd, lv[0].b, c->fast_r64,
                  c->red_part);
     PARIS_CHECK(ctx_reduce_finish(c, 3, s));
     double bn2 = s[2];
@@ -499,12 +567,11 @@ static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result
     res->res0 = tres;
     int it = 0;
     int nu1 = o->nu1 > 0 ? o->nu1 : 2, nu2 = o->nu2 > 0 ? o->nu2 : 2;
-    double rz = 0.0, rzo = 0.0;
+    double rz = 0.0;
+    T* z = nullptr;
     if (!done) {
-        PARIS_CUDA_TRY(c, cudaMemsetAsync(c->fast_z64, 0, c->N * sizeof(double), c->stream));
-        PARIS_CHECK(precondition<T>(c, nu1, nu2, &rz, &rzo));
-        PARIS_CUDA_TRY(c, cudaMemcpyAsync(c->fast_d64, c->fast_z64, c->N * sizeof(double), cudaMemcpyDeviceToDevice,
-                                          c->stream));
+        PARIS_CHECK(precondition<T>(c, nu1, nu2, &z, &rz));
+        PARIS_LAUNCH_N(c, kname<T>("pcg_dir"), c->N, k_pcg_dir<T>, div_up(c->N, 256), 256, 0, c->fast_d64, z, 0.0, c->N);
     }
     while (!done && it < o->maxit) {
         double dq;
@@ -512,9 +579,9 @@ static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result
         PARIS_CHECK(ctx_reduce_finish(c, 1, &dq));
         if (!(dq > 0.0)) break;
         double alpha = rz / dq;
-        PARIS_LAUNCH_N(c, "pcg_update_fp64", c->N, k_pcg_update, red_grid(c, k_pcg_update, 256), kRowBlock, 0, p, c->fast_r64, c->fast_d64, c->fast_q64, alpha, c->L,
+        PARIS_LAUNCH_N(c, kname<T>("pcg_update"), c->N, k_pcg_update<T>, red_grid(c, k_pcg_update<T>, 256), kRowBlock, 0, p, c->fast_r64, c->fast_d64, c->fast_q64, lv[0].b, z, alpha, c->L,
                      c->red_part);
-        PARIS_CHECK(ctx_reduce_finish(c, 2, s));
+        PARIS_CHECK(ctx_reduce_finish(c, 3, s));
         it++;
         done = converged(o, s[0], s[1], bn2, c->N, &tres, &rel);
         if (tres != tres) {
@@ -523,13 +590,12 @@ static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result
             return PARIS_NAN_DETECTED;
         }
         if (done) break;
-        double rz_new, r_zold;
-        PARIS_CHECK(precondition<T>(c, nu1, nu2, &rz_new, &r_zold));
+        double r_zold = s[2], rz_new;
+        PARIS_CHECK(precondition<T>(c, nu1, nu2, &z, &rz_new));
         double beta = (rz_new - r_zold) / rz;   // flexible (Polak-Ribiere) form
         rz = rz_new;
-        PARIS_LAUNCH(c, k_pcg_dir, div_up(c->N, 256), 256, 0, c->fast_d64, c->fast_z64, beta, c->N);
+        PARIS_LAUNCH_N(c, kname<T>("pcg_dir"), c->N, k_pcg_dir<T>, div_up(c->N, 256), 256, 0, c->fast_d64, z, beta, c->N);
     }
-    (void)rzo;
     res->it = done ? it : o->maxit + 1;
     res->res = tres;
     res->rel_res = rel;

@@ -400,14 +400,15 @@ static int fast_coefs(paris_ctx* c) {
 // blocks, at least 8 planes per block.
 template <typename T>
 static int sweep_chunk(paris_ctx* c, const FastLevel<T>& l) {
+    using Cfg = typename SwGeo<T>::Cfg;
     static int per_sm = 0;   // resident blocks per SM (the same on every B200)
     if (!per_sm) {
-        cudaFuncSetAttribute(k_rb_sweep<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<T>());
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rb_sweep<T>, kSwThreads, sweep_smem<T>()) !=
+        cudaFuncSetAttribute(k_rb_sweep_cfg<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<T>());
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rb_sweep_cfg<Cfg>, Cfg::NT, sweep_smem<T>()) !=
                 cudaSuccess || per_sm < 1)
             per_sm = 1;
     }
-    long tiles = (long)div_up(l.n[0], kSwTX) * div_up(l.n[1], kSwTY);
+    long tiles = (long)div_up(l.n[0], kSwTX) * div_up(l.n[1], Cfg::TY);
     long nbz = (long)per_sm * c->nsm / tiles;
     long cap = l.n[2] / 8;
     if (nbz > cap) nbz = cap;
@@ -418,8 +419,9 @@ static int sweep_chunk(paris_ctx* c, const FastLevel<T>& l) {
 template <typename T>
 static int sweep_fused(paris_ctx* c, const FastLevel<T>& l, const T* xin, T* xout, const T* xc, int first) {
     int zc = sweep_chunk<T>(c, l);
-    dim3 grid(div_up(l.n[0], kSwTX), div_up(l.n[1], kSwTY), div_up(l.n[2], zc));
-    PARIS_LAUNCH_N(c, kname<T>(xin ? "mg_sweep" : "mg_sweep_zero"), l.N, k_rb_sweep<T>, grid, kSwThreads,
+    using Cfg = typename SwGeo<T>::Cfg;
+    dim3 grid(div_up(l.n[0], kSwTX), div_up(l.n[1], Cfg::TY), div_up(l.n[2], zc));
+    PARIS_LAUNCH_N(c, kname<T>(xin ? "mg_sweep" : "mg_sweep_zero"), l.N, k_rb_sweep_cfg<Cfg>, grid, Cfg::NT,
                    sweep_smem<T>(), view(l), xin, xout, xc, c->bnd, first, zc);
     return PARIS_OK;
 }

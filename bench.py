@@ -169,6 +169,8 @@ ALGO_BYTES = {
     "mg_sweep_f64": 48.0,
     "mg_sweep_zero_f32": 20.0,    # first sweep from x = 0: no iterate read
     "mg_sweep_zero_f64": 40.0,
+    "mg_sweep_lower_f32": 24.0,   # levels below the finest: the same bytes, served from L2
+    "mg_sweep_lower_f64": 48.0,
     "mg_smooth_f32": 12.0,        # half of a red-black sweep: (p 4 + 3 faces 12 + rhs 4 + p write 4)/2
     "mg_smooth_f64": 24.0,
     "mg_restrict_f32": 20.5,      # x 4 + b 4 + 3 faces 12 + coarse rhs 4/8
@@ -197,6 +199,13 @@ def gpu_step(gpu, capi, k, dt, mode, pcg):
     r = gpu.new_solver(0.0, maxit=200, mode=mode, rel_tol=REL_TOL, pcg=pcg)
     gpu.project_velocity(dt)
     return r
+
+
+# DRAM bytes per cell of the dominant kernel measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum of one 256^3 launch, 415.9 MB
+# over 16,777,216 cells): fills roofline.traffic, scaled by the cells a launch
+# processes
+NCU_DRAM_BYTES_PER_CELL = {"mg_sweep_f32": 415.9e6 / 16777216}
 
 
 def roofline(report, peak):
@@ -341,9 +350,14 @@ def run_b200(args, dist):
     peak, peak_kind = measured_peak()
 
     if args.profile_only:
+        # the steps alone form the NVTX range "paris_steps" (ncu --nvtx-include)
         gpu.profile(True)
+        gpu.sync()
+        torch.cuda.nvtx.range_push("paris_steps")
         for k in range(max(1, args.steps)):
             gpu_step(gpu, capi, k, dt, capi.MG_MIXED, args.pcg)
+        gpu.sync()
+        torch.cuda.nvtx.range_pop()
         gpu.profile(False)
         rep = gpu.profile_report()
         if dist.rank == 0:
@@ -454,7 +468,9 @@ def run_b200(args, dist):
         "mcell_updates_per_s": value * n ** 3 / 1e6,
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": top["kernel"], "achieved": top["gbs"], "peak": peak,
-                     "unit": "GB/s", "frac": top["frac"], "traffic": None,
+                     "unit": "GB/s", "frac": top["frac"],
+                     "traffic": (NCU_DRAM_BYTES_PER_CELL[top["kernel"]] * top["algo_bytes_per_launch"] /
+                                 ALGO_BYTES[top["kernel"]] if top["kernel"] in NCU_DRAM_BYTES_PER_CELL else None),
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                      "algo_bytes_per_launch": top["algo_bytes_per_launch"]},
         "kernels": rows[:12],

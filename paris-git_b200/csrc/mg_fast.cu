@@ -319,10 +319,11 @@ template <>
 const char* kname<float>(const char* base) {
     static const char* names[] = {"mg_smooth_f32", "mg_restrict_f32", "mg_prolong_f32", "mg_coarse_cycle_f32",
                                   "mg_correct_f32", "mg_residual_fp64(r32)", "mg_sweep_f32", "mg_sweep_zero_f32",
-                                  "pcg_update_fp64(z32)", "pcg_rz(z32)", "pcg_dir(z32)"};
+                                  "pcg_update_fp64(z32)", "pcg_rz(z32)", "pcg_dir(z32)", "mg_sweep_lower_f32"};
     static const char* keys[] = {"mg_smooth", "mg_restrict", "mg_prolong", "mg_coarse_cycle", "mg_correct",
-                                 "mg_residual_fp64", "mg_sweep", "mg_sweep_zero", "pcg_update", "pcg_rz", "pcg_dir"};
-    for (int q = 0; q < 11; q++)
+                                 "mg_residual_fp64", "mg_sweep", "mg_sweep_zero", "pcg_update", "pcg_rz", "pcg_dir",
+                                 "mg_sweep_lower"};
+    for (int q = 0; q < 12; q++)
         if (!strcmp(base, keys[q])) return names[q];
     return base;
 }
@@ -330,10 +331,11 @@ template <>
 const char* kname<double>(const char* base) {
     static const char* names[] = {"mg_smooth_f64", "mg_restrict_f64", "mg_prolong_f64", "mg_coarse_cycle_f64",
                                   "mg_correct_f64", "mg_residual_fp64(r64)", "mg_sweep_f64", "mg_sweep_zero_f64",
-                                  "pcg_update_fp64(z64)", "pcg_rz(z64)", "pcg_dir(z64)"};
+                                  "pcg_update_fp64(z64)", "pcg_rz(z64)", "pcg_dir(z64)", "mg_sweep_lower_f64"};
     static const char* keys[] = {"mg_smooth", "mg_restrict", "mg_prolong", "mg_coarse_cycle", "mg_correct",
-                                 "mg_residual_fp64", "mg_sweep", "mg_sweep_zero", "pcg_update", "pcg_rz", "pcg_dir"};
-    for (int q = 0; q < 11; q++)
+                                 "mg_residual_fp64", "mg_sweep", "mg_sweep_zero", "pcg_update", "pcg_rz", "pcg_dir",
+                                 "mg_sweep_lower"};
+    for (int q = 0; q < 12; q++)
         if (!strcmp(base, keys[q])) return names[q];
     return base;
 }
@@ -417,11 +419,13 @@ static int sweep_chunk(paris_ctx* c, const FastLevel<T>& l) {
 }
 
 template <typename T>
-static int sweep_fused(paris_ctx* c, const FastLevel<T>& l, const T* xin, T* xout, const T* xc, int first) {
+static int sweep_fused(paris_ctx* c, int L, const FastLevel<T>& l, const T* xin, T* xout, const T* xc, int first) {
     int zc = sweep_chunk<T>(c, l);
     using Cfg = typename SwGeo<T>::Cfg;
     dim3 grid(div_up(l.n[0], kSwTX), div_up(l.n[1], Cfg::TY), div_up(l.n[2], zc));
-    PARIS_LAUNCH_N(c, kname<T>(xin ? "mg_sweep" : "mg_sweep_zero"), l.N, k_rb_sweep_cfg<Cfg>, grid, Cfg::NT,
+        // level 0 streams from HBM; the lower levels are resident in L2
+    const char* label = L > 0 ? "mg_sweep_lower" : (xin ? "mg_sweep" : "mg_sweep_zero");
+    PARIS_LAUNCH_N(c, kname<T>(label), l.N, k_rb_sweep_cfg<Cfg>, grid, Cfg::NT,
                    sweep_smem<T>(), view(l), xin, xout, xc, c->bnd, first, zc);
     return PARIS_OK;
 }
@@ -448,7 +452,7 @@ static int vcycle(paris_ctx* c, int nu1, int nu2, T** x0) {
             const T* in = nullptr;
             T* out = l.x;
             for (int s = 0; s < nu1; s++) {
-                PARIS_CHECK(sweep_fused<T>(c, l, in, out, nullptr, 0));
+                PARIS_CHECK(sweep_fused<T>(c, L, l, in, out, nullptr, 0));
                 in = out;
                 out = out == l.x ? l.x2 : l.x;
             }
@@ -476,7 +480,7 @@ static int vcycle(paris_ctx* c, int nu1, int nu2, T** x0) {
             T* in = cur[L];
             for (int s = 0; s < nu2; s++) {
                 T* out = in == l.x ? l.x2 : l.x;
-                PARIS_CHECK(sweep_fused<T>(c, l, in, out, s == 0 ? cur[L + 1] : nullptr, 1));
+                PARIS_CHECK(sweep_fused<T>(c, L, l, in, out, s == 0 ? cur[L + 1] : nullptr, 1));
                 in = out;
             }
             cur[L] = in;

@@ -15,7 +15,9 @@
 static constexpr long kCoarseCells = 4096;   // 16^3
 static constexpr int kMaxLevels = 16;
 static constexpr int kCoarseSweeps = 8;
-static constexpr long kFusedCells = 1L << 18;   // levels of at least 64^3 cells use the fused sweep
+static constexpr long kWarpCells = 64;   // coarse levels of at most 4^3 cells run in one warp
+static constexpr long kFusedCells = 1L << 18;
+static constexpr size_t kCoarseSmemMax = 227 * 1024;   // opt-in shared memory per block   // levels of at least 64^3 cells use the fused sweep
 
 template <typename T>
 struct LV {
@@ -108,48 +110,119 @@ static inline dim3 row_grid(long n0, int n1, int n2) { return dim3(div_up(n0, 12
 
 #include "mg_sweep.cuh"
 
-// The V-cycle from level L0 down to the coarsest, in one block.
+// The V-cycle from level L0 down to the coarsest, in one block, on copies of
+// those levels in shared memory: the coefficients of every level and the
+// right-hand side of level L0 are loaded, the cycle runs, and the iterate of
+// level L0 is written back.
 template <typename T>
-__global__ void __launch_bounds__(1024) k_fast_coarse_cycle(const LVSet<T> S, int L0, int nl, const Bnd B, int nu1,
-                                                            int nu2) {
+__global__ void __launch_bounds__(512) k_fast_coarse_cycle(const LVSet<T> G, int L0, int nl, const Bnd B, int nu1,
+                                                            int nu2, int in_smem) {
     const int tid = threadIdx.x, nt = blockDim.x;
-    auto smooth = [&](const LV<T>& v, int color) {
-        int h0 = (v.n0 + 1) >> 1;
-        long tot = (long)h0 * v.n1 * v.n2;
-        for (long t = tid; t < tot; t += nt) {
-            int ih = (int)(t % h0), j = (int)((t / h0) % v.n1), k = (int)(t / ((long)h0 * v.n1));
+    extern __shared__ __align__(16) unsigned char cc_raw[];
+    __shared__ LV<T> S[kMaxLevels];   // level views, read by value in every phase
+    if (tid == 0) {
+        T* p = reinterpret_cast<T*>(cc_raw);
+        for (int L = L0; L < nl; L++) {
+            LV<T> l = G.l[L];
+            if (in_smem) {
+                T* cx = p;
+                l.cx = cx; l.cy = cx + l.N; l.cz = cx + 2 * l.N;
+                l.b = cx + 3 * l.N;
+                l.x = cx + 4 * l.N;
+                p = cx + 5 * l.N;
+            }
+            S[L] = l;
+        }
+    }
+    __syncthreads();
+    if (in_smem) {
+        for (int L = L0; L < nl; L++) {
+            const LV<T> g = G.l[L], l = S[L];
+            T* cx = const_cast<T*>(l.cx);
+            T* cy = const_cast<T*>(l.cy);
+            T* cz = const_cast<T*>(l.cz);
+            for (int t = tid; t < (int)g.N; t += nt) {
+                cx[t] = g.cx[t]; cy[t] = g.cy[t]; cz[t] = g.cz[t];
+                if (L == L0) l.b[t] = g.b[t];
+            }
+        }
+        __syncthreads();
+    }
+    // 32-bit index arithmetic throughout (levels here have at most a few
+    // thousand cells; 64-bit division would dominate every phase).  Levels of
+    // at most kWarpCells cells are worked by warp 0 alone with warp barriers.
+    const int lane = tid & 31;
+    auto smooth = [&](const LV<T> v, int color, bool warp) {
+        const int t0 = warp ? lane : tid, st = warp ? 32 : nt;
+        const int h0 = (v.n0 + 1) >> 1, hn = h0 * v.n1;
+        const int tot = hn * v.n2;
+        for (int t = t0; t < tot; t += st) {
+            int k = t / hn, r = t - k * hn;
+            int j = r / h0, ih = r - j * h0;
             int i = 2 * ih + ((j + k + color) & 1);
             if (i < v.n0) smooth_cell(v, B, i, j, k);
         }
-        __syncthreads();
+        if (warp) __syncwarp();
+        else __syncthreads();
     };
-    for (int L = L0; L < nl; L++) {
-        const LV<T>& v = S.l[L];
-        for (long t = tid; t < v.N; t += nt) v.x[t] = (T)0;
-        __syncthreads();
+    auto down = [&](int L, bool warp) {   // zero, pre-smooth and restrict level L, or solve the coarsest
+        const int t0 = warp ? lane : tid, st = warp ? 32 : nt;
+        const LV<T> v = S[L];
+        for (int t = t0; t < (int)v.N; t += st) v.x[t] = (T)0;
+        if (warp) __syncwarp();
+        else __syncthreads();
         if (L == nl - 1) {
-            for (int s = 0; s < kCoarseSweeps; s++) { smooth(v, 0); smooth(v, 1); }
-            for (int s = 0; s < kCoarseSweeps; s++) { smooth(v, 1); smooth(v, 0); }
-            break;
+            for (int s = 0; s < kCoarseSweeps; s++) { smooth(v, 0, warp); smooth(v, 1, warp); }
+            for (int s = 0; s < kCoarseSweeps; s++) { smooth(v, 1, warp); smooth(v, 0, warp); }
+            return;
         }
-        for (int s = 0; s < nu1; s++) { smooth(v, 0); smooth(v, 1); }
-        const LV<T>& c = S.l[L + 1];
-        for (long t = tid; t < c.N; t += nt) {
-            int i = (int)(t % c.n0), j = (int)((t / c.n0) % c.n1), k = (int)(t / ((long)c.n0 * c.n1));
+        for (int s = 0; s < nu1; s++) { smooth(v, 0, warp); smooth(v, 1, warp); }
+        const LV<T> c = S[L + 1];
+        const int cn = c.n0 * c.n1;
+        for (int t = t0; t < (int)c.N; t += st) {
+            int k = t / cn, r = t - k * cn;
+            int j = r / c.n0, i = r - j * c.n0;
             restrict_cell(v, c, B, i, j, k);
         }
-        __syncthreads();
-    }
-    for (int L = nl - 2; L >= L0; L--) {
-        const LV<T>& v = S.l[L];
-        const LV<T>& c = S.l[L + 1];
-        for (long t = tid; t < v.N; t += nt) {
-            int i = (int)(t % v.n0), j = (int)((t / v.n0) % v.n1), k = (int)(t / ((long)v.n0 * v.n1));
+        if (warp) __syncwarp();
+        else __syncthreads();
+    };
+    auto up = [&](int L, bool warp) {     // prolong into level L and post-smooth it
+        const int t0 = warp ? lane : tid, st = warp ? 32 : nt;
+        const LV<T> v = S[L], c = S[L + 1];
+        const int fn = v.n0 * v.n1;
+        for (int t = t0; t < (int)v.N; t += st) {
+            int k = t / fn, r = t - k * fn;
+            int j = r / v.n0, i = r - j * v.n0;
             v.x[t] += c.x[cidx(c.n0, c.n1, i >> 1, j >> 1, k >> 1)];
         }
+        if (warp) __syncwarp();
+        else __syncthreads();
+        for (int s = 0; s < nu2; s++) { smooth(v, 1, warp); smooth(v, 0, warp); }
+    };
+    int Lw = L0;   // first level worked by warp 0
+    while (Lw < nl && S[Lw].N > kWarpCells) Lw++;
+    for (int L = L0; L < Lw; L++) down(L, false);
+    if (Lw < nl) {
+        if (tid < 32) {
+            for (int L = Lw; L < nl; L++) down(L, true);
+            for (int L = nl - 2; L >= Lw; L--) up(L, true);
+        }
         __syncthreads();
-        for (int s = 0; s < nu2; s++) { smooth(v, 1); smooth(v, 0); }
     }
+    for (int L = min(Lw, nl - 1) - 1; L >= L0; L--) up(L, false);
+    if (in_smem) {
+        const LV<T> g = G.l[L0], l = S[L0];
+        for (int t = tid; t < (int)g.N; t += nt) g.x[t] = l.x[t];
+    }
+}
+
+// shared memory of k_fast_coarse_cycle: five arrays per level from L0 down
+template <typename T>
+static size_t coarse_smem(const std::vector<FastLevel<T>>& lv, int L0) {
+    size_t n = 0;
+    for (int L = L0; L < (int)lv.size(); L++) n += 5 * (size_t)lv[L].N;
+    return n * sizeof(T);
 }
 
 // level-0 coefficients from the FP64 compact matrix
@@ -399,20 +472,20 @@ static int fast_coefs(paris_ctx* c) {
 }
 
 // Planes per block of the fused sweep: enough blocks for one wave of resident
-// blocks, at least 8 planes per block.
+// blocks, at least 4 planes per block.
 template <typename T>
 static int sweep_chunk(paris_ctx* c, const FastLevel<T>& l) {
     using Cfg = typename SwGeo<T>::Cfg;
     static int per_sm = 0;   // resident blocks per SM (the same on every B200)
     if (!per_sm) {
-        cudaFuncSetAttribute(k_rb_sweep_cfg<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<T>());
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rb_sweep_cfg<Cfg>, Cfg::NT, sweep_smem<T>()) !=
+        cudaFuncSetAttribute(k_rb_sweep2_cfg<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<T>());
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rb_sweep2_cfg<Cfg>, Cfg::NT, sweep_smem<T>()) !=
                 cudaSuccess || per_sm < 1)
             per_sm = 1;
     }
     long tiles = (long)div_up(l.n[0], kSwTX) * div_up(l.n[1], Cfg::TY);
     long nbz = (long)per_sm * c->nsm / tiles;
-    long cap = l.n[2] / 8;
+    long cap = l.n[2] / 4;
     if (nbz > cap) nbz = cap;
     if (nbz < 1) nbz = 1;
     return (int)div_up(l.n[2], nbz);
@@ -425,7 +498,7 @@ static int sweep_fused(paris_ctx* c, int L, const FastLevel<T>& l, const T* xin,
     dim3 grid(div_up(l.n[0], kSwTX), div_up(l.n[1], Cfg::TY), div_up(l.n[2], zc));
         // level 0 streams from HBM; the lower levels are resident in L2
     const char* label = L > 0 ? "mg_sweep_lower" : (xin ? "mg_sweep" : "mg_sweep_zero");
-    PARIS_LAUNCH_N(c, kname<T>(label), l.N, k_rb_sweep_cfg<Cfg>, grid, Cfg::NT,
+    PARIS_LAUNCH_N(c, kname<T>(label), l.N, k_rb_sweep2_cfg<Cfg>, grid, Cfg::NT,
                    sweep_smem<T>(), view(l), xin, xout, xc, c->bnd, first, zc);
     return PARIS_OK;
 }
@@ -472,7 +545,18 @@ static int vcycle(paris_ctx* c, int nu1, int nu2, T** x0) {
     }
     LVSet<T> S;
     for (int L = 0; L < nl; L++) S.l[L] = view(lv[L]);
-    PARIS_LAUNCH_N(c, kname<T>("mg_coarse_cycle"), lv[Lc].N, k_fast_coarse_cycle<T>, 1, 1024, 0, S, Lc, nl, c->bnd, nu1, nu2);
+    // the levels run in shared memory when they fit (always for L0 <= 16^3)
+    size_t csm = coarse_smem(lv, Lc);
+    const int in_smem = csm <= kCoarseSmemMax ? 1 : 0;
+    if (!in_smem) csm = 0;
+    static size_t csm_set = 0;   // opt-in size set for this instantiation
+    if (csm > csm_set) {
+        PARIS_CUDA_TRY(c, cudaFuncSetAttribute(k_fast_coarse_cycle<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)csm));
+        csm_set = csm;
+    }
+    PARIS_LAUNCH_N(c, kname<T>("mg_coarse_cycle"), lv[Lc].N, k_fast_coarse_cycle<T>, 1, 512, csm, S, Lc, nl, c->bnd, nu1, nu2,
+                   in_smem);
     cur[Lc] = lv[Lc].x;
     for (int L = Lc - 1; L >= 0; L--) {
         const FastLevel<T>& l = lv[L];

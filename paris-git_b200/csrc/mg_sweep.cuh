@@ -3,10 +3,11 @@
 //
 // One full sweep (colour F = `first`, then the other colour S) in one pass
 // over memory.  A block owns a kSwTX x TY column of cells and marches up a
-// chunk of planes with a wavefront:
-//   step kk:  F at plane kk on the tile plus a one-cell ring (from the old
-//             iterate), then S at plane kk-1 on the tile (from the new F
-//             values of planes kk-2..kk); plane kk-1 is then final.
+// chunk of planes with a wavefront, two planes per step:
+//   step (f0, f1 = f0+1):  F at planes f0 and f1 on the tile plus a one-cell
+//             ring (from the old iterate), then S at planes f0-1 and f0 on the
+//             tile (from the new F values of the planes around them); planes
+//             f0-1 and f0 are then final and stored.
 // Planes of the iterate (tile + two-cell ring) and of the coefficients are
 // staged in shared memory with 16-byte cp.async, D steps ahead of their use,
 // so that enough bytes are in flight per SM to cover the HBM latency; each
@@ -15,8 +16,8 @@
 // place, so blocks never see each other's new values and the sweep computes
 // exactly the two colour passes of k_fast_smooth.  With `xc`, the coarse-grid
 // correction (injection from the level below) is added to the iterate as it
-// arrives.  Ring-buffer slots rotate with the step; the per-step work outside
-// the point updates is a handful of integer operations per thread.
+// arrives, fetched into registers one step ahead.  Ring-buffer slots rotate
+// with the step.
 //
 // Requirements (checked by the host): n0 a multiple of 16 / sizeof(T) and all
 // dimensions even (true of every level above the coarsest).
@@ -36,46 +37,18 @@ template <typename T>
 struct SwGeo;
 template <>
 struct SwGeo<float> {
-    using Cfg = SwCfg<float, 16, 2, 320, 3>;   // 512 cells per plane step, three blocks per SM
+    using Cfg = SwCfg<float, 16, 1, 320, 2>;   // 32x16 tiles, two planes staged ahead, two blocks per SM
 };
 template <>
 struct SwGeo<double> {
-    using Cfg = SwCfg<double, 8, 3, 256, 2>;   // two blocks per SM within shared memory
+    using Cfg = SwCfg<double, 8, 1, 256, 2>;   // 32x8 tiles: two blocks per SM within shared memory
 };
 
 template <class C>
-struct Sw {
-    using T = typename C::type;
-    static constexpr int NT = C::NT;
-    static constexpr int TY = C::TY;
-    static constexpr int D = C::D;                    // planes staged ahead of use
-    static constexpr int RX = kSwTX + 8;              // region x0-4 .. x0+TX+3 (16-byte aligned rows)
-    static constexpr int RY = TY + 4;                 // y0-2 .. y0+TY+1
-    static constexpr int RP = RX * RY;
-    // live planes: iterate kk-2..kk+1, coefficients kk-1..kk, cz kk-2..kk,
-    // each plus D in flight
-    static constexpr int XS = D + 4, CS = D + 2, ZS = D + 3;
-    static constexpr int SLOTS = XS + 3 * CS + ZS;
-    static constexpr int FROW = (kSwTX + 2) / 2;      // F cells per ring row
-    static constexpr int FCELLS = FROW * (TY + 2);
-    static constexpr int FPER = (FCELLS + NT - 1) / NT;
-    static constexpr int SCELLS = kSwTX / 2 * TY;     // S cells (= output pairs) of the tile
-    static constexpr int VEC = 16 / sizeof(T);
-    static constexpr int RXC = RX / VEC;
-    static constexpr int CH = RXC * RY;               // 16-byte chunks per array plane
-    static constexpr int CPER = (RP + NT - 1) / NT;
-    static constexpr uint32_t SLOT_BYTES = sizeof(T) * RP;
-    static_assert(SCELLS <= NT, "one output pair per thread");
-};
-
-template <class C>
-static constexpr size_t sweep_smem_cfg() {
-    return sizeof(typename C::type) * (size_t)Sw<C>::RP * Sw<C>::SLOTS;
-}
-
+static constexpr size_t sweep2_smem_cfg();
 template <typename T>
 static constexpr size_t sweep_smem() {
-    return sweep_smem_cfg<typename SwGeo<T>::Cfg>();
+    return sweep2_smem_cfg<typename SwGeo<T>::Cfg>();
 }
 
 template <typename T>
@@ -109,19 +82,47 @@ __device__ inline int sw_add(int s, int d, int S) {
     return s >= S ? s - S : (s < 0 ? s + S : s);
 }
 
+// ---------------------------------------------------------------------------
+// Step s works on f0 = z0-1+2s and f1 = f0+1; the barriers and the ring
+// bookkeeping of a step are shared by two planes, and each thread has two
+// independent updates per phase.  Live planes: iterate f0-2..f1+1,
+// coefficients f0-1..f1, cz f0-2..f1, each plus 2D staged ahead.
+template <class C>
+struct Sw2 {
+    using T = typename C::type;
+    static constexpr int NT = C::NT, TY = C::TY, D = C::D;
+    static constexpr int RX = kSwTX + 8, RY = TY + 4, RP = RX * RY;
+    static constexpr int XS = 5 + 2 * D, CS = 3 + 2 * D, ZS = 4 + 2 * D;
+    static constexpr int SLOTS = XS + 3 * CS + ZS;
+    static constexpr int FROW = (kSwTX + 2) / 2;
+    static constexpr int FCELLS = FROW * (TY + 2);
+    static constexpr int FPER = (FCELLS + NT - 1) / NT;
+    static constexpr int SCELLS = kSwTX / 2 * TY;
+    static constexpr int VEC = 16 / sizeof(T);
+    static constexpr int RXC = RX / VEC;
+    static constexpr int CH = RXC * RY;
+    static constexpr int CPER = (RP + NT - 1) / NT;
+    static constexpr uint32_t SLOT_BYTES = sizeof(T) * RP;
+    static_assert(SCELLS <= NT, "one output pair per thread");
+    static_assert(CH <= NT, "one chunk of each array per thread");
+};
+
+template <class C>
+static constexpr size_t sweep2_smem_cfg() {
+    return sizeof(typename C::type) * (size_t)Sw2<C>::RP * Sw2<C>::SLOTS;
+}
+
 template <class C>
 __global__ void __launch_bounds__(C::NT, C::MINB)
-    k_rb_sweep_cfg(const LV<typename C::type> v, const typename C::type* __restrict__ xin,
-                   typename C::type* __restrict__ xout, const typename C::type* __restrict__ xc, const Bnd B, int first,
-                   int zc) {
+    k_rb_sweep2_cfg(const LV<typename C::type> v, const typename C::type* __restrict__ xin,
+                    typename C::type* __restrict__ xout, const typename C::type* __restrict__ xc, const Bnd B,
+                    int first, int zc) {
     using T = typename C::type;
-    using G = Sw<C>;
+    using G = Sw2<C>;
     constexpr int NT = G::NT;
     constexpr int RX = G::RX, RP = G::RP, TY = G::TY, VEC = G::VEC;
-    static_assert(G::CH <= NT, "one chunk of each array per thread");
     extern __shared__ __align__(16) unsigned char sw_raw[];
     T* const sm = reinterpret_cast<T*>(sw_raw);
-    // rings: iterate (XS slots), cx, cy, b (CS slots each), cz (ZS slots)
     T* const rx_ = sm;
     T* const rcx = sm + G::XS * RP;
     T* const rcy = rcx + G::CS * RP;
@@ -133,10 +134,9 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
     const long plane = (long)n0 * n1;
     const int x0 = blockIdx.x * kSwTX, y0 = blockIdx.y * TY;
     const int z0 = blockIdx.z * zc, z1 = min(z0 + zc, n2);
-    const int kb = z0 - 2;   // first staged plane: slot of plane k = (k - kb) mod ring size
+    const int kb = z0 - 2;   // slot of plane k in a ring of S slots: (k - kb) % S
+    auto slot = [&](int k, int S) { return (k - kb) % S; };
 
-    // the 16-byte chunk this thread stages of every array plane: its byte
-    // offset within a slot and its in-plane element offset (-1: zero fill)
     const bool ld = tid < G::CH;
     uint32_t creg = 0;
     long cin = -1;
@@ -156,27 +156,21 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
         bool ok = base != nullptr && cin >= 0 && gk >= 0;
         cp_async16(sa, ok ? base + cin + plane * gk : v.b, ok ? 16 : 0);
     };
-    // issue the loads of iterate plane kx into slot sx (if kx_on) and of the
-    // coefficients of plane kc into slots sc (cx, cy, b) and sz (cz)
-    // (if kc_on; cz alone if cz_only)
-    auto stage = [&](int kx, int sx, bool kx_on, int kc, int sc, int sz, bool kc_on, bool cz_only) {
-        if (!ld) return;
-        if (kx_on) copy(s_x + G::SLOT_BYTES * sx, xin, sw_wrap(kx, n2, B.per[2]));
-        if (kc_on) {
-            const int gk = sw_wrap(kc, n2, B.per[2]);
-            if (!cz_only) {
-                const uint32_t oc = G::SLOT_BYTES * sc;
-                copy(s_cx + oc, v.cx, gk);
-                copy(s_cy + oc, v.cy, gk);
-                copy(s_b + oc, v.b, gk);
-            }
-            copy(s_cz + G::SLOT_BYTES * sz, v.cz, gk);
+    auto stage_x = [&](int k) {
+        if (ld && k <= z1 + 1) copy(s_x + G::SLOT_BYTES * slot(k, G::XS), xin, sw_wrap(k, n2, B.per[2]));
+    };
+    auto stage_c = [&](int k, bool cz_only) {
+        if (!ld || k > z1) return;
+        const int gk = sw_wrap(k, n2, B.per[2]);
+        if (!cz_only) {
+            const uint32_t oc = G::SLOT_BYTES * slot(k, G::CS);
+            copy(s_cx + oc, v.cx, gk);
+            copy(s_cy + oc, v.cy, gk);
+            copy(s_b + oc, v.b, gk);
         }
+        copy(s_cz + G::SLOT_BYTES * slot(k, G::ZS), v.cz, gk);
     };
 
-    // F cells of this thread (FPER per plane): region index of the even
-    // candidate column, parity of (x0-1, row) against `first`, and which of
-    // the two candidate columns is a real cell (bit 0: even, bit 1: odd)
     int fr0[G::FPER], fpar[G::FPER], fok[G::FPER];
 #pragma unroll
     for (int q = 0; q < G::FPER; q++) {
@@ -195,25 +189,21 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
             }
         }
     }
-    // the output pair of this thread: tile columns 2c, 2c+1 of tile row sry
     const int sry = 2 + tid / (kSwTX / 2);
     const int scol = tid % (kSwTX / 2);
     const int sgi = x0 + 2 * scol, sgj = y0 + sry - 2;
     const bool s_out = tid < G::SCELLS && sgi < n0 && sgj < n1;
-    const int srl = 4 + 2 * scol + RX * sry;           // left cell of the pair
+    const int srl = 4 + 2 * scol + RX * sry;
     const int spar = (sgj + first) & 1;
 
-    // coarse-grid correction: parents of the iterate elements of this thread
-    // (in-plane offset, -1 outside a wall), fetched into registers one step
-    // before the plane is added to
     int coff[G::CPER];
-    T cval[G::CPER];
+    T cval[2][G::CPER];
     const int cn0 = n0 >> 1;
     const long cplane = (long)cn0 * (n1 >> 1);
 #pragma unroll
     for (int q = 0; q < G::CPER; q++) {
         coff[q] = -1;
-        cval[q] = (T)0;
+        cval[0][q] = cval[1][q] = (T)0;
         int e = tid + q * NT;
         if (xc && e < RP) {
             int gi = sw_wrap(x0 - 4 + e % RX, n0, B.per[0]);
@@ -221,23 +211,20 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
             if (gi >= 0 && gj >= 0) coff[q] = (gi >> 1) + cn0 * (gj >> 1);
         }
     }
-    auto fetch_coarse = [&](int k) {
+    auto fetch_coarse = [&](int h, int k) {
         int gk = sw_wrap(k, n2, B.per[2]);
         const T* cp = xc + cplane * (gk >> 1);
 #pragma unroll
-        for (int q = 0; q < G::CPER; q++) cval[q] = (gk >= 0 && coff[q] >= 0) ? cp[coff[q]] : (T)0;
+        for (int q = 0; q < G::CPER; q++) cval[h][q] = (gk >= 0 && coff[q] >= 0) ? cp[coff[q]] : (T)0;
     };
-    auto add_coarse = [&](int slot) {
-        T* d = rx_ + slot * RP;
+    auto add_coarse = [&](int h, int k) {
+        T* d = rx_ + slot(k, G::XS) * RP;
 #pragma unroll
         for (int q = 0; q < G::CPER; q++) {
             int e = tid + q * NT;
-            if (e < RP) d[e] += cval[q];
+            if (e < RP) d[e] += cval[h][q];
         }
     };
-
-    // point update of region cell r in plane xk (formula and operation order
-    // of smooth_cell)
     auto update = [&](int r, T* xk, const T* xm, const T* xp, const T* cxk, const T* cyk, const T* bk,
                       const T* czk, const T* czm) {
         T a1 = cxk[r - 1], a2 = cxk[r], a3 = cyk[r - RX], a4 = cyk[r], a5 = czm[r], a6 = czk[r];
@@ -245,79 +232,89 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
         T s = a1 * xk[r - 1] + a2 * xk[r + 1] + a3 * xk[r - RX] + a4 * xk[r + RX] + a5 * xm[r] + a6 * xp[r] + bk[r];
         if (d > (T)0) xk[r] = s / d;
     };
+    // F at plane k (tile + ring) and S at plane k (tile) with its output; the
+    // slot pointers of the planes involved are passed in
+    auto f_at = [&](int k, T* xk, const T* xm, const T* xp, const T* cxk, const T* cyk, const T* bk, const T* czk,
+                    const T* czm) {
+        if (sw_wrap(k, n2, B.per[2]) < 0) return;
+#pragma unroll
+        for (int q = 0; q < G::FPER; q++) {
+            if (fr0[q] < 0) continue;
+            const int off = fpar[q] ^ (k & 1);
+            if ((fok[q] >> off) & 1) update(fr0[q] + off, xk, xm, xp, cxk, cyk, bk, czk, czm);
+        }
+    };
+    auto s_at = [&](int k, T* xk, const T* xm, const T* xp, const T* cxk, const T* cyk, const T* bk, const T* czk,
+                    const T* czm) {
+        if (k < z0 || k >= z1 || !s_out) return;
+        const int rS = srl + ((spar ^ (k & 1)) ? 0 : 1);
+        update(rS, xk, xm, xp, cxk, cyk, bk, czk, czm);
+        using V2 = typename SwVec<T>::V2;
+        V2 pr;
+        pr.x = xk[srl];
+        pr.y = xk[srl + 1];
+        *reinterpret_cast<V2*>(xout + sgi + (long)n0 * sgj + plane * k) = pr;
+    };
 
-    // prologue.  Group 0: iterate planes z0-2..z0 (slots 0..2), coefficients
-    // of plane z0-1 (slot 1), cz of plane z0-2 (slot 0).  Groups 1..D-1:
-    // iterate plane z0+j and coefficients of plane z0-1+j, as a step issues.
-    stage(z0 - 2, 0, true, z0 - 2, 0, 0, true, true);
-    stage(z0 - 1, 1, true, z0 - 1, 1, 1, true, false);
-    stage(z0, 2, true, 0, 0, 0, false, false);
+    // prologue: group 0 = iterate z0-2..z0+1, coefficients z0-1, z0, cz z0-2;
+    // group g (1..D-1) = iterate z0+2g, z0+2g+1 and coefficients z0-1+2g, z0+2g
+    for (int k = z0 - 2; k <= z0 + 1; k++) stage_x(k);
+    stage_c(z0 - 2, true);
+    stage_c(z0 - 1, false);
+    stage_c(z0, false);
     cp_async_commit();
 #pragma unroll
-    for (int j = 1; j < G::D; j++) {
-        stage(z0 + j, (j + 2) % G::XS, z0 + j <= z1 + 1, z0 - 1 + j, (j + 1) % G::CS, (j + 1) % G::ZS, z0 - 1 + j <= z1,
-              false);
+    for (int g = 1; g < G::D; g++) {
+        stage_x(z0 + 2 * g);
+        stage_x(z0 + 2 * g + 1);
+        stage_c(z0 - 1 + 2 * g, false);
+        stage_c(z0 + 2 * g, false);
         cp_async_commit();
     }
-
-    // ring positions of plane kk-1 in the iterate, coefficient and cz rings
-    int xs1 = 0, cs1 = 0, zs1 = 0;
-    for (int kk = z0 - 1; kk <= z1; kk++) {
-        cp_async_wait_newest<G::D - 1>();   // the group carrying iterate kk+1 and coefficients kk
+    // ring positions of plane f0-2 (iterate, cz) and f0-1 (coefficients),
+    // advanced by two each step (plane z0-2 sits in slot 0 of every ring)
+    int xb = G::XS - 1, cb = 0, zb = G::ZS - 1;
+    for (int f0 = z0 - 1; f0 <= z1; f0 += 2) {
+        cp_async_wait_newest<G::D - 1>();
         __syncthreads();
-        // iterate plane kk+1+D and coefficients of plane kk+D into the slots
-        // freed by planes kk-3 (iterate, cz) and kk-2 (coefficients)
-        stage(kk + 1 + G::D, sw_add(xs1, -2, G::XS), kk + 1 + G::D <= z1 + 1, kk + G::D, sw_add(cs1, -1, G::CS),
-              sw_add(zs1, -2, G::ZS), kk + G::D <= z1, false);
+        stage_x(f0 + 2 * G::D + 1);
+        stage_x(f0 + 2 * G::D + 2);
+        stage_c(f0 + 2 * G::D, false);
+        stage_c(f0 + 2 * G::D + 1, false);
         cp_async_commit();
-        const int xk0 = sw_next(xs1, G::XS), xkp = sw_add(xs1, 2, G::XS);
-        if (xc) {   // the planes that arrived: group 0's, then one per step
-            if (kk == z0 - 1) {
-                for (int k = 0; k < 3; k++) {
-                    fetch_coarse(z0 - 2 + k);
-                    add_coarse(k);
+        if (xc) {   // the iterate planes that arrived: group 0's, then two per step
+            if (f0 == z0 - 1) {
+                for (int k = z0 - 2; k <= z0 + 1; k++) {
+                    fetch_coarse(0, k);
+                    add_coarse(0, k);
                 }
             } else {
-                add_coarse(xkp);
+                if (f0 + 1 <= z1 + 1) add_coarse(0, f0 + 1);   // planes above z1+1 are never staged
+                if (f0 + 2 <= z1 + 1) add_coarse(1, f0 + 2);
             }
-            fetch_coarse(kk + 2);   // for the plane that arrives next step
+            fetch_coarse(0, f0 + 3);
+            fetch_coarse(1, f0 + 4);
             __syncthreads();
         }
-        T* const xm1 = rx_ + xs1 * RP;       // plane kk-1
-        T* const xk = rx_ + xk0 * RP;        // plane kk
-        // F at plane kk on the tile + ring
-        if (sw_wrap(kk, n2, B.per[2]) >= 0) {
-            const int ck = sw_next(cs1, G::CS);
-            const T* cxk = rcx + ck * RP;
-            const T* cyk = rcy + ck * RP;
-            const T* bk = rb + ck * RP;
-            const T* czk = rcz + sw_next(zs1, G::ZS) * RP;
-            const T* czm = rcz + zs1 * RP;
-            const T* xp = rx_ + xkp * RP;
-#pragma unroll
-            for (int q = 0; q < G::FPER; q++) {
-                if (fr0[q] < 0) continue;
-                const int off = fpar[q] ^ (kk & 1);
-                if ((fok[q] >> off) & 1) update(fr0[q] + off, xk, xm1, xp, cxk, cyk, bk, czk, czm);
-            }
-        }
+        // iterate planes f0-2 .. f0+2, coefficient planes f0-1 .. f0+1, cz f0-2 .. f0+1
+        T* const xm2 = rx_ + xb * RP;
+        T* const xm1 = rx_ + sw_add(xb, 1, G::XS) * RP;
+        T* const x0p = rx_ + sw_add(xb, 2, G::XS) * RP;
+        T* const x1p = rx_ + sw_add(xb, 3, G::XS) * RP;
+        T* const x2p = rx_ + sw_add(xb, 4, G::XS) * RP;
+        const int c0 = sw_add(cb, 1, G::CS), c1 = sw_add(cb, 2, G::CS);
+        const T* const zm2 = rcz + zb * RP;
+        const T* const zm1 = rcz + sw_add(zb, 1, G::ZS) * RP;
+        const T* const z0p = rcz + sw_add(zb, 2, G::ZS) * RP;
+        const T* const z1p = rcz + sw_add(zb, 3, G::ZS) * RP;
+        f_at(f0, x0p, xm1, x1p, rcx + c0 * RP, rcy + c0 * RP, rb + c0 * RP, z0p, zm1);
+        if (f0 + 1 <= z1) f_at(f0 + 1, x1p, x0p, x2p, rcx + c1 * RP, rcy + c1 * RP, rb + c1 * RP, z1p, z0p);
         __syncthreads();
-        // S at plane kk-1 on the tile; store the finished pair of plane kk-1
-        const int ks = kk - 1;
-        if (ks >= z0 && s_out) {
-            const T* xm2 = rx_ + sw_add(xs1, -1, G::XS) * RP;   // plane kk-2
-            const int rS = srl + ((spar ^ (ks & 1)) ? 0 : 1);
-            update(rS, xm1, xm2, xk, rcx + cs1 * RP, rcy + cs1 * RP, rb + cs1 * RP, rcz + zs1 * RP,
-                   rcz + sw_add(zs1, -1, G::ZS) * RP);
-            using V2 = typename SwVec<T>::V2;
-            V2 pr;
-            pr.x = xm1[srl];
-            pr.y = xm1[srl + 1];
-            *reinterpret_cast<V2*>(xout + sgi + (long)n0 * sgj + plane * ks) = pr;
-        }
-        xs1 = xk0;
-        cs1 = sw_next(cs1, G::CS);
-        zs1 = sw_next(zs1, G::ZS);
+        s_at(f0 - 1, xm1, xm2, x0p, rcx + cb * RP, rcy + cb * RP, rb + cb * RP, zm1, zm2);
+        s_at(f0, x0p, xm1, x1p, rcx + c0 * RP, rcy + c0 * RP, rb + c0 * RP, z0p, zm1);
+        xb = sw_add(xb, 2, G::XS);
+        cb = sw_add(cb, 2, G::CS);
+        zb = sw_add(zb, 2, G::ZS);
     }
     cp_async_wait_all_groups();
 }

@@ -35,7 +35,7 @@ struct Metric {
 // coefficients A2, A4, A6 and the right-hand side A8 of every cell, plus the
 // checks of check_and_debug_Poisson / check_poisson_setup.
 // part slots: 0 = sum A8, 1 = number of cells failing a check
-__global__ void k_setup_poisson(const double* __restrict__ u, const double* __restrict__ v,
+__global__ void __launch_bounds__(256, 3) k_setup_poisson(const double* __restrict__ u, const double* __restrict__ v,
                                 const double* __restrict__ w, const double* __restrict__ rho,
                                 double* __restrict__ cx, double* __restrict__ cy, double* __restrict__ cz,
                                 double* __restrict__ rhs, const Layout L, const Bnd B, const Metric M,

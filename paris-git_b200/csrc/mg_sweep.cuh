@@ -137,38 +137,55 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
     const int kb = z0 - 2;   // slot of plane k in a ring of S slots: (k - kb) % S
     auto slot = [&](int k, int S) { return (k - kb) % S; };
 
+    // the 16-byte chunk this thread stages of every array plane: shared
+    // address in slot 0 of each ring and global address in plane 0 (valid
+    // only when the chunk lies in the domain or its periodic image)
     const bool ld = tid < G::CH;
     uint32_t creg = 0;
-    long cin = -1;
+    long cin = 0;
+    bool cok = false;
     if (ld) {
         int ry = tid / G::RXC, cxq = tid % G::RXC;
         int gi = sw_wrap(x0 - 4 + VEC * cxq, n0, B.per[0]);
         int gj = sw_wrap(y0 - 2 + ry, n1, B.per[1]);
         creg = (uint32_t)(sizeof(T) * (ry * RX + VEC * cxq));
-        if (gi >= 0 && gj >= 0) cin = gi + (long)n0 * gj;
+        if (gi >= 0 && gj >= 0) {
+            cin = gi + (long)n0 * gj;
+            cok = true;
+        }
     }
     const uint32_t s_x = (uint32_t)__cvta_generic_to_shared(rx_) + creg;
     const uint32_t s_cx = (uint32_t)__cvta_generic_to_shared(rcx) + creg;
     const uint32_t s_cy = (uint32_t)__cvta_generic_to_shared(rcy) + creg;
     const uint32_t s_b = (uint32_t)__cvta_generic_to_shared(rb) + creg;
     const uint32_t s_cz = (uint32_t)__cvta_generic_to_shared(rcz) + creg;
-    auto copy = [&](uint32_t sa, const T* base, int gk) {
-        bool ok = base != nullptr && cin >= 0 && gk >= 0;
-        cp_async16(sa, ok ? base + cin + plane * gk : v.b, ok ? 16 : 0);
+    const T* const g_x = xin ? xin + cin : v.b;
+    const T* const g_cx = v.cx + cin;
+    const T* const g_cy = v.cy + cin;
+    const T* const g_b = v.b + cin;
+    const T* const g_cz = v.cz + cin;
+    const bool xok = cok && xin != nullptr;
+    // iterate plane k into slot sx (k above z1+1 is never needed)
+    auto stage_x = [&](int k, int sx) {
+        if (!ld || k > z1 + 1) return;
+        const int gk = sw_wrap(k, n2, B.per[2]);
+        const bool ok = xok && gk >= 0;
+        cp_async16(s_x + G::SLOT_BYTES * sx, ok ? g_x + plane * gk : v.b, ok ? 16 : 0);
     };
-    auto stage_x = [&](int k) {
-        if (ld && k <= z1 + 1) copy(s_x + G::SLOT_BYTES * slot(k, G::XS), xin, sw_wrap(k, n2, B.per[2]));
-    };
-    auto stage_c = [&](int k, bool cz_only) {
+    // coefficients of plane k into slot sc (cx, cy, b) and sz (cz), or cz alone
+    auto stage_c = [&](int k, int sc, int sz, bool cz_only) {
         if (!ld || k > z1) return;
         const int gk = sw_wrap(k, n2, B.per[2]);
+        const bool ok = cok && gk >= 0;
+        const long po = ok ? plane * gk : 0;
+        const int nb = ok ? 16 : 0;
         if (!cz_only) {
-            const uint32_t oc = G::SLOT_BYTES * slot(k, G::CS);
-            copy(s_cx + oc, v.cx, gk);
-            copy(s_cy + oc, v.cy, gk);
-            copy(s_b + oc, v.b, gk);
+            const uint32_t oc = G::SLOT_BYTES * sc;
+            cp_async16(s_cx + oc, ok ? g_cx + po : v.b, nb);
+            cp_async16(s_cy + oc, ok ? g_cy + po : v.b, nb);
+            cp_async16(s_b + oc, ok ? g_b + po : v.b, nb);
         }
-        copy(s_cz + G::SLOT_BYTES * slot(k, G::ZS), v.cz, gk);
+        cp_async16(s_cz + G::SLOT_BYTES * sz, ok ? g_cz + po : v.b, nb);
     };
 
     int fr0[G::FPER], fpar[G::FPER], fok[G::FPER];
@@ -258,17 +275,17 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
 
     // prologue: group 0 = iterate z0-2..z0+1, coefficients z0-1, z0, cz z0-2;
     // group g (1..D-1) = iterate z0+2g, z0+2g+1 and coefficients z0-1+2g, z0+2g
-    for (int k = z0 - 2; k <= z0 + 1; k++) stage_x(k);
-    stage_c(z0 - 2, true);
-    stage_c(z0 - 1, false);
-    stage_c(z0, false);
+    for (int k = z0 - 2; k <= z0 + 1; k++) stage_x(k, slot(k, G::XS));
+    stage_c(z0 - 2, 0, 0, true);
+    stage_c(z0 - 1, 1, 1, false);
+    stage_c(z0, 2, 2, false);
     cp_async_commit();
 #pragma unroll
     for (int g = 1; g < G::D; g++) {
-        stage_x(z0 + 2 * g);
-        stage_x(z0 + 2 * g + 1);
-        stage_c(z0 - 1 + 2 * g, false);
-        stage_c(z0 + 2 * g, false);
+        stage_x(z0 + 2 * g, slot(z0 + 2 * g, G::XS));
+        stage_x(z0 + 2 * g + 1, slot(z0 + 2 * g + 1, G::XS));
+        stage_c(z0 - 1 + 2 * g, slot(z0 - 1 + 2 * g, G::CS), slot(z0 - 1 + 2 * g, G::ZS), false);
+        stage_c(z0 + 2 * g, slot(z0 + 2 * g, G::CS), slot(z0 + 2 * g, G::ZS), false);
         cp_async_commit();
     }
     // ring positions of plane f0-2 (iterate, cz) and f0-1 (coefficients),
@@ -277,10 +294,12 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
     for (int f0 = z0 - 1; f0 <= z1; f0 += 2) {
         cp_async_wait_newest<G::D - 1>();
         __syncthreads();
-        stage_x(f0 + 2 * G::D + 1);
-        stage_x(f0 + 2 * G::D + 2);
-        stage_c(f0 + 2 * G::D, false);
-        stage_c(f0 + 2 * G::D + 1, false);
+        // slots of planes f0+2D+1, f0+2D+2 (iterate) and f0+2D, f0+2D+1
+        // (coefficients): those of planes f0-4, f0-3 and f0-3, f0-2
+        stage_x(f0 + 2 * G::D + 1, sw_add(xb, -2, G::XS));
+        stage_x(f0 + 2 * G::D + 2, sw_add(xb, -1, G::XS));
+        stage_c(f0 + 2 * G::D, sw_add(cb, -2, G::CS), sw_add(zb, -2, G::ZS), false);
+        stage_c(f0 + 2 * G::D + 1, sw_add(cb, -1, G::CS), sw_add(zb, -1, G::ZS), false);
         cp_async_commit();
         if (xc) {   // the iterate planes that arrived: group 0's, then two per step
             if (f0 == z0 - 1) {

@@ -408,8 +408,12 @@ def run_b200(args, dist):
     for k in range(2):
         gpu_step(gpu, capi, 2000 + k, dt, capi.MG_MIXED, args.pcg)
     gpu.profile(False)
-    rows = roofline(gpu.profile_report(), peak)
+    report = gpu.profile_report()
+    rows = roofline(report, peak)
     top = rows[0]
+    # summed kernel time per step (the rest of ms_per_step is the GPU waiting
+    # on the host between launches)
+    kernel_ms_per_step = sum(ms for _, ms, _ in report.values()) / 2
 
     # end to end through the C-ABI with pinned host buffers
     e2e = None
@@ -467,6 +471,7 @@ def run_b200(args, dist):
         "mg_iterations": {"mixed": its, "fp64": its64, ("mixed_dc" if args.pcg else "mixed_pcg"): itsdc},
         "mcell_updates_per_s": value * n ** 3 / 1e6,
         "gpu_launches": launches,
+        "kernel_ms_per_step": round(kernel_ms_per_step, 3),
         "roofline": {"bound": "hbm", "kernel": top["kernel"], "achieved": top["gbs"], "peak": peak,
                      "unit": "GB/s", "frac": top["frac"],
                      "traffic": (NCU_DRAM_BYTES_PER_CELL[top["kernel"]] * top["algo_bytes_per_launch"] /

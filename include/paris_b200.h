@@ -149,6 +149,30 @@ int paris_get_all_curvatures(paris_handle_t h, double* kappa_host);
 /* surfaceForce(du,dv,dw,rho), paris.f90:2862-2957 (adds to du,dv,dw) */
 int paris_surface_force(paris_handle_t h);
 
+/* ---- momentum predictor ---------------------------------------------- */
+#define PARIS_CONV_QUICK     0   /* AdvectionScheme = 'QUICK'    */
+#define PARIS_CONV_ENO       1   /* AdvectionScheme = 'ENO'      */
+#define PARIS_CONV_SUPERBEE  2   /* AdvectionScheme = 'Superbee' */
+#define PARIS_CONV_WENO      3   /* AdvectionScheme = 'WENO'     */
+/* momentumConvection, paris.f90:1957-1984 (QUICK :2288-2414; ENO, Superbee,
+ * WENO: momentumConvection_onedim :1991-2071): DU, DV, DW are assigned on
+ * the updated faces from U, V, W (ghosts filled)                          */
+int paris_momentum_convection(paris_handle_t h, int32_t scheme);
+/* explicitMomDiff(u,v,w,rho,mu,du,dv,dw), paris.f90:2757-2808 (adds)      */
+int paris_explicit_mom_diff(paris_handle_t h);
+/* volumeForce(rho,rho1,rho2,dpdx,dpdy,dpdz,BuoyancyCase,fx,fy,fz,gx,gy,gz,
+ * du,dv,dw,rho_ave), paris.f90:2813-2860 with fx = fy = fz = 0 (adds)     */
+int paris_volume_force(paris_handle_t h, double dpdx, double dpdy, double dpdz, int32_t buoyancy_case,
+                       double gx, double gy, double gz, double rho_ave);
+/* u = u + dt*du (whole arrays), paris.f90:442-444                         */
+int paris_advance_velocity(paris_handle_t h, double dt);
+/* SetVelocityBC(u,v,w,...) for walls (bdry_cond 0) and periodic (1)
+ * boundaries, modules.f90:951-973,1061-1105, then do_ghost_vector
+ * (modules.f90:1628).  wall_vel: WallVel(6,3) in Fortran order, face f
+ * (1 x-, 2 x+, 3 y-, 4 y+, 5 z-, 6 z+) component c at (f-1)+6*(c-1);
+ * NULL for resting walls.  Other boundary types return PARIS_BAD_ARGS.    */
+int paris_set_velocity_bc(paris_handle_t h, const double* wall_vel);
+
 /* ---- pressure projection ---------------------------------------------- */
 /* SetPressureBC + SetupPoisson + Poisson_BCs + check_poisson_setup,
  * modules.f90:916-949,2722-2892; newsolver.f90:275-344                     */

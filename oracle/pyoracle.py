@@ -68,6 +68,11 @@ def lib():
             "og_mycs": (None, [P, P]),
             "og_fd32": (None, [P, P]),
             "og_face_B": (None, [G, P, P, P, P]),
+            "og_momentum_convection": (I, [G, I, P, P, P, P, P, P]),
+            "og_explicit_mom_diff": (I, [G, P, P, P, P, P, P, P, P]),
+            "og_volume_force": (I, [G, P, D, D, D, I, D, D, D, D, P, P, P]),
+            "og_advance_velocity": (I, [G, D, P, P, P, P, P, P]),
+            "og_set_velocity_bc": (I, [G, P, P, P, P]),
             "og_projection_forward_B": (I, [G, D, P, P, P, P, P, P, P, P, P, P, D, I]),
             "og_projection_adjoint": (I, [G, D, P, P, P, P, P, P, P, P, P, P, P, P, P, D, I]),
         }
@@ -285,3 +290,29 @@ def updated_faces(desc, d):
         hi[d] -= 1
     m[g:g + hi[2], g:g + hi[1], g:g + hi[0]] = True
     return m
+
+
+def momentum_convection(desc, scheme, u, v, w, du, dv, dw):
+    """momentumConvection: assigns du, dv, dw (in place) from u, v, w."""
+    return lib().og_momentum_convection(ctypes.byref(desc), scheme, _p(u), _p(v), _p(w), _p(du), _p(dv), _p(dw))
+
+
+def explicit_mom_diff(desc, u, v, w, rho, mu, du, dv, dw):
+    return lib().og_explicit_mom_diff(ctypes.byref(desc), _p(u), _p(v), _p(w), _p(rho), _p(mu), _p(du), _p(dv),
+                                      _p(dw))
+
+
+def volume_force(desc, rho, du, dv, dw, dpdx=0.0, dpdy=0.0, dpdz=0.0, buoyancy=0, gx=0.0, gy=0.0, gz=0.0,
+                 rho_ave=0.0):
+    return lib().og_volume_force(ctypes.byref(desc), _p(rho), dpdx, dpdy, dpdz, buoyancy, gx, gy, gz, rho_ave,
+                                 _p(du), _p(dv), _p(dw))
+
+
+def advance_velocity(desc, dt, u, v, w, du, dv, dw):
+    return lib().og_advance_velocity(ctypes.byref(desc), dt, _p(u), _p(v), _p(w), _p(du), _p(dv), _p(dw))
+
+
+def set_velocity_bc(desc, u, v, w, wall_vel=None):
+    """wall_vel: (6, 3) array WallVel(face, component) or None."""
+    wv = None if wall_vel is None else np.ascontiguousarray(np.asarray(wall_vel, dtype=np.float64).reshape(6, 3).T)
+    return lib().og_set_velocity_bc(ctypes.byref(desc), _p(u), _p(v), _p(w), _p(wv))

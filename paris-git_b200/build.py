@@ -27,6 +27,7 @@ SOURCES = {
     "adjoint.cu": True,
     "noalloc.cu": True,
     "st.cu": True,
+    "momentum.cu": True,
 }
 
 

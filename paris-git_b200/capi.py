@@ -116,6 +116,8 @@ _LIB = None
 _P = ctypes.c_void_p
 _D = ctypes.c_double
 _I = ctypes.c_int32
+CONV_QUICK, CONV_ENO, CONV_SUPERBEE, CONV_WENO = 0, 1, 2, 3
+
 _PROTOS = {
     "paris_gpu_init": (_I, [ctypes.POINTER(GridDesc), ctypes.POINTER(_P)]),
     "paris_gpu_finalize": (_I, [_P]),
@@ -136,6 +138,11 @@ _PROTOS = {
     "paris_get_all_heights": (_I, [_P]),
     "paris_get_all_curvatures": (_I, [_P, _P]),
     "paris_surface_force": (_I, [_P]),
+    "paris_momentum_convection": (_I, [_P, _I]),
+    "paris_explicit_mom_diff": (_I, [_P]),
+    "paris_volume_force": (_I, [_P, _D, _D, _D, _I, _D, _D, _D, _D]),
+    "paris_advance_velocity": (_I, [_P, _D]),
+    "paris_set_velocity_bc": (_I, [_P, _P]),
     "paris_setup_poisson": (_I, [_P, _D, _D]),
     "paris_setup_test_mg": (_I, [_P]),
     "paris_new_solver": (_I, [_P, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveResult)]),

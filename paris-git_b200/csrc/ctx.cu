@@ -14,10 +14,10 @@ void ctx_set_error(paris_ctx* c, const char* fmt, ...) {
 }
 
 // Coordinates of the reference's uniform grid, paris.f90:3057-3100 (xform=0).
-static void make_axis(int n, int ng, double L, std::vector<double>& x, std::vector<double>& dx,
-                      std::vector<double>& dxh) {
+static void make_axis(int n, int ng, double L, std::vector<double>& x, std::vector<double>& xh,
+                      std::vector<double>& dx, std::vector<double>& dxh) {
     int nt = n + 2 * ng;
-    std::vector<double> xh(nt);
+    xh.assign(nt, 0.0);
     x.assign(nt, 0.0); dx.assign(nt, 0.0); dxh.assign(nt, 0.0);
     const double form = 0.0;
     for (int f = 1; f <= nt; f++) {
@@ -221,9 +221,9 @@ extern "C" int paris_gpu_init(const paris_grid_desc* desc, paris_handle_t* out) 
         c->bnd.wall_hi[a] = desc->bdry_cond[a + 3] == PARIS_BC_WALL || desc->bdry_cond[a + 3] == PARIS_BC_SHEAR;
     }
     for (int o = 0; o < 6; o++) c->bnd.vofbc[o] = desc->vofbdry_cond[o];
-    make_axis(desc->nx, desc->ng, desc->xlength, c->h_x, c->h_dx, c->h_dxh);
-    make_axis(desc->ny, desc->ng, desc->ylength, c->h_y, c->h_dy, c->h_dyh);
-    make_axis(desc->nz, desc->ng, desc->zlength, c->h_z, c->h_dz, c->h_dzh);
+    make_axis(desc->nx, desc->ng, desc->xlength, c->h_x, c->h_xh, c->h_dx, c->h_dxh);
+    make_axis(desc->ny, desc->ng, desc->ylength, c->h_y, c->h_yh, c->h_dy, c->h_dyh);
+    make_axis(desc->nz, desc->ng, desc->zlength, c->h_z, c->h_zh, c->h_dz, c->h_dzh);
     int s = PARIS_OK;
     if (!s) s = upload_vec(c, &c->dx, c->h_dx);
     if (!s) s = upload_vec(c, &c->dxh, c->h_dxh);
@@ -234,6 +234,9 @@ extern "C" int paris_gpu_init(const paris_grid_desc* desc, paris_handle_t* out) 
     if (!s) s = upload_vec(c, &c->xc, c->h_x);
     if (!s) s = upload_vec(c, &c->yc, c->h_y);
     if (!s) s = upload_vec(c, &c->zc, c->h_z);
+    if (!s) s = upload_vec(c, &c->xh, c->h_xh);
+    if (!s) s = upload_vec(c, &c->yh, c->h_yh);
+    if (!s) s = upload_vec(c, &c->zh, c->h_zh);
     if (!s && cudaMalloc(&c->red_part, 8L * kRedBlocks * sizeof(double)) != cudaSuccess) s = PARIS_CUDA_ERROR;
     if (!s && cudaMalloc(&c->red_out, 8 * sizeof(double)) != cudaSuccess) s = PARIS_CUDA_ERROR;
     if (!s && cudaMallocHost(&c->red_host, 8 * sizeof(double)) != cudaSuccess) s = PARIS_CUDA_ERROR;
@@ -261,7 +264,7 @@ extern "C" int paris_gpu_finalize(paris_handle_t c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (int f = 0; f < PARIS_NFIELDS; f++) free_ptr(c->fld[f]);
     for (void* p : {(void*)c->dx, (void*)c->dxh, (void*)c->dy, (void*)c->dyh, (void*)c->dz, (void*)c->dzh,
-                    (void*)c->xc, (void*)c->yc, (void*)c->zc, (void*)c->c2, (void*)c->flag, (void*)c->cg,
+                    (void*)c->xc, (void*)c->yc, (void*)c->zc, (void*)c->xh, (void*)c->yh, (void*)c->zh, (void*)c->c2, (void*)c->flag, (void*)c->cg,
                     (void*)c->height, (void*)c->i32stage, (void*)c->cx, (void*)c->cy, (void*)c->cz,
                     (void*)c->rhs, (void*)c->A, (void*)c->red_part, (void*)c->red_out, (void*)c->fast_r64,
                     (void*)c->fast_d64, (void*)c->fast_q64,

@@ -39,7 +39,8 @@ struct paris_ctx {
     // metrics (index i+ng, i interior-relative), device copies
     double *dx = nullptr, *dxh = nullptr, *dy = nullptr, *dyh = nullptr, *dz = nullptr, *dzh = nullptr;
     double *xc = nullptr, *yc = nullptr, *zc = nullptr;   // cell centres x(i), y(j), z(k)
-    std::vector<double> h_dx, h_dxh, h_dy, h_dyh, h_dz, h_dzh, h_x, h_y, h_z;
+    double *xh = nullptr, *yh = nullptr, *zh = nullptr;   // face positions xh(i) (face i+1/2)
+    std::vector<double> h_dx, h_dxh, h_dy, h_dyh, h_dz, h_dzh, h_x, h_y, h_z, h_xh, h_yh, h_zh;
     // ghosted fields (index PARIS_FIELD_*; VOF_FLAG/A/HEIGHT/PHASE kept apart)
     double* fld[PARIS_NFIELDS] = {};
     double* c2 = nullptr;          // second cvof buffer of the sweeps

@@ -207,6 +207,33 @@ class ParisGpu:
         """project_velocity(), paris.f90:882."""
         self._check(self.lib.paris_project_velocity(self.h, float(dt)), "project_velocity")
 
+    # -- momentum predictor ----------------------------------------------------
+    def momentum_convection(self, scheme=capi.CONV_QUICK):
+        """momentumConvection(), paris.f90:1957: DU, DV, DW from U, V, W."""
+        self._check(self.lib.paris_momentum_convection(self.h, int(scheme)), "momentumConvection")
+
+    def explicit_mom_diff(self):
+        """explicitMomDiff(u,v,w,rho,mu,du,dv,dw), paris.f90:2757."""
+        self._check(self.lib.paris_explicit_mom_diff(self.h), "explicitMomDiff")
+
+    def volume_force(self, dpdx=0.0, dpdy=0.0, dpdz=0.0, buoyancy=0, gx=0.0, gy=0.0, gz=0.0, rho_ave=0.0):
+        """volumeForce(...), paris.f90:2813, with no front-tracking force."""
+        self._check(self.lib.paris_volume_force(self.h, float(dpdx), float(dpdy), float(dpdz), int(buoyancy),
+                                                float(gx), float(gy), float(gz), float(rho_ave)), "volumeForce")
+
+    def advance_velocity(self, dt):
+        """u = u + dt*du, paris.f90:442."""
+        self._check(self.lib.paris_advance_velocity(self.h, float(dt)), "advance_velocity")
+
+    def set_velocity_bc(self, wall_vel=None):
+        """SetVelocityBC for walls / periodic boundaries + do_ghost_vector.
+        wall_vel: WallVel as a (6, 3) array (face, component) or None."""
+        if wall_vel is None:
+            self._check(self.lib.paris_set_velocity_bc(self.h, None), "SetVelocityBC")
+        else:
+            wv = np.ascontiguousarray(np.asarray(wall_vel, dtype=np.float64).reshape(6, 3).T)   # Fortran order
+            self._check(self.lib.paris_set_velocity_bc(self.h, _ptr(wv)), "SetVelocityBC")
+
     def projection_adjoint(self, dt, g, rel_tol=1e-12, maxit=100, mode=capi.MG_FP64, pcg=1):
         """Reverse mode of setup_poisson + new_solver + project_velocity.
 

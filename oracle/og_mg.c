@@ -368,6 +368,11 @@ static void og_mg_iteration(og_mg* mg, double beta, int norm) {
  * maxit (it = maxit+1). */
 int og_new_solver_mg(const paris_grid_desc* desc, const double* A, double* p, double maxError,
                      double beta, int maxit, int norm, int* it_out, double* tres2_out, double* hist) {
+    /* init_MG, MGsolver.f90:43-46: 2^n cells per direction */
+    for (int a = 0; a < 3; a++) {
+        int n = a == 0 ? desc->nx : (a == 1 ? desc->ny : desc->nz);
+        if (n < 2 || (n & (n - 1))) return PARIS_BAD_ARGS;
+    }
     og_grid* g = og_grid_new(desc);
     og_mg* mg = og_mg_new(g);
     int LMG = mg->LMG, ng = g->ng;

@@ -316,3 +316,35 @@ def set_velocity_bc(desc, u, v, w, wall_vel=None):
     """wall_vel: (6, 3) array WallVel(face, component) or None."""
     wv = None if wall_vel is None else np.ascontiguousarray(np.asarray(wall_vel, dtype=np.float64).reshape(6, 3).T)
     return lib().og_set_velocity_bc(ctypes.byref(desc), _p(u), _p(v), _p(w), _p(wv))
+
+
+def ns_step(desc, st, itimestep, dt, scheme=0, gravity=(0.0, 0.0, 0.0), buoyancy=0, rho_ave=0.0,
+            dpdx=(0.0, 0.0, 0.0), wall_vel=None, max_error=1e-12, maxit=2000):
+    """The step loop of paris.f90:281-656 (explicit, two-phase VOF, no front
+    tracking, no free surface) on the oracle; st: dict of ghosted arrays
+    cvof, flag, u, v, w, p, rho, mu (updated in place).  The pressure is
+    solved by the reference multigrid to the absolute RMS residual
+    max_error.  Returns the solver's cycle count."""
+    u, v, w = st["u"], st["v"], st["w"]
+    du, dv, dw = (zeros(desc) for _ in range(3))
+    rho = linfunc(desc, st["cvof"], desc.rho1, desc.rho2, desc.dens_mean)
+    mu = linfunc(desc, st["cvof"], desc.mu1, desc.mu2, desc.visc_mean)
+    momentum_convection(desc, scheme, u, v, w, du, dv, dw)
+    vofsweeps(desc, itimestep, dt, st["cvof"], st["flag"], u, v, w)
+    H = get_all_heights(desc, st["cvof"], st["flag"])
+    rho = linfunc(desc, st["cvof"], desc.rho1, desc.rho2, desc.dens_mean)
+    if desc.sigma > 0.0:
+        kap, _, _ = get_all_curvatures(desc, st["cvof"], st["flag"], H)
+        surface_force(desc, st["cvof"], kap, rho, du, dv, dw)
+    explicit_mom_diff(desc, u, v, w, rho, mu, du, dv, dw)
+    volume_force(desc, rho, du, dv, dw, dpdx[0], dpdx[1], dpdx[2], buoyancy, gravity[0], gravity[1], gravity[2],
+                 rho_ave)
+    advance_velocity(desc, dt, u, v, w, du, dv, dw)
+    set_velocity_bc(desc, u, v, w, wall_vel)
+    _, A = setup_poisson(desc, u, v, w, rho, dt)
+    _, it, _, _ = new_solver_mg(desc, A, st["p"], max_error, maxit=maxit)
+    project_velocity(desc, u, v, w, st["p"], rho, dt)
+    set_velocity_bc(desc, u, v, w, wall_vel)
+    st["rho"] = linfunc(desc, st["cvof"], desc.rho1, desc.rho2, desc.dens_mean)
+    st["mu"] = linfunc(desc, st["cvof"], desc.mu1, desc.mu2, desc.visc_mean)
+    return it

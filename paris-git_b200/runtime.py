@@ -234,6 +234,40 @@ class ParisGpu:
             wv = np.ascontiguousarray(np.asarray(wall_vel, dtype=np.float64).reshape(6, 3).T)   # Fortran order
             self._check(self.lib.paris_set_velocity_bc(self.h, _ptr(wv)), "SetVelocityBC")
 
+    def ns_step(self, itimestep, dt, scheme=capi.CONV_QUICK, gravity=(0.0, 0.0, 0.0), buoyancy=0, rho_ave=0.0,
+                dpdx=(0.0, 0.0, 0.0), wall_vel=None, solve=None):
+        """One explicit time step in the order of the PARIS step loop
+        (paris.f90:281-656: itime_scheme 1, two-phase VOF, no front
+        tracking, no free surface): property update, momentum convection,
+        VOF sweeps, heights, density, surface tension (when sigma > 0),
+        viscous diffusion, volume force, u += dt*du, velocity BCs, then the
+        projection (SetupPoisson, NewSolver, project_velocity, velocity BCs)
+        and the property update.  `solve`: keyword arguments of new_solver
+        (default: the B200 mixed solver to ||r||/||b|| < 1e-10).  Returns the
+        solver's result."""
+        solve = dict(solve or {"max_error": 0.0, "rel_tol": 1e-10, "maxit": 200, "mode": capi.MG_MIXED, "pcg": 1})
+        for f in (capi.F_DU, capi.F_DV, capi.F_DW):
+            self.fill_field(f, 0.0)
+        self.linfunc(capi.F_RHO)
+        self.linfunc(capi.F_MU)
+        self.momentum_convection(scheme)
+        self.vof_sweeps(itimestep, dt)
+        self.get_all_heights()
+        self.linfunc(capi.F_RHO)
+        if self.desc.sigma > 0.0:
+            self.surface_force()
+        self.explicit_mom_diff()
+        self.volume_force(dpdx[0], dpdx[1], dpdx[2], buoyancy, gravity[0], gravity[1], gravity[2], rho_ave)
+        self.advance_velocity(dt)
+        self.set_velocity_bc(wall_vel)
+        self.setup_poisson(dt)
+        r = self.new_solver(**solve)
+        self.project_velocity(dt)
+        self.set_velocity_bc(wall_vel)
+        self.linfunc(capi.F_RHO)
+        self.linfunc(capi.F_MU)
+        return r
+
     def projection_adjoint(self, dt, g, rel_tol=1e-12, maxit=100, mode=capi.MG_FP64, pcg=1):
         """Reverse mode of setup_poisson + new_solver + project_velocity.
 

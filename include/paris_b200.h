@@ -31,6 +31,7 @@ extern "C" {
 #define PARIS_CUDA_ERROR     4  /* a CUDA runtime call failed */
 #define PARIS_SETUP_ERROR    5  /* check_poisson_setup failed (newsolver.f90:275-344) */
 #define PARIS_NO_DEVICE      6  /* no usable CUDA device */
+#define PARIS_CFL_TOO_LARGE  7  /* get_cfl_and_check: CFL above cflmax_allowed (paris.f90:1072) */
 
 /* ---- boundary conditions ----------------------------------------------- */
 /* BDRY_COND of the &PARAMETERS namelist (order x- y- z- x+ y+ z+).          */
@@ -172,6 +173,48 @@ int paris_advance_velocity(paris_handle_t h, double dt);
  * (1 x-, 2 x+, 3 y-, 4 y+, 5 z-, 6 z+) component c at (f-1)+6*(c-1);
  * NULL for resting walls.  Other boundary types return PARIS_BAD_ARGS.    */
 int paris_set_velocity_bc(paris_handle_t h, const double* wall_vel);
+
+/* ---- time-step control and flow statistics ---------------------------- */
+/* TimeStepSize(dt, vof_phase), paris.f90:968-1041, for a run without a free
+ * surface: vmax = max over the interior of sqrt(u^2+v^2+w^2) taken at the
+ * same (i,j,k) of the three face fields, vmax_phys = max(1e-3, u_inject)
+ * (u_inject = max(ugas_inject, uliq_inject), 0 without injection),
+ * dt = min(cfl * h / max(vmax_phys, vmax), max_dt) with h = minval(dx).
+ * vmax_out may be NULL.                                                      */
+int paris_time_step_size(paris_handle_t h, double cfl, double max_dt, double u_inject, double* dt,
+                         double* vmax_out);
+/* get_cfl_and_check(dt), paris.f90:1045-1074: cfl = vmax*dt/h; returns
+ * PARIS_CFL_TOO_LARGE (with *cfl written) when cfl > cflmax_allowed (the
+ * reference stops with "CFL too large"; cflmax_allowed defaults to 0.5).    */
+int paris_get_cfl_and_check(paris_handle_t h, double dt, double cflmax_allowed, double* cfl);
+
+#define PARIS_NSTATS 25
+#define PARIS_STATS_RISING_BUBBLE   1   /* test_risingbubble  */
+#define PARIS_STATS_PHASE_INVERSION 2   /* test_PhaseInversion */
+#define PARIS_STATS_TURB            4   /* test_turb           */
+typedef struct paris_stats_opts {
+    /* volumeForce arguments of the step the statistics follow: calcStats
+     * sums fx, fy, fz = -dpdx + (rho_face - rro)*g as volumeForce left them */
+    double  dpdx, dpdy, dpdz;
+    double  gx, gy, gz;
+    double  rho_ave;             /* rro of BuoyancyCase 3 */
+    int32_t buoyancy_case;       /* BuoyancyCase 0..3 */
+    int32_t force_valid;         /* 0: fx = fy = fz = 0 (before the first step) */
+    int32_t test_flags;          /* PARIS_STATS_* */
+    int32_t reserved[3];
+} paris_stats_opts;
+/* calcStats, paris.f90:1116-1267: stats[0..24] = stats(1:25) (1 wall shear
+ * on y, 2 <u>, 3-5 <f>, 6 <rho>, 7 <p>, 8-9 momentum, 10 liquid volume
+ * fraction, 11 x centre of mass, 12-13 kinetic energy per phase, 14-15
+ * y-momentum per phase, 17-18 inflow/outflow pressure, 19 PLIC interface
+ * area, 20-21 potential energy, 22-23 enstrophy per phase, 24 rise velocity
+ * or top-layer fraction, 25 mixed-cell count) from the device fields, after
+ * the velocity BCs of the step.  Column 9 uses uold, which the reference
+ * keeps only for itime_scheme 2; with the explicit scheme it is zero, and it
+ * is zero here.  Sums are block partials added in a fixed order, so they are
+ * reproducible but not in the reference's loop order.  opts NULL: no force,
+ * no test flags.                                                             */
+int paris_calc_stats(paris_handle_t h, const paris_stats_opts* opts, double* stats);
 
 /* ---- pressure projection ---------------------------------------------- */
 /* SetPressureBC + SetupPoisson + Poisson_BCs + check_poisson_setup,

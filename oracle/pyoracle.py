@@ -75,6 +75,9 @@ def lib():
             "og_set_velocity_bc": (I, [G, P, P, P, P]),
             "og_projection_forward_B": (I, [G, D, P, P, P, P, P, P, P, P, P, P, D, I]),
             "og_projection_adjoint": (I, [G, D, P, P, P, P, P, P, P, P, P, P, P, P, P, D, I]),
+            "og_time_step_size": (I, [G, P, P, P, D, D, D, P, P]),
+            "og_get_cfl_and_check": (I, [G, P, P, P, D, D, P]),
+            "og_calc_stats": (I, [G, P, P, P, P, P, P, P, P, ctypes.POINTER(capi.StatsOpts), P, P]),
         }
         for name, (res, args) in protos.items():
             f = getattr(_lib, name)
@@ -348,3 +351,30 @@ def ns_step(desc, st, itimestep, dt, scheme=0, gravity=(0.0, 0.0, 0.0), buoyancy
     st["rho"] = linfunc(desc, st["cvof"], desc.rho1, desc.rho2, desc.dens_mean)
     st["mu"] = linfunc(desc, st["cvof"], desc.mu1, desc.mu2, desc.visc_mean)
     return it
+
+
+def time_step_size(desc, u, v, w, cfl, max_dt, u_inject=0.0):
+    """TimeStepSize (no free surface): returns (dt, vmax)."""
+    dt, vmax = ctypes.c_double(), ctypes.c_double()
+    st = lib().og_time_step_size(ctypes.byref(desc), _p(u), _p(v), _p(w), cfl, max_dt, u_inject, ctypes.byref(dt),
+                                 ctypes.byref(vmax))
+    assert st == 0
+    return dt.value, vmax.value
+
+
+def get_cfl_and_check(desc, u, v, w, dt, cflmax_allowed=0.5):
+    """get_cfl_and_check: returns (status, cfl)."""
+    cfl = ctypes.c_double()
+    st = lib().og_get_cfl_and_check(ctypes.byref(desc), _p(u), _p(v), _p(w), dt, cflmax_allowed, ctypes.byref(cfl))
+    return st, cfl.value
+
+
+def calc_stats(desc, u, v, w, rho, p, cvof, mu, flag, opts=None):
+    """calcStats: returns (stats(1:25), sums of |term| per column)."""
+    capi = _grid_desc_type()
+    out, ab = np.zeros(25), np.zeros(25)
+    f32 = np.ascontiguousarray(flag, dtype=np.int32)
+    st = lib().og_calc_stats(ctypes.byref(desc), _p(u), _p(v), _p(w), _p(rho), _p(p), _p(cvof), _p(mu), _p(f32),
+                             ctypes.byref(opts) if opts is not None else None, _p(out), _p(ab))
+    assert st == 0, st
+    return out, ab

@@ -28,6 +28,7 @@ SOURCES = {
     "noalloc.cu": True,
     "st.cu": True,
     "momentum.cu": True,
+    "stats.cu": True,
 }
 
 

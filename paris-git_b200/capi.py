@@ -11,9 +11,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIBNAME = "libparis_b200.so"
 
 # status codes
-OK, NOT_CONVERGED, NAN_DETECTED, BAD_ARGS, CUDA_ERROR, SETUP_ERROR, NO_DEVICE = range(7)
+OK, NOT_CONVERGED, NAN_DETECTED, BAD_ARGS, CUDA_ERROR, SETUP_ERROR, NO_DEVICE, CFL_TOO_LARGE = range(8)
 STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "NAN_DETECTED", 3: "BAD_ARGS",
-                4: "CUDA_ERROR", 5: "SETUP_ERROR", 6: "NO_DEVICE"}
+                4: "CUDA_ERROR", 5: "SETUP_ERROR", 6: "NO_DEVICE", 7: "CFL_TOO_LARGE"}
 
 # boundary conditions
 BC_WALL, BC_PERIODIC, BC_SHEAR = 0, 1, 2
@@ -66,6 +66,30 @@ class SolveOpts(ctypes.Structure):
         ("pcg", ctypes.c_int32),
         ("reserved", ctypes.c_int32 * 3),
     ]
+
+
+NSTATS = 25
+STATS_RISING_BUBBLE, STATS_PHASE_INVERSION, STATS_TURB = 1, 2, 4
+
+
+class StatsOpts(ctypes.Structure):
+    _fields_ = [
+        ("dpdx", ctypes.c_double), ("dpdy", ctypes.c_double), ("dpdz", ctypes.c_double),
+        ("gx", ctypes.c_double), ("gy", ctypes.c_double), ("gz", ctypes.c_double),
+        ("rho_ave", ctypes.c_double),
+        ("buoyancy_case", ctypes.c_int32), ("force_valid", ctypes.c_int32), ("test_flags", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 3),
+    ]
+
+
+def make_stats_opts(dpdx=(0.0, 0.0, 0.0), gravity=(0.0, 0.0, 0.0), rho_ave=0.0, buoyancy=0, force_valid=1,
+                    test_flags=0):
+    o = StatsOpts()
+    o.dpdx, o.dpdy, o.dpdz = (float(a) for a in dpdx)
+    o.gx, o.gy, o.gz = (float(a) for a in gravity)
+    o.rho_ave, o.buoyancy_case, o.force_valid, o.test_flags = float(rho_ave), int(buoyancy), int(force_valid), \
+        int(test_flags)
+    return o
 
 
 class SolveResult(ctypes.Structure):
@@ -143,6 +167,9 @@ _PROTOS = {
     "paris_volume_force": (_I, [_P, _D, _D, _D, _I, _D, _D, _D, _D]),
     "paris_advance_velocity": (_I, [_P, _D]),
     "paris_set_velocity_bc": (_I, [_P, _P]),
+    "paris_time_step_size": (_I, [_P, _D, _D, _D, _P, _P]),
+    "paris_get_cfl_and_check": (_I, [_P, _D, _D, _P]),
+    "paris_calc_stats": (_I, [_P, ctypes.POINTER(StatsOpts), _P]),
     "paris_setup_poisson": (_I, [_P, _D, _D]),
     "paris_setup_test_mg": (_I, [_P]),
     "paris_new_solver": (_I, [_P, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveResult)]),

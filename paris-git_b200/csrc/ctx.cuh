@@ -78,6 +78,8 @@ struct paris_ctx {
     double* fast_d64 = nullptr;
     double* fast_q64 = nullptr;
     double* adj = nullptr;         // projection adjoint: 10 ghosted fields + N (allocated on first use)
+    double* stats_part = nullptr;  // calcStats: PARIS_NSTATS slots of kRedBlocks partials (on first use)
+    double* stats_out = nullptr;
     int64_t launches = 0;
     char err[512] = {0};
     // per-kernel event timing

@@ -234,6 +234,32 @@ class ParisGpu:
             wv = np.ascontiguousarray(np.asarray(wall_vel, dtype=np.float64).reshape(6, 3).T)   # Fortran order
             self._check(self.lib.paris_set_velocity_bc(self.h, _ptr(wv)), "SetVelocityBC")
 
+    # -- time-step control and statistics ------------------------------------
+    def time_step_size(self, cfl, max_dt, u_inject=0.0):
+        """TimeStepSize (no free surface): returns (dt, vmax)."""
+        dt, vmax = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.paris_time_step_size(self.h, float(cfl), float(max_dt), float(u_inject),
+                                                  ctypes.byref(dt), ctypes.byref(vmax)), "TimeStepSize")
+        return dt.value, vmax.value
+
+    def get_cfl_and_check(self, dt, cflmax_allowed=0.5):
+        """get_cfl_and_check: returns the CFL number; raises ParisError
+        (CFL_TOO_LARGE) above cflmax_allowed, where the reference stops."""
+        cfl = ctypes.c_double()
+        self._check(self.lib.paris_get_cfl_and_check(self.h, float(dt), float(cflmax_allowed), ctypes.byref(cfl)),
+                    "get_cfl_and_check")
+        return cfl.value
+
+    def calc_stats(self, opts=None, **kw):
+        """calcStats: the 25 columns stats(1:25) as a float64 array.  opts: a
+        capi.StatsOpts, or keyword arguments of capi.make_stats_opts."""
+        o = opts if opts is not None else capi.make_stats_opts(**kw)
+        out = np.zeros(capi.NSTATS)
+        self._check(self.lib.paris_calc_stats(self.h, ctypes.byref(o), _ptr(out)), "calcStats")
+        return out
+
+    calcStats = calc_stats
+
     def ns_step(self, itimestep, dt, scheme=capi.CONV_QUICK, gravity=(0.0, 0.0, 0.0), buoyancy=0, rho_ave=0.0,
                 dpdx=(0.0, 0.0, 0.0), wall_vel=None, solve=None):
         """One explicit time step in the order of the PARIS step loop

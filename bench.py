@@ -13,6 +13,11 @@ the same step through the C-ABI with host buffers (u* uploaded, u,v,w,cvof
 downloaded every step).  `--impl reference` times the reference algorithm
 (the CPU restatement in oracle/) on the host cores.
 
+`--workload rising_bubble` times instead the full explicit Navier-Stokes step
+(momentum predictor, VOF, heights, curvature, CSF, projection) on a gas
+bubble of radius 0.125 rising in liquid in the walled box [0,1]x[0,1]x[0,2]
+at 512x512x1024, with the time step of TimeStepSize (CFL 0.5, MaxDt 5e-4).
+
 Prints one JSON line (rank 0).
 """
 import argparse
@@ -39,7 +44,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--n", type=int, default=256, help="cells per direction of the workload")
+    ap.add_argument("--workload", default="projection", choices=["projection", "rising_bubble"])
+    ap.add_argument("--n", type=int, default=None,
+                    help="cells per direction (projection: 256; rising_bubble: 512 across, twice that in z)")
     ap.add_argument("--pcg", type=int, default=1, help="1: FP64 flexible CG preconditioned by the V-cycle, 0: defect correction")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -186,6 +193,15 @@ ALGO_BYTES = {
     "setup_poisson": 64.0,        # u,v,w,rho 32 + 3 faces + rhs 32
     "project_velocity": 64.0,     # p,rho 16 + u,v,w read+write 48
     "linfunc": 16.0,              # cvof 8 + rho 8 (ghosted cells)
+    # the rest of a full Navier-Stokes step (rising-bubble workload)
+    "mom_convection": 48.0,       # u,v,w 24 + du,dv,dw 24
+    "mom_diffusion": 88.0,        # u,v,w,rho,mu 40 + du,dv,dw read+write 48
+    "volume_force": 56.0,         # rho 8 + du,dv,dw read+write 48
+    "advance_velocity": 72.0,     # u,v,w read+write 48 + du,dv,dw 24
+    "surface_force": 72.0,        # cvof, kappa, rho 24 + du,dv,dw read+write 48
+    "heights_pass1": 25.0,        # per direction: cvof 8 + flag 1 + two height arrays 16
+    "vmax": 24.0,                 # u,v,w
+    "calc_stats": 57.0,           # u,v,w,rho,p,cvof,mu 56 + flag 1
 }
 
 
@@ -487,11 +503,218 @@ def run_b200(args, dist):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# rising bubble: the full explicit Navier-Stokes step
+BUBBLE = {"radius": 0.125, "centre": (0.5, 0.5, 0.5), "rho_l": 1000.0, "rho_g": 1.0, "mu_l": 1e-3, "mu_g": 1e-5,
+          "sigma": 0.0245, "gravity": (0.0, 0.0, -9.81), "cfl": 0.5, "max_dt": 5e-4}
+BUBBLE_METRIC = "steps/s, rising bubble 512x512x1024, full NS step (mixed MG to 1e-9)"
+# The pressure of this flow carries the hydrostatic field (|p| up to 1.4e4)
+# and the face coefficients dt/(rho h^2) reach 131 in the gas at h = 1/512:
+# p itself is stored to ~1e-12, which bounds the true residual near 1.2e-10
+# of ||b||.  The solve stops at 1e-9, above that floor.
+BUBBLE_REL_TOL = 1e-9
+
+
+def bubble_desc(capi, n, device=0):
+    """The walled box [0,1]x[0,1]x[0,2] at h = 1/n.  Phase 2 (cvof = 1, inside
+    the sphere) is the gas, phase 1 the liquid: PARIS's input checks
+    (paris.f90:3750-3773) then read dx^2 rho_l/(MaxDt mu_l) >= 6 and
+    dx^3 rho_l/(MaxDt^2 sigma) >= 2, both met by MaxDt = 5e-4 at n = 512."""
+    B = BUBBLE
+    return capi.make_desc((n, n, 2 * n), length=(1.0, 1.0, 2.0), bc="wall", rho1=B["rho_l"], rho2=B["rho_g"],
+                          mu1=B["mu_l"], mu2=B["mu_g"], sigma=B["sigma"], device=device)
+
+
+def bubble_config(n, world=1):
+    B = BUBBLE
+    return {"workload": f"rising bubble: walled box [0,1]x[0,1]x[0,2] at {n}x{n}x{2 * n} (h=1/{n}), gas bubble "
+                        f"R={B['radius']} at {B['centre']}, rho {B['rho_l']:g}/{B['rho_g']:g}, mu "
+                        f"{B['mu_l']:g}/{B['mu_g']:g} (mu_l chosen: water-like), sigma {B['sigma']}, g=-9.81 in z; "
+                        "full explicit NS step (QUICK convection, CIAM VOF, heights, curvature, CSF, explicit "
+                        "viscosity, gravity, projection by the B200 mixed MG to ||r||/||b|| < 1e-9 from the "
+                        f"previous p); dt from TimeStepSize (CFL {B['cfl']}, MaxDt {B['max_dt']}) each step",
+            "cells": n * n * 2 * n, "parallelism": f"replicas x{world}", "l2": "inputs larger than L2"}
+
+
+def bubble_cpu_sample(pkg, n_cpu, steps=2, warmup=1):
+    """The reference step on the host cores (the oracle's ns_step, reference
+    MG to the same relative residual) on the same bubble at n_cpu x n_cpu x
+    2 n_cpu, from rest; returns (seconds per step, cells, cores)."""
+    from oracle import pyoracle as orc
+    capi, B = pkg.capi, BUBBLE
+    d = bubble_desc(capi, n_cpu)
+    cvof, flag, _ = orc.init_spheres(d, [B["centre"]], [B["radius"]], refinement=8)
+    st = {"cvof": cvof, "flag": flag, "u": orc.zeros(d), "v": orc.zeros(d), "w": orc.zeros(d), "p": orc.zeros(d)}
+    ts = []
+    for k in range(1, warmup + steps + 1):
+        t0 = time.perf_counter()
+        dt, _ = orc.time_step_size(d, st["u"], st["v"], st["w"], B["cfl"], B["max_dt"])
+        orc.ns_step(d, st, k, dt, gravity=B["gravity"], rel_tol=BUBBLE_REL_TOL, maxit=4000)
+        if k > warmup:
+            ts.append(time.perf_counter() - t0)
+    return float(np.mean(ts)), n_cpu * n_cpu * 2 * n_cpu, len(os.sched_getaffinity(0))
+
+
+def run_bubble_reference(args, dist):
+    pkg = load_pkg()
+    if dist.rank != 0:
+        return 0
+    n, n_cpu = args.n, min(args.n, 32)
+    t, cells, cores = bubble_cpu_sample(pkg, n_cpu, steps=max(1, min(args.steps, 3)), warmup=min(args.warmup, 1))
+    full = n * n * 2 * n
+    v = cells / full / t   # steps/s at the full size, from the per-cell rate of the sample
+    line = {
+        "impl": "reference", "metric": BUBBLE_METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": bubble_config(n),
+        "mcell_updates_per_s": cells / t / 1e6,
+        "cpu_baseline": {"value": v, "unit": "steps/s", "cores": cores, "kind": "port",
+                         "sample": f"the oracle's step (reference MG) at {n_cpu}x{n_cpu}x{2 * n_cpu} from rest, "
+                                   f"{t:.2f} s per step, scaled by cells to {n}x{n}x{2 * n}"},
+        "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_bubble(args, dist):
+    import torch
+    pkg = load_pkg()
+    capi, runtime, B = pkg.capi, pkg.runtime, BUBBLE
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    n = args.n
+    gpu = runtime.ParisGpu(bubble_desc(capi, n, dev))
+    gpu.init_spheres([B["centre"]], [B["radius"]], refinement=8)
+    for f in (capi.F_U, capi.F_V, capi.F_W, capi.F_P):
+        gpu.fill_field(f, 0.0)
+    gpu.linfunc(capi.F_RHO)
+    gpu.linfunc(capi.F_MU)
+    stream = torch.cuda.ExternalStream(gpu.stream())
+    peak, peak_kind = measured_peak()
+    s0 = gpu.calc_stats(force_valid=0)
+    k = [0]
+    solve = {"max_error": 0.0, "rel_tol": BUBBLE_REL_TOL, "maxit": 200, "mode": capi.MG_MIXED, "pcg": 1}
+
+    def step():
+        dt, _ = gpu.time_step_size(B["cfl"], B["max_dt"])     # TimeStepSize, dtFlag 2
+        k[0] += 1
+        return dt, gpu.ns_step(k[0], dt, gravity=B["gravity"], solve=solve)
+
+    if args.profile_only:
+        for _ in range(args.warmup):
+            step()
+        gpu.profile(True)
+        gpu.sync()
+        torch.cuda.nvtx.range_push("paris_steps")
+        for _ in range(max(1, args.steps)):
+            step()
+        gpu.sync()
+        torch.cuda.nvtx.range_pop()
+        gpu.profile(False)
+        if dist.rank == 0:
+            print(json.dumps({"profile": roofline(gpu.profile_report(), peak)}), flush=True)
+        gpu.close()
+        return 0
+
+    for _ in range(args.warmup):
+        step()
+    gpu.sync()
+    dist.barrier()
+    clocks = Clocks(dev)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dts, its = [], []
+    l0 = gpu.launch_count()
+    e0.record(stream)
+    for _ in range(args.steps):
+        dt, r = step()
+        dts.append(dt)
+        its.append(r.it)
+    e1.record(stream)
+    e1.synchronize()
+    gpu.sync()
+    clk = clocks.stop()
+    launches = gpu.launch_count() - l0
+    ms = dist.max(e0.elapsed_time(e1))
+    dist.barrier()
+    # per-kernel CUDA-event profile of two more steps
+    gpu.profile(True)
+    for _ in range(2):
+        step()
+    gpu.profile(False)
+    report = gpu.profile_report()
+    rows = roofline(report, peak)
+    kernel_ms_per_step = sum(m for _, m, _ in report.values()) / 2
+    # end to end: each step also reads back its statistics line, as the
+    # reference's loop does with nstats = 1 (the state stays on the device)
+    e_steps = max(1, min(args.steps, 10))
+    opts = capi.make_stats_opts(gravity=B["gravity"])
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e_steps):
+        step()
+        s1 = gpu.calc_stats(opts)
+    e1.record(stream)
+    e1.synchronize()
+    ems = dist.max(e0.elapsed_time(e1))
+    dist.barrier()
+    zc = gpu.download(capi.F_CVOF)
+    g = 2
+    cells = n * n * 2 * n
+    vol0, vol1 = s0[9], s1[9]
+    # bubble centre height: the cvof-weighted mean of z over the interior
+    zcen = (np.arange(2 * n) + 0.5) / n
+    ci = zc[g:-g, g:-g, g:-g]
+    zbub = float((ci.sum(axis=(1, 2)) * zcen).sum() / ci.sum())
+    cpu = None
+    if dist.rank == 0 and not args.no_cpu_baseline:
+        n_cpu = min(n, 32)
+        t, ccells, cores = bubble_cpu_sample(pkg, n_cpu)
+        cpu = {"value": ccells / cells / t, "unit": "steps/s", "cores": cores, "kind": "port",
+               "sample": f"the oracle's step (reference MG) at {n_cpu}x{n_cpu}x{2 * n_cpu} from rest, "
+                         f"{t:.2f} s per step, scaled by cells to {n}x{n}x{2 * n}"}
+    gpu.close()
+    if dist.rank != 0:
+        return 0
+    value = dist.world * args.steps / (ms / 1e3)
+    top = rows[0]
+    line = {
+        "metric": BUBBLE_METRIC, "value": value, "unit": "steps/s", "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic", "config": bubble_config(n, dist.world),
+        "mcell_updates_per_s": value * cells / 1e6,
+        "dt": [min(dts), max(dts)], "mg_iterations": its, "gpu_launches": launches,
+        "kernel_ms_per_step": round(kernel_ms_per_step, 3),
+        "gas_volume": {"initial": vol0, "final": vol1, "rel_change": abs(vol1 - vol0) / vol0},
+        "bubble_centre_z": zbub,
+        "roofline": {"bound": "hbm", "kernel": top["kernel"], "achieved": top["gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": top["frac"], "traffic": None,
+                     "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                     "algo_bytes_per_launch": top["algo_bytes_per_launch"]},
+        "kernels": rows[:20],
+        "clocks": clk,
+        "e2e": {"value": dist.world * e_steps / (ems / 1e3), "unit": "steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 8 * (capi.NSTATS + 2), "steps": e_steps,
+                "note": "state resident on the device; per step the time step and the statistics line "
+                        "come back to the host"},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.n is None:
+        args.n = 512 if args.workload == "rising_bubble" else 256
     dist = Dist()
     try:
-        rc = run_reference(args, dist) if args.impl == "reference" else run_b200(args, dist)
+        if args.workload == "rising_bubble":
+            rc = run_bubble_reference(args, dist) if args.impl == "reference" else run_bubble(args, dist)
+        else:
+            rc = run_reference(args, dist) if args.impl == "reference" else run_b200(args, dist)
     finally:
         dist.close()
     return rc

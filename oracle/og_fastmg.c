@@ -11,8 +11,13 @@
  *   - red-black Gauss-Seidel V(nu1,nu2) cycles, black-red after the
  *     coarse correction (symmetric cycle), coarsest level smoothed;
  *   - an FP64 outer loop: defect correction p += V(b - A p), or
- *     preconditioned CG with the V-cycle as preconditioner;
- *   - inner cycle in FP32 (mixed) or FP64.
+ *     preconditioned CG with the V-cycle as preconditioner, with A applied
+ *     in flux form b + sum_f a_f (x_f - x_c); CG checks the true residual
+ *     when the recursive one meets the tolerance and restarts from it (at
+ *     most twice) when the two have drifted apart;
+ *   - inner cycle in FP32 (mixed) or FP64;
+ *   - on a singular system (walls and periodic boundaries only) the initial
+ *     guess with its mean taken out, the mean put back at the end.
  * The CUDA kernels of paris-git_b200/csrc/mg_fast.cu follow the same steps.
  */
 #include <math.h>
@@ -100,6 +105,27 @@ static void resid_##SUF(const fm_mg* mg, fm_level* l, const T* b, const T* x, T*
                 FM_NBR(T, l, per, x, i, j, k, 0, 0, 1, pt);                                  \
                 T d = a1 + a2 + a3 + a4 + a5 + a6;                                           \
                 r[q] = b[q] - d * x[q] + a1 * pw + a2 * pe + a3 * ps + a4 * pn + a5 * pb + a6 * pt; \
+            }                                                                                \
+}                                                                                            \
+/* r = b - A x in flux form, b + sum_f a_f (x_f - x_c): the FP64 outer loop */               \
+static void resid_flux_##SUF(const fm_mg* mg, fm_level* l, const T* b, const T* x, T* r) {   \
+    const int* per = mg->per;                                                                \
+    for (int k = 0; k < l->n[2]; k++)                                                        \
+        for (int j = 0; j < l->n[1]; j++)                                                    \
+            for (int i = 0; i < l->n[0]; i++) {                                              \
+                long q = FIDX(l, i, j, k);                                                   \
+                T a1 = FM_WEST(l, per, l->CX, i, j, k, 0), a2 = l->CX[q];                    \
+                T a3 = FM_WEST(l, per, l->CY, i, j, k, 1), a4 = l->CY[q];                    \
+                T a5 = FM_WEST(l, per, l->CZ, i, j, k, 2), a6 = l->CZ[q];                    \
+                T pw, pe, ps, pn, pb, pt, pc = x[q];                                         \
+                FM_NBR(T, l, per, x, i, j, k, -1, 0, 0, pw);                                 \
+                FM_NBR(T, l, per, x, i, j, k, 1, 0, 0, pe);                                  \
+                FM_NBR(T, l, per, x, i, j, k, 0, -1, 0, ps);                                 \
+                FM_NBR(T, l, per, x, i, j, k, 0, 1, 0, pn);                                  \
+                FM_NBR(T, l, per, x, i, j, k, 0, 0, -1, pb);                                 \
+                FM_NBR(T, l, per, x, i, j, k, 0, 0, 1, pt);                                  \
+                r[q] = b[q] + (a1 * (pw - pc) + a2 * (pe - pc) + a3 * (ps - pc) + a4 * (pn - pc) + \
+                               a5 * (pb - pc) + a6 * (pt - pc));                             \
             }                                                                                \
 }                                                                                            \
 static void restrict_##SUF(const fm_level* f, fm_level* c, const T* rf, T* bc) {             \
@@ -236,16 +262,31 @@ int og_fastmg_solve(const paris_grid_desc* desc, const double* A, double* p, dou
     double* d = malloc(N * 8);
     double* q_ = malloc(N * 8);
     for (long q = 0; q < N; q++) b[q] = A[7 * N + q];
+    /* walls and periodic boundaries leave the system singular (constants
+     * are its null space): solve from the initial guess with its mean taken
+     * out and put the mean back at the end */
+    int sing = 1;
+    for (int a = 0; a < 3; a++) {
+        int lo = desc->bdry_cond[a], hi = desc->bdry_cond[a + 3];
+        int wall_lo = lo == PARIS_BC_WALL || lo == PARIS_BC_SHEAR, wall_hi = hi == PARIS_BC_WALL || hi == PARIS_BC_SHEAR;
+        if (!mg.per[a] && !(wall_lo && wall_hi)) sing = 0;
+    }
+    double shift = 0.0;
+    if (sing) {
+        for (long q = 0; q < N; q++) shift += p[q];
+        shift /= (double)N;
+        for (long q = 0; q < N; q++) p[q] = p[q] - shift;
+    }
     double bn = sqrt(dot(b, b, N));
     if (bn == 0.0) bn = 1.0;
-    resid_d(&mg, l0, b, p, r);
+    resid_flux_d(&mg, l0, b, p, r);
     double rn = sqrt(dot(r, r, N));
     int it = 0;
     if (!pcg) {
         while (it < maxit && rn / bn >= rel_tol) {
             precond(&mg, r, z);
             for (long q = 0; q < N; q++) p[q] += z[q];
-            resid_d(&mg, l0, b, p, r);
+            resid_flux_d(&mg, l0, b, p, r);
             rn = sqrt(dot(r, r, N));
             if (hist) hist[it] = rn / bn;
             it++;
@@ -254,9 +295,10 @@ int og_fastmg_solve(const paris_grid_desc* desc, const double* A, double* p, dou
         precond(&mg, r, z);
         memcpy(d, z, N * 8);
         double rz = dot(r, z, N);
+        int restarts = 0;
         while (it < maxit && rn / bn >= rel_tol) {
             memset(q_, 0, N * 8);
-            resid_d(&mg, l0, q_, d, q_);   /* q_ = 0 - A d */
+            resid_flux_d(&mg, l0, q_, d, q_);   /* q_ = 0 - A d */
             for (long q = 0; q < N; q++) q_[q] = -q_[q];
             double dq = dot(d, q_, N);
             double alpha = rz / dq;
@@ -264,7 +306,19 @@ int og_fastmg_solve(const paris_grid_desc* desc, const double* A, double* p, dou
             rn = sqrt(dot(r, r, N));
             if (hist) hist[it] = rn / bn;
             it++;
-            if (rn / bn < rel_tol) break;
+            if (rn / bn < rel_tol) {
+                /* check the true residual; restart from it when rounding has
+                 * let the recursive one drift away (at most twice) */
+                resid_flux_d(&mg, l0, b, p, r);
+                rn = sqrt(dot(r, r, N));
+                if (hist) hist[it - 1] = rn / bn;
+                if (rn / bn < rel_tol || restarts == 2) break;
+                restarts++;
+                precond(&mg, r, z);
+                memcpy(d, z, N * 8);
+                rz = dot(r, z, N);
+                continue;
+            }
             double* zold = q_;          /* reuse */
             memcpy(zold, z, N * 8);
             precond(&mg, r, z);
@@ -277,6 +331,8 @@ int og_fastmg_solve(const paris_grid_desc* desc, const double* A, double* p, dou
             for (long q = 0; q < N; q++) d[q] = z[q] + beta * d[q];
         }
     }
+    if (shift != 0.0)
+        for (long q = 0; q < N; q++) p[q] = p[q] + shift;
     free(b); free(r); free(z); free(d); free(q_);
     for (int L = 0; L < nl; L++) {
         fm_level* l = &mg.L[L];

@@ -322,12 +322,13 @@ def set_velocity_bc(desc, u, v, w, wall_vel=None):
 
 
 def ns_step(desc, st, itimestep, dt, scheme=0, gravity=(0.0, 0.0, 0.0), buoyancy=0, rho_ave=0.0,
-            dpdx=(0.0, 0.0, 0.0), wall_vel=None, max_error=1e-12, maxit=2000):
+            dpdx=(0.0, 0.0, 0.0), wall_vel=None, max_error=1e-12, maxit=2000, rel_tol=None):
     """The step loop of paris.f90:281-656 (explicit, two-phase VOF, no front
     tracking, no free surface) on the oracle; st: dict of ghosted arrays
     cvof, flag, u, v, w, p, rho, mu (updated in place).  The pressure is
     solved by the reference multigrid to the absolute RMS residual
-    max_error.  Returns the solver's cycle count."""
+    max_error, or, with rel_tol, to rel_tol times the RMS of the right-hand
+    side (||r||_2/||b||_2 < rel_tol).  Returns the solver's cycle count."""
     u, v, w = st["u"], st["v"], st["w"]
     du, dv, dw = (zeros(desc) for _ in range(3))
     rho = linfunc(desc, st["cvof"], desc.rho1, desc.rho2, desc.dens_mean)
@@ -345,6 +346,8 @@ def ns_step(desc, st, itimestep, dt, scheme=0, gravity=(0.0, 0.0, 0.0), buoyancy
     advance_velocity(desc, dt, u, v, w, du, dv, dw)
     set_velocity_bc(desc, u, v, w, wall_vel)
     _, A = setup_poisson(desc, u, v, w, rho, dt)
+    if rel_tol is not None:
+        max_error = rel_tol * float(np.sqrt(np.mean(A[7] ** 2)))
     _, it, _, _ = new_solver_mg(desc, A, st["p"], max_error, maxit=maxit)
     project_velocity(desc, u, v, w, st["p"], rho, dt)
     set_velocity_bc(desc, u, v, w, wall_vel)

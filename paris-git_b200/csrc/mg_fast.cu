@@ -257,8 +257,13 @@ __device__ inline double pfield(const double* __restrict__ p, const Layout& L, c
     return p[lidx(L, i, j, k)];
 }
 
-// (A x)_m with the symmetric face form: A1 = cx(i-1), A2 = cx(i), ...,
-// A7 = A1+..+A6 in the reference's order.  x: ghosted field or compact.
+// (A x)_m with the symmetric face form: A1 = cx(i-1), A2 = cx(i), ...
+// The FP64 outer loop applies A in flux form, sum_f a_f (x_f - x_c): a
+// constant x gives exactly 0 (constants are the null space of the singular
+// system), and only neighbour differences are rounded, not coef * |x|.  A
+// warm-started pressure carries the hydrostatic field (|p| ~ 1e4 at density
+// ratio 1000 and g = 9.81); with the d*x form its rounding, coef * |p| * eps
+// per cell, was above the 1e-10 relative residual at h = 1/512.
 struct Mat64 {
     const double *cx, *cy, *cz, *rhs;
 };
@@ -270,8 +275,8 @@ __device__ inline double ax_compact(const Mat64& A, const double* __restrict__ x
     west_coefs(v, B, i, j, k, m, a1, a3, a5);
     double a2 = A.cx[m], a4 = A.cy[m], a6 = A.cz[m];
     nbrs(v, x, B, i, j, k, m, xw, xe, xs, xn, xb, xt);
-    double d = a1 + a2 + a3 + a4 + a5 + a6;
-    return d * x[m] - (a1 * xw + a2 * xe + a3 * xs + a4 * xn + a5 * xb + a6 * xt);
+    const double xc = x[m];
+    return -(a1 * (xw - xc) + a2 * (xe - xc) + a3 * (xs - xc) + a4 * (xn - xc) + a5 * (xb - xc) + a6 * (xt - xc));
 }
 
 // r = b - A p on the ghosted p (wrap in the kernel); writes r as T into the
@@ -290,11 +295,11 @@ __global__ void k_fast_residual64(const Mat64 A, const double* __restrict__ p, c
         double a5 = k > 0 ? A.cz[m - sz] : (B.per[2] ? A.cz[m + sz * (L.n[2] - 1)] : 0.0);
         double a2 = A.cx[m], a4 = A.cy[m], a6 = A.cz[m];
         long n = lidx(L, i, j, k);
-        double d = a1 + a2 + a3 + a4 + a5 + a6;
         double b = A.rhs[m];
-        double r = b - d * p[n] + a1 * pfield(p, L, B, i - 1, j, k) + a2 * pfield(p, L, B, i + 1, j, k) +
-                   a3 * pfield(p, L, B, i, j - 1, k) + a4 * pfield(p, L, B, i, j + 1, k) +
-                   a5 * pfield(p, L, B, i, j, k - 1) + a6 * pfield(p, L, B, i, j, k + 1);
+        const double pc = p[n];
+        double r = b + (a1 * (pfield(p, L, B, i - 1, j, k) - pc) + a2 * (pfield(p, L, B, i + 1, j, k) - pc) +
+                        a3 * (pfield(p, L, B, i, j - 1, k) - pc) + a4 * (pfield(p, L, B, i, j + 1, k) - pc) +
+                        a5 * (pfield(p, L, B, i, j, k - 1) - pc) + a6 * (pfield(p, L, B, i, j, k + 1) - pc));
         if (rT) rT[m] = (T)r;
         if (r64) r64[m] = r;
         s2 += r * r;
@@ -642,7 +647,12 @@ static int precondition(paris_ctx* c, int nu1, int nu2, T** z, double* rz) {
 
 // Flexible CG (Polak-Ribiere beta) preconditioned by one V-cycle, in FP64.
 // z stays in the V-cycle's output buffer until the next V-cycle starts: the
-// update kernel forms r.zold before that.
+// update kernel forms r.zold before that.  The residual is updated
+// recursively; when it meets the tolerance the true residual b - A p is
+// formed and checked, and CG restarts from it (at most kMaxRestarts times)
+// when rounding has let the two drift apart, so the residual reported is the
+// true one.
+static constexpr int kMaxRestarts = 2;
 template <typename T>
 static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* res, const double* rhs, double* p) {
     auto& lv = levels<T>(c);
@@ -663,6 +673,7 @@ static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result
         PARIS_CHECK(precondition<T>(c, nu1, nu2, &z, &rz));
         PARIS_LAUNCH_N(c, kname<T>("pcg_dir"), c->N, k_pcg_dir<T>, div_up(c->N, 256), 256, 0, c->fast_d64, z, 0.0, c->N);
     }
+    int restarts = 0;
     while (!done && it < o->maxit) {
         double dq;
         PARIS_LAUNCH_N(c, "pcg_matvec_fp64", c->N, k_pcg_matvec, red_grid(c, k_pcg_matvec, 256), kRowBlock, 0, A, c->fast_d64, c->fast_q64, c->L, c->bnd, c->red_part);
@@ -679,7 +690,20 @@ static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result
             res->it = it; res->res = tres; res->rel_res = rel;
             return PARIS_NAN_DETECTED;
         }
-        if (done) break;
+        if (done) {
+            // the true residual (also the right-hand side of a restart)
+            PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>,
+                           red_grid(c, k_fast_residual64<T>, 256), kRowBlock, 0, A, p, c->L, c->bnd, lv[0].b,
+                           c->fast_r64, c->red_part);
+            PARIS_CHECK(ctx_reduce_finish(c, 3, s));
+            done = converged(o, s[0], s[1], bn2, c->N, &tres, &rel);
+            if (done || restarts == kMaxRestarts) break;
+            restarts++;
+            PARIS_CHECK(precondition<T>(c, nu1, nu2, &z, &rz));
+            PARIS_LAUNCH_N(c, kname<T>("pcg_dir"), c->N, k_pcg_dir<T>, div_up(c->N, 256), 256, 0, c->fast_d64, z, 0.0,
+                           c->N);
+            continue;
+        }
         double r_zold = s[2], rz_new;
         PARIS_CHECK(precondition<T>(c, nu1, nu2, &z, &rz_new));
         double beta = (rz_new - r_zold) / rz;   // flexible (Polak-Ribiere) form
@@ -692,9 +716,54 @@ static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result
     return done ? PARIS_OK : PARIS_NOT_CONVERGED;
 }
 
+// Interior sum of a ghosted field (slot 0 of the reduction buffer).
+__global__ void k_interior_sum(const double* __restrict__ x, const Layout L, double* part) {
+    __shared__ double sh[32];
+    double s = 0.0;
+    ROWS_BEGIN(L.n[0], L.n[1], L.n[2])
+        s += x[lidx(L, i, j, k)];
+    ROWS_END
+    s = block_sum<256>(s, sh);
+    if (linear_tid() == 0) part[blockIdx.x] = s;
+}
+
+__global__ void k_interior_shift(double* __restrict__ x, const Layout L, double m) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L.n[0]) return;
+    const long n = lidx(L, i, blockIdx.y, blockIdx.z);
+    x[n] = x[n] + m;
+}
+
+// Walls (shear walls included) and periodic boundaries leave the pressure
+// equation singular: constants are its null space.
+static bool singular(const paris_ctx* c) {
+    for (int a = 0; a < 3; a++)
+        if (!c->bnd.per[a] && !(c->bnd.wall_lo[a] && c->bnd.wall_hi[a])) return false;
+    return true;
+}
+
 int mg_fast_solve_into(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* res, const double* rhs,
                        double* x) {
     if (!c->have_matrix) return PARIS_BAD_ARGS;
+    // A singular system is solved from its initial guess with the mean taken
+    // out, and the mean is put back afterwards.  A warm start with a large
+    // constant part (the hydrostatic pressure of the previous step) otherwise
+    // leaves a rounding-sized mean in r = b - A x: the inconsistent part of
+    // the singular system, which the V-cycle's coarsest level turns into a
+    // growing constant in the search direction, and PCG stalls.
+    double shift = 0.0;
+    if (singular(c)) {
+        PARIS_LAUNCH_N(c, "mean_shift", c->N, k_interior_sum, red_grid(c, k_interior_sum, 256), kRowBlock, 0, x, c->L,
+                       c->red_part);
+        double sum;
+        PARIS_CHECK(ctx_reduce_finish(c, 1, &sum));
+        shift = sum / (double)c->N;
+        if (shift != 0.0 && shift == shift)
+            PARIS_LAUNCH_N(c, "mean_shift", c->N, k_interior_shift, row_grid(c->d.nx, c->d.ny, c->d.nz), 128, 0, x,
+                           c->L, -shift);
+        else
+            shift = 0.0;
+    }
     int st;
     if (o->mode == PARIS_MG_MIXED) {
         PARIS_CHECK(fast_alloc<float>(c));
@@ -705,6 +774,9 @@ int mg_fast_solve_into(paris_ctx* c, const paris_solve_opts* o, paris_solve_resu
         PARIS_CHECK(fast_coefs<double>(c));
         st = o->pcg ? solve_pcg<double>(c, o, res, rhs, x) : solve_dc<double>(c, o, res, rhs, x);
     }
+    if (shift != 0.0)
+        PARIS_LAUNCH_N(c, "mean_shift", c->N, k_interior_shift, row_grid(c->d.nx, c->d.ny, c->d.nz), 128, 0, x, c->L,
+                       shift);
     if (st == PARIS_OK || st == PARIS_NOT_CONVERGED) PARIS_CHECK(ctx_ghost_fill(c, x));
     return st;
 }

@@ -185,3 +185,34 @@ def test_fast_mg_fused_levels_follow_oracle(gpu_lib, capi, runtime, orc, workloa
     assert rm.rel_res < 1e-10 and rm.it <= it_ref + 2
     _, itm_ref, _ = orc.fastmg_solve(desc, A, np.zeros((n, n, n)), 1e-10, maxit=60, mixed=True, pcg=True)
     assert abs(rm.it - itm_ref) <= 1
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_warm_start_with_a_large_constant(gpu_lib, capi, runtime, orc, workloads, mode):
+    """Walls leave the pressure equation singular.  A warm start carrying a
+    large constant (the hydrostatic level a previous step leaves in p) must
+    converge like a cold start: the solver takes the mean of the initial
+    guess out for the solve and puts it back, so the returned p keeps the
+    caller's level (up to the mean of the correction)."""
+    n = 128
+    desc, cvof, rho, vel = drop_problem(capi, orc, workloads, n, bc="wall", ndrops=12)
+    m = capi.MG_FP64 if mode == "fp64" else capi.MG_MIXED
+    dt = 1e-3
+    with runtime.ParisGpu(desc) as gpu:
+        upload_state(gpu, capi, cvof, rho, vel)
+        gpu.setup_poisson(dt)
+        cold = gpu.new_solver(0.0, maxit=60, mode=m, rel_tol=1e-10, pcg=1)
+        p = gpu.download(capi.F_P)
+        rng = np.random.default_rng(3)
+        g = desc.ng
+        warm = p + 1e5
+        orc.interior(desc, warm)[...] += 1e-3 * np.abs(p).max() * rng.standard_normal((n, n, n))
+        gpu.upload(capi.F_P, warm)
+        r = gpu.new_solver(0.0, maxit=60, mode=m, rel_tol=1e-10, pcg=1)
+        pw = gpu.download(capi.F_P)
+    assert cold.rel_res < 1e-10 and r.rel_res < 1e-10 and r.it <= cold.it
+    wi = orc.interior(desc, warm)
+    # the level: the warm start's mean plus the small mean of the solver's correction
+    assert abs(orc.interior(desc, pw).mean() - wi.mean()) <= 1e-6 * abs(wi.mean())
+    d = orc.interior(desc, pw) - orc.interior(desc, p)
+    assert np.abs(d - d.mean()).max() <= 1e-8 * np.abs(p).max()

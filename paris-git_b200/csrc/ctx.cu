@@ -269,7 +269,7 @@ extern "C" int paris_gpu_finalize(paris_handle_t c) {
                     (void*)c->rhs, (void*)c->A, (void*)c->red_part, (void*)c->red_out, (void*)c->fast_r64,
                     (void*)c->fast_d64, (void*)c->fast_q64,
                     (void*)c->vflux, (void*)c->mixlist, (void*)c->mixcount, (void*)c->kflag, (void*)c->st_list,
-                    (void*)c->st_count, (void*)c->adj, (void*)c->stats_part, (void*)c->stats_out})
+                    (void*)c->st_count, (void*)c->adj, (void*)c->stats_part, (void*)c->stats_out, (void*)c->mom_tab})
         free_ptr(p);
     for (auto& l : c->ref) { free_ptr(l.K); free_ptr(l.p); free_ptr(l.e); }
     for (auto& l : c->fl32) { free_ptr(l.cx); free_ptr(l.cy); free_ptr(l.cz); free_ptr(l.b); free_ptr(l.x); free_ptr(l.x2); }

@@ -78,6 +78,8 @@ struct paris_ctx {
     double* fast_d64 = nullptr;
     double* fast_q64 = nullptr;
     double* adj = nullptr;         // projection adjoint: 10 ghosted fields + N (allocated on first use)
+    double* mom_tab = nullptr;     // momentum predictor: per-index QUICK coefficients and metric reciprocals
+    int mom_tab_exact = 0;         // their reciprocals of k, 1-k, k-1, dx, dxh are exact (powers of two)
     double* stats_part = nullptr;  // calcStats: PARIS_NSTATS slots of kRedBlocks partials (on first use)
     double* stats_out = nullptr;
     int64_t launches = 0;

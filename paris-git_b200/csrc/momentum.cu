@@ -11,6 +11,8 @@
 // order, so results equal the FP64 restatement bit for bit.  The face values
 // the reference keeps in its `work` array are recomputed where they are used
 // (same operands, same operations), one thread per cell.
+#include <cmath>
+
 #include "ctx.cuh"
 
 namespace {
@@ -25,68 +27,171 @@ struct Vel {
     const double *u, *v, *w;
 };
 
-// inter(x0,x1,x2,x,y0,y1,y2), paris.f90:2390-2411 (QUICK branch)
-__device__ inline double inter(double x0, double x1, double x2, double x, double y0, double y1, double y2) {
-    double xi = (x - x0) / (x1 - x0);
-    double k = (x2 - x0) / (x1 - x0);
-    double a = (y2 - k * k * y1 + (k * k - 1.0) * y0) / k / (1.0 - k);
-    double b = (y2 - k * y1 + (k - 1.0) * y0) / k / (k - 1.0);
+// The coordinate part of inter() for one face: xi and k from x0, x1, x2, x,
+// computed once per index on the host with the same IEEE operations (so the
+// values are those inter() forms), plus the reciprocals of k, 1 - k, k - 1.
+// On a uniform grid with a power-of-two cell count k = -1, so the divisions
+// of inter() by k, 1 - k and k - 1 are by powers of two: multiplying by the
+// exact reciprocal then rounds to the same double as dividing, and the
+// kernel takes that form (R = true) when every reciprocal it uses is exact.
+struct QuickCoef {
+    double xi, k, rk, r1k, rkm1;
+};
+// Per axis, index t = ii + ng: Q[4t + 0] own axis, vel > 0; 4t + 1 own
+// axis, otherwise; 4t + 2 cross axis, vel > 0; 4t + 3 cross axis, otherwise.
+// rd = 1./d, rdh = 1./dh (the metric reciprocals of explicitMomDiff).
+struct MomTab {
+    const QuickCoef* q[3];
+    const double* rd[3];
+    const double* rdh[3];
+};
+
+// inter(x0,x1,x2,x,y0,y1,y2), paris.f90:2390-2411 (QUICK branch), with the
+// coordinate part from the table
+template <bool R>
+__device__ inline double inter_q(const QuickCoef* __restrict__ c, double y0, double y1, double y2) {
+    const double k = c->k, xi = c->xi;
+    double a, b;
+    if (R) {
+        a = ((y2 - k * k * y1 + (k * k - 1.0) * y0) * c->rk) * c->r1k;
+        b = ((y2 - k * y1 + (k - 1.0) * y0) * c->rk) * c->rkm1;
+    } else {
+        a = (y2 - k * k * y1 + (k * k - 1.0) * y0) / k / (1.0 - k);
+        b = (y2 - k * y1 + (k - 1.0) * y0) / k / (k - 1.0);
+    }
     return y0 + a * xi + b * (xi * xi);
 }
 
 // QUICK value of a component at its own cell centre ii along its axis
 // (work(:,:,:,d) of the component's own direction): phi at n, stride st
-__device__ inline double quick_same(const double* __restrict__ phi, long n, long st, const Ax& A, int ii, int g) {
-    double pm1 = phi[n - st], p0 = phi[n];
-    if (pm1 + p0 > 0.0)
-        return inter(A.h[ii - 1 + g], A.h[ii + g], A.h[ii - 2 + g], A.c[ii + g], pm1, p0, phi[n - 2 * st]);
-    return inter(A.h[ii + g], A.h[ii - 1 + g], A.h[ii + 1 + g], A.c[ii + g], p0, pm1, phi[n + st]);
+template <bool R>
+__device__ inline double quick_same(const double* __restrict__ phi, long n, long st, const QuickCoef* __restrict__ Q,
+                                    int t) {
+    const double pm1 = phi[n - st], p0 = phi[n];
+    const bool up = pm1 + p0 > 0.0;
+    const double y2 = phi[up ? n - 2 * st : n + st];
+    return inter_q<R>(Q + 4 * t + (up ? 0 : 1), up ? pm1 : p0, up ? p0 : pm1, y2);
+}
+// the same with the two coefficient sets of a uniform axis
+__device__ inline QuickCoef pick(bool up, const QuickCoef& a, const QuickCoef& b) {
+    return QuickCoef{up ? a.xi : b.xi, up ? a.k : b.k, up ? a.rk : b.rk, up ? a.r1k : b.r1k, up ? a.rkm1 : b.rkm1};
+}
+__device__ inline double quick_same_u(const double* __restrict__ phi, long n, long st, const QuickCoef& cu,
+                                      const QuickCoef& cd) {
+    const double pm1 = phi[n - st], p0 = phi[n];
+    const bool up = pm1 + p0 > 0.0;
+    const QuickCoef c = pick(up, cu, cd);
+    return inter_q<true>(&c, up ? pm1 : p0, up ? p0 : pm1, phi[up ? n - 2 * st : n + st]);
 }
 
 // QUICK value of a component on the face jj+1/2 of another axis, upwinded
 // by vel(n) + vel(n + sc)
+template <bool R>
 __device__ inline double quick_cross(const double* __restrict__ phi, const double* __restrict__ vel, long n, long st,
-                                     long sc, const Ax& A, int jj, int g) {
-    if (vel[n] + vel[n + sc] > 0.0)
-        return inter(A.c[jj + g], A.c[jj + 1 + g], A.c[jj - 1 + g], A.h[jj + g], phi[n], phi[n + st], phi[n - st]);
-    return inter(A.c[jj + 1 + g], A.c[jj + g], A.c[jj + 2 + g], A.h[jj + g], phi[n + st], phi[n], phi[n + 2 * st]);
+                                     long sc, const QuickCoef* __restrict__ Q, int t) {
+    const bool up = vel[n] + vel[n + sc] > 0.0;
+    const double a = phi[n], b = phi[n + st];
+    const double y2 = phi[up ? n - st : n + 2 * st];
+    return inter_q<R>(Q + 4 * t + (up ? 2 : 3), up ? a : b, up ? b : a, y2);
+}
+__device__ inline double quick_cross_u(const double* __restrict__ phi, const double* __restrict__ vel, long n, long st,
+                                       long sc, const QuickCoef& cu, const QuickCoef& cd) {
+    const double a = phi[n], b = phi[n + st];
+    const bool up = vel[n] + vel[n + sc] > 0.0;
+    const QuickCoef c = pick(up, cu, cd);
+    return inter_q<true>(&c, up ? a : b, up ? b : a, phi[up ? n - st : n + 2 * st]);
 }
 
-__device__ inline long stride(const Layout& L, int a) { return a == 0 ? 1 : (a == 1 ? L.pitch : L.plane); }
+// x / den, or x * (1/den) where that reciprocal is exact (same double)
+template <bool R>
+__device__ inline double over(double x, double den, double rden) {
+    return R ? x * rden : x / den;
+}
+
+// The coefficients of a uniform grid: every index carries the same four
+// coefficient sets and metric reciprocals per axis (checked bit for bit on
+// the host), passed by value so the kernel loads no table.
+struct QuickUniform {
+    QuickCoef q[3][4];
+    double d[3], dh[3], rd[3], rdh[3];
+};
 
 // momentumConvectionQUICK: du, dv, dw assigned on the faces project_velocity
 // updates (is..ieu etc.)
-__global__ void k_conv_quick(Vel V, double* __restrict__ du, double* __restrict__ dv, double* __restrict__ dw,
-                             const Layout L, const Bnd B, const Geo G) {
+template <bool R>
+__global__ void __launch_bounds__(256) k_conv_quick(Vel V, double* __restrict__ du, double* __restrict__ dv,
+                                                    double* __restrict__ dw, const Layout L, const Bnd B, const Geo G,
+                                                    const MomTab T) {
     int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
     if (i >= L.n[0] || j >= L.n[1] || k >= L.n[2]) return;
     const int g = L.ng;
     const long n = lidx(L, i, j, k), sx = 1, sy = L.pitch, sz = L.plane;
     const double *u = V.u, *v = V.v, *w = V.w;
-    const Ax &X = G.a[0], &Y = G.a[1], &Z = G.a[2];
+    const QuickCoef *QX = T.q[0], *QY = T.q[1], *QZ = T.q[2];
+    const int I = i + g, J = j + g, K = k + g;
     if (i < L.n[0] - 1 || B.per[0]) {
-        double a = quick_same(u, n + sx, sx, X, i + 1, g), b = quick_same(u, n, sx, X, i, g);
-        double w2 = quick_cross(u, v, n, sy, sx, Y, j, g), w2m = quick_cross(u, v, n - sy, sy, sx, Y, j - 1, g);
-        double w3 = quick_cross(u, w, n, sz, sx, Z, k, g), w3m = quick_cross(u, w, n - sz, sz, sx, Z, k - 1, g);
-        du[n] = -(a * a - b * b) / X.dh[i + g]
-            - 0.5 * ((v[n] + v[n + sx]) * w2 - (v[n - sy] + v[n + sx - sy]) * w2m) / Y.d[j + g]
-            - 0.5 * ((w[n] + w[n + sx]) * w3 - (w[n - sz] + w[n + sx - sz]) * w3m) / Z.d[k + g];
+        double a = quick_same<R>(u, n + sx, sx, QX, I + 1), b = quick_same<R>(u, n, sx, QX, I);
+        double w2 = quick_cross<R>(u, v, n, sy, sx, QY, J), w2m = quick_cross<R>(u, v, n - sy, sy, sx, QY, J - 1);
+        double w3 = quick_cross<R>(u, w, n, sz, sx, QZ, K), w3m = quick_cross<R>(u, w, n - sz, sz, sx, QZ, K - 1);
+        du[n] = over<R>(-(a * a - b * b), G.a[0].dh[I], T.rdh[0][I])
+            - over<R>(0.5 * ((v[n] + v[n + sx]) * w2 - (v[n - sy] + v[n + sx - sy]) * w2m), G.a[1].d[J], T.rd[1][J])
+            - over<R>(0.5 * ((w[n] + w[n + sx]) * w3 - (w[n - sz] + w[n + sx - sz]) * w3m), G.a[2].d[K], T.rd[2][K]);
     }
     if (j < L.n[1] - 1 || B.per[1]) {
-        double a = quick_same(v, n + sy, sy, Y, j + 1, g), b = quick_same(v, n, sy, Y, j, g);
-        double w1 = quick_cross(v, u, n, sx, sy, X, i, g), w1m = quick_cross(v, u, n - sx, sx, sy, X, i - 1, g);
-        double w3 = quick_cross(v, w, n, sz, sy, Z, k, g), w3m = quick_cross(v, w, n - sz, sz, sy, Z, k - 1, g);
-        dv[n] = -0.5 * ((u[n] + u[n + sy]) * w1 - (u[n - sx] + u[n - sx + sy]) * w1m) / X.d[i + g]
-            - (a * a - b * b) / Y.dh[j + g]
-            - 0.5 * ((w[n] + w[n + sy]) * w3 - (w[n - sz] + w[n + sy - sz]) * w3m) / Z.d[k + g];
+        double a = quick_same<R>(v, n + sy, sy, QY, J + 1), b = quick_same<R>(v, n, sy, QY, J);
+        double w1 = quick_cross<R>(v, u, n, sx, sy, QX, I), w1m = quick_cross<R>(v, u, n - sx, sx, sy, QX, I - 1);
+        double w3 = quick_cross<R>(v, w, n, sz, sy, QZ, K), w3m = quick_cross<R>(v, w, n - sz, sz, sy, QZ, K - 1);
+        dv[n] = over<R>(-0.5 * ((u[n] + u[n + sy]) * w1 - (u[n - sx] + u[n - sx + sy]) * w1m), G.a[0].d[I], T.rd[0][I])
+            - over<R>(a * a - b * b, G.a[1].dh[J], T.rdh[1][J])
+            - over<R>(0.5 * ((w[n] + w[n + sy]) * w3 - (w[n - sz] + w[n + sy - sz]) * w3m), G.a[2].d[K], T.rd[2][K]);
     }
     if (k < L.n[2] - 1 || B.per[2]) {
-        double a = quick_same(w, n + sz, sz, Z, k + 1, g), b = quick_same(w, n, sz, Z, k, g);
-        double w1 = quick_cross(w, u, n, sx, sz, X, i, g), w1m = quick_cross(w, u, n - sx, sx, sz, X, i - 1, g);
-        double w2 = quick_cross(w, v, n, sy, sz, Y, j, g), w2m = quick_cross(w, v, n - sy, sy, sz, Y, j - 1, g);
-        dw[n] = -0.5 * ((u[n] + u[n + sz]) * w1 - (u[n - sx] + u[n - sx + sz]) * w1m) / X.d[i + g]
-            - 0.5 * ((v[n] + v[n + sz]) * w2 - (v[n - sy] + v[n - sy + sz]) * w2m) / Y.d[j + g]
-            - (a * a - b * b) / Z.dh[k + g];
+        double a = quick_same<R>(w, n + sz, sz, QZ, K + 1), b = quick_same<R>(w, n, sz, QZ, K);
+        double w1 = quick_cross<R>(w, u, n, sx, sz, QX, I), w1m = quick_cross<R>(w, u, n - sx, sx, sz, QX, I - 1);
+        double w2 = quick_cross<R>(w, v, n, sy, sz, QY, J), w2m = quick_cross<R>(w, v, n - sy, sy, sz, QY, J - 1);
+        dw[n] = over<R>(-0.5 * ((u[n] + u[n + sz]) * w1 - (u[n - sx] + u[n - sx + sz]) * w1m), G.a[0].d[I], T.rd[0][I])
+            - over<R>(0.5 * ((v[n] + v[n + sz]) * w2 - (v[n - sy] + v[n - sy + sz]) * w2m), G.a[1].d[J], T.rd[1][J])
+            - over<R>(a * a - b * b, G.a[2].dh[K], T.rdh[2][K]);
+    }
+}
+
+// momentumConvectionQUICK on a uniform grid with exact reciprocals
+__global__ void __launch_bounds__(256) k_conv_quick_uniform(Vel V, double* __restrict__ du, double* __restrict__ dv,
+                                                            double* __restrict__ dw, const Layout L, const Bnd B,
+                                                            const QuickUniform Q) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= L.n[0] || j >= L.n[1] || k >= L.n[2]) return;
+    const long n = lidx(L, i, j, k), sx = 1, sy = L.pitch, sz = L.plane;
+    const double *u = V.u, *v = V.v, *w = V.w;
+    if (i < L.n[0] - 1 || B.per[0]) {
+        double a = quick_same_u(u, n + sx, sx, Q.q[0][0], Q.q[0][1]), b = quick_same_u(u, n, sx, Q.q[0][0], Q.q[0][1]);
+        double w2 = quick_cross_u(u, v, n, sy, sx, Q.q[1][2], Q.q[1][3]);
+        double w2m = quick_cross_u(u, v, n - sy, sy, sx, Q.q[1][2], Q.q[1][3]);
+        double w3 = quick_cross_u(u, w, n, sz, sx, Q.q[2][2], Q.q[2][3]);
+        double w3m = quick_cross_u(u, w, n - sz, sz, sx, Q.q[2][2], Q.q[2][3]);
+        du[n] = -(a * a - b * b) * Q.rdh[0]
+            - (0.5 * ((v[n] + v[n + sx]) * w2 - (v[n - sy] + v[n + sx - sy]) * w2m)) * Q.rd[1]
+            - (0.5 * ((w[n] + w[n + sx]) * w3 - (w[n - sz] + w[n + sx - sz]) * w3m)) * Q.rd[2];
+    }
+    if (j < L.n[1] - 1 || B.per[1]) {
+        double a = quick_same_u(v, n + sy, sy, Q.q[1][0], Q.q[1][1]), b = quick_same_u(v, n, sy, Q.q[1][0], Q.q[1][1]);
+        double w1 = quick_cross_u(v, u, n, sx, sy, Q.q[0][2], Q.q[0][3]);
+        double w1m = quick_cross_u(v, u, n - sx, sx, sy, Q.q[0][2], Q.q[0][3]);
+        double w3 = quick_cross_u(v, w, n, sz, sy, Q.q[2][2], Q.q[2][3]);
+        double w3m = quick_cross_u(v, w, n - sz, sz, sy, Q.q[2][2], Q.q[2][3]);
+        dv[n] = (-0.5 * ((u[n] + u[n + sy]) * w1 - (u[n - sx] + u[n - sx + sy]) * w1m)) * Q.rd[0]
+            - (a * a - b * b) * Q.rdh[1]
+            - (0.5 * ((w[n] + w[n + sy]) * w3 - (w[n - sz] + w[n + sy - sz]) * w3m)) * Q.rd[2];
+    }
+    if (k < L.n[2] - 1 || B.per[2]) {
+        double a = quick_same_u(w, n + sz, sz, Q.q[2][0], Q.q[2][1]), b = quick_same_u(w, n, sz, Q.q[2][0], Q.q[2][1]);
+        double w1 = quick_cross_u(w, u, n, sx, sz, Q.q[0][2], Q.q[0][3]);
+        double w1m = quick_cross_u(w, u, n - sx, sx, sz, Q.q[0][2], Q.q[0][3]);
+        double w2 = quick_cross_u(w, v, n, sy, sz, Q.q[1][2], Q.q[1][3]);
+        double w2m = quick_cross_u(w, v, n - sy, sy, sz, Q.q[1][2], Q.q[1][3]);
+        dw[n] = (-0.5 * ((u[n] + u[n + sz]) * w1 - (u[n - sx] + u[n - sx + sz]) * w1m)) * Q.rd[0]
+            - (0.5 * ((v[n] + v[n + sz]) * w2 - (v[n - sy] + v[n - sy + sz]) * w2m)) * Q.rd[1]
+            - (a * a - b * b) * Q.rdh[2];
     }
 }
 
@@ -161,16 +266,22 @@ __global__ void k_conv_onedim(Vel V, double* __restrict__ du, double* __restrict
 namespace {
 
 // explicitMomDiff, paris.f90:2757-2808 (adds to du, dv, dw)
-__global__ void k_mom_diff(Vel V, const double* __restrict__ rho, const double* __restrict__ mu,
-                           double* __restrict__ du, double* __restrict__ dv, double* __restrict__ dw, const Layout L,
-                           const Bnd B, const Geo G) {
+template <bool UNI>
+__global__ void __launch_bounds__(256) k_mom_diff(Vel V, const double* __restrict__ rho, const double* __restrict__ mu,
+                                                  double* __restrict__ du, double* __restrict__ dv,
+                                                  double* __restrict__ dw, const Layout L, const Bnd B, const MomTab T,
+                                                  const QuickUniform Q) {
     int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
     if (i >= L.n[0] || j >= L.n[1] || k >= L.n[2]) return;
     const int g = L.ng;
     const long n = lidx(L, i, j, k), sx = 1, sy = L.pitch, sz = L.plane;
     const double *u = V.u, *v = V.v, *w = V.w;
-    const double *dx = G.a[0].d, *dxh = G.a[0].dh, *dy = G.a[1].d, *dyh = G.a[1].dh, *dz = G.a[2].d,
-                 *dzh = G.a[2].dh;
+    // 1./dx(i) etc. from the table (the same IEEE divisions, done once per
+    // index), or on a uniform grid the one value every index holds
+    const double *rdx = T.rd[0], *rdxh = T.rdh[0], *rdy = T.rd[1], *rdyh = T.rdh[1], *rdz = T.rd[2],
+                 *rdzh = T.rdh[2];
+#define RD(p, a, t) (UNI ? Q.rd[a] : p[t])
+#define RDH(p, a, t) (UNI ? Q.rdh[a] : p[t])
     const int I = i + g, J = j + g, K = k + g;   // metric index
 #define M(o) mu[n + (o)]
 #define U(o) u[n + (o)]
@@ -178,43 +289,45 @@ __global__ void k_mom_diff(Vel V, const double* __restrict__ rho, const double* 
 #define W(o) w[n + (o)]
     if (i < L.n[0] - 1 || B.per[0]) {
         du[n] = du[n] + (
-            (1. / dxh[I]) * 2. * (M(sx) * (1. / dx[I + 1]) * (U(sx) - U(0)) - M(0) * (1. / dx[I]) * (U(0) - U(-sx)))
-            + (1. / dy[J]) * (0.25 * (M(0) + M(sx) + M(sx + sy) + M(sy)) *
-                                  ((1. / dyh[J]) * (U(sy) - U(0)) + (1. / dxh[I]) * (VV(sx) - VV(0))) -
+            RDH(rdxh, 0, I) * 2. * (M(sx) * RD(rdx, 0, I + 1) * (U(sx) - U(0)) - M(0) * RD(rdx, 0, I) * (U(0) - U(-sx)))
+            + RD(rdy, 1, J) * (0.25 * (M(0) + M(sx) + M(sx + sy) + M(sy)) *
+                                  (RDH(rdyh, 1, J) * (U(sy) - U(0)) + RDH(rdxh, 0, I) * (VV(sx) - VV(0))) -
                               0.25 * (M(0) + M(sx) + M(sx - sy) + M(-sy)) *
-                                  ((1. / dyh[J - 1]) * (U(0) - U(-sy)) + (1. / dxh[I]) * (VV(sx - sy) - VV(-sy))))
-            + (1. / dz[K]) * (0.25 * (M(0) + M(sx) + M(sx + sz) + M(sz)) *
-                                  ((1. / dzh[K]) * (U(sz) - U(0)) + (1. / dxh[I]) * (W(sx) - W(0))) -
+                                  (RDH(rdyh, 1, J - 1) * (U(0) - U(-sy)) + RDH(rdxh, 0, I) * (VV(sx - sy) - VV(-sy))))
+            + RD(rdz, 2, K) * (0.25 * (M(0) + M(sx) + M(sx + sz) + M(sz)) *
+                                  (RDH(rdzh, 2, K) * (U(sz) - U(0)) + RDH(rdxh, 0, I) * (W(sx) - W(0))) -
                               0.25 * (M(0) + M(sx) + M(sx - sz) + M(-sz)) *
-                                  ((1. / dzh[K - 1]) * (U(0) - U(-sz)) + (1. / dxh[I]) * (W(sx - sz) - W(-sz))))
+                                  (RDH(rdzh, 2, K - 1) * (U(0) - U(-sz)) + RDH(rdxh, 0, I) * (W(sx - sz) - W(-sz))))
             ) / (0.5 * (rho[n + sx] + rho[n]));
     }
     if (j < L.n[1] - 1 || B.per[1]) {
         dv[n] = dv[n] + (
-            (1. / dx[I]) * (0.25 * (M(0) + M(sx) + M(sx + sy) + M(sy)) *
-                                ((1. / dyh[J]) * (U(sy) - U(0)) + (1. / dxh[I]) * (VV(sx) - VV(0))) -
+            RD(rdx, 0, I) * (0.25 * (M(0) + M(sx) + M(sx + sy) + M(sy)) *
+                                (RDH(rdyh, 1, J) * (U(sy) - U(0)) + RDH(rdxh, 0, I) * (VV(sx) - VV(0))) -
                             0.25 * (M(0) + M(sy) + M(sy - sx) + M(-sx)) *
-                                ((1. / dyh[J]) * (U(sy - sx) - U(-sx)) + (1. / dxh[I - 1]) * (VV(0) - VV(-sx))))
-            + (1. / dyh[J]) * 2. * (M(sy) * (1. / dy[J + 1]) * (VV(sy) - VV(0)) - M(0) * (1. / dy[J]) * (VV(0) - VV(-sy)))
-            + (1. / dz[K]) * (0.25 * (M(0) + M(sy) + M(sy + sz) + M(sz)) *
-                                  ((1. / dzh[K]) * (VV(sz) - VV(0)) + (1. / dyh[J]) * (W(sy) - W(0))) -
+                                (RDH(rdyh, 1, J) * (U(sy - sx) - U(-sx)) + RDH(rdxh, 0, I - 1) * (VV(0) - VV(-sx))))
+            + RDH(rdyh, 1, J) * 2. * (M(sy) * RD(rdy, 1, J + 1) * (VV(sy) - VV(0)) - M(0) * RD(rdy, 1, J) * (VV(0) - VV(-sy)))
+            + RD(rdz, 2, K) * (0.25 * (M(0) + M(sy) + M(sy + sz) + M(sz)) *
+                                  (RDH(rdzh, 2, K) * (VV(sz) - VV(0)) + RDH(rdyh, 1, J) * (W(sy) - W(0))) -
                               0.25 * (M(0) + M(sy) + M(sy - sz) + M(-sz)) *
-                                  ((1. / dzh[K - 1]) * (VV(0) - VV(-sz)) + (1. / dyh[J]) * (W(sy - sz) - W(-sz))))
+                                  (RDH(rdzh, 2, K - 1) * (VV(0) - VV(-sz)) + RDH(rdyh, 1, J) * (W(sy - sz) - W(-sz))))
             ) / (0.5 * (rho[n + sy] + rho[n]));
     }
     if (k < L.n[2] - 1 || B.per[2]) {
         dw[n] = dw[n] + (
-            (1. / dx[I]) * (0.25 * (M(0) + M(sx) + M(sx + sz) + M(sz)) *
-                                ((1. / dzh[K]) * (U(sz) - U(0)) + (1. / dxh[I]) * (W(sx) - W(0))) -
+            RD(rdx, 0, I) * (0.25 * (M(0) + M(sx) + M(sx + sz) + M(sz)) *
+                                (RDH(rdzh, 2, K) * (U(sz) - U(0)) + RDH(rdxh, 0, I) * (W(sx) - W(0))) -
                             0.25 * (M(0) + M(-sx) + M(-sx + sz) + M(sz)) *
-                                ((1. / dzh[K]) * (U(-sx + sz) - U(-sx)) + (1. / dxh[I - 1]) * (W(0) - W(-sx))))
-            + (1. / dy[J]) * (0.25 * (M(0) + M(sy) + M(sy + sz) + M(sz)) *
-                                  ((1. / dzh[K]) * (VV(sz) - VV(0)) + (1. / dyh[J]) * (W(sy) - W(0))) -
+                                (RDH(rdzh, 2, K) * (U(-sx + sz) - U(-sx)) + RDH(rdxh, 0, I - 1) * (W(0) - W(-sx))))
+            + RD(rdy, 1, J) * (0.25 * (M(0) + M(sy) + M(sy + sz) + M(sz)) *
+                                  (RDH(rdzh, 2, K) * (VV(sz) - VV(0)) + RDH(rdyh, 1, J) * (W(sy) - W(0))) -
                               0.25 * (M(0) + M(-sy) + M(-sy + sz) + M(sz)) *
-                                  ((1. / dzh[K]) * (VV(-sy + sz) - VV(-sy)) + (1. / dyh[J - 1]) * (W(0) - W(-sy))))
-            + (1. / dzh[K]) * 2. * (M(sz) * (1. / dz[K + 1]) * (W(sz) - W(0)) - M(0) * (1. / dz[K]) * (W(0) - W(-sz)))
+                                  (RDH(rdzh, 2, K) * (VV(-sy + sz) - VV(-sy)) + RDH(rdyh, 1, J - 1) * (W(0) - W(-sy))))
+            + RDH(rdzh, 2, K) * 2. * (M(sz) * RD(rdz, 2, K + 1) * (W(sz) - W(0)) - M(0) * RD(rdz, 2, K) * (W(0) - W(-sz)))
             ) / (0.5 * (rho[n + sz] + rho[n]));
     }
+#undef RD
+#undef RDH
 #undef M
 #undef U
 #undef VV
@@ -306,6 +419,109 @@ Geo geo(const paris_ctx* c) {
 }
 Vel vel(const paris_ctx* c) { return Vel{c->fld[PARIS_FIELD_U], c->fld[PARIS_FIELD_V], c->fld[PARIS_FIELD_W]}; }
 
+bool pow2(double x) {
+    int e;
+    const double m = std::frexp(x, &e);
+    return m == 0.5 || m == -0.5;
+}
+
+// The per-index tables of MomTab, built once per grid on the host from the
+// host copies of the coordinates (the same doubles the device holds).
+int mom_tables(paris_ctx* c, MomTab* T, bool* exact, QuickUniform* U = nullptr, bool* uniform = nullptr) {
+    const int g = c->L.ng;
+    const std::vector<double>* C[3] = {&c->h_x, &c->h_y, &c->h_z};
+    const std::vector<double>* H[3] = {&c->h_xh, &c->h_yh, &c->h_zh};
+    const std::vector<double>* D[3] = {&c->h_dx, &c->h_dy, &c->h_dz};
+    const std::vector<double>* DH[3] = {&c->h_dxh, &c->h_dyh, &c->h_dzh};
+    const int per = (int)(sizeof(QuickCoef) / sizeof(double));   // doubles per coefficient set
+    long off[3], total = 0;
+    for (int a = 0; a < 3; a++) {
+        off[a] = total;
+        total += (long)C[a]->size() * (4 * per + 2);
+    }
+    if (!c->mom_tab) {
+        std::vector<double> tab(total, 0.0);
+        bool ex = true;
+        for (int a = 0; a < 3; a++) {
+            const std::vector<double>&x = *C[a], &xh = *H[a], &d = *D[a], &dh = *DH[a];
+            const int nt = (int)x.size(), n = c->L.n[a];
+            QuickCoef* Q = reinterpret_cast<QuickCoef*>(tab.data() + off[a]);
+            double* rd = tab.data() + off[a] + 4L * per * nt;
+            double* rdh = rd + nt;
+            // inter(x0,x1,x2,x): xi and k exactly as inter() forms them
+            auto set = [&](QuickCoef& q, double x0, double x1, double x2, double xx, bool used) {
+                q.xi = (xx - x0) / (x1 - x0);
+                q.k = (x2 - x0) / (x1 - x0);
+                const double omk = 1.0 - q.k, km1 = q.k - 1.0;
+                q.rk = 1.0 / q.k;
+                q.r1k = 1.0 / omk;
+                q.rkm1 = 1.0 / km1;
+                if (used) ex = ex && pow2(q.k) && pow2(omk) && pow2(km1);
+            };
+            for (int t = 0; t < nt; t++) {
+                // own axis: ii = t - g in [0, n]; cross axis: jj = t - g in [-1, n-1]
+                const bool own = t >= g && t <= n + g, cross = t >= g - 1 && t <= n + g - 1;
+                if (t >= 2) set(Q[4 * t + 0], xh[t - 1], xh[t], xh[t - 2], x[t], own);
+                if (t >= 1 && t + 1 < nt) set(Q[4 * t + 1], xh[t], xh[t - 1], xh[t + 1], x[t], own);
+                if (t >= 1 && t + 1 < nt) set(Q[4 * t + 2], x[t], x[t + 1], x[t - 1], xh[t], cross);
+                if (t + 2 < nt) set(Q[4 * t + 3], x[t + 1], x[t], x[t + 2], xh[t], cross);
+                rd[t] = 1. / d[t];
+                rdh[t] = 1. / dh[t];
+                if (t >= g && t < n + g) ex = ex && pow2(d[t]) && pow2(dh[t]);
+            }
+        }
+        PARIS_CUDA_TRY(c, cudaMalloc(&c->mom_tab, total * sizeof(double)));
+        PARIS_CUDA_TRY(c, cudaMemcpy(c->mom_tab, tab.data(), total * sizeof(double), cudaMemcpyHostToDevice));
+        c->mom_tab_exact = ex ? 1 : 0;
+    }
+    for (int a = 0; a < 3; a++) {
+        const long nt = (long)C[a]->size();
+        T->q[a] = reinterpret_cast<const QuickCoef*>(c->mom_tab + off[a]);
+        T->rd[a] = c->mom_tab + off[a] + 4L * per * nt;
+        T->rdh[a] = T->rd[a] + nt;
+    }
+    *exact = c->mom_tab_exact != 0;
+    if (uniform) {
+        // every index the kernel reads holds the same coefficients, bit for bit
+        // (then rebuilt here from the host coordinates: same arithmetic)
+        bool uni = *exact;
+        for (int a = 0; a < 3 && uni; a++) {
+            const std::vector<double>&x = *C[a], &xh = *H[a], &d = *D[a], &dh = *DH[a];
+            const int n = c->L.n[a];
+            auto coef = [&](int v, int t) {
+                QuickCoef q;
+                double x0, x1, x2, xx;
+                if (v == 0) { x0 = xh[t - 1]; x1 = xh[t]; x2 = xh[t - 2]; xx = x[t]; }
+                else if (v == 1) { x0 = xh[t]; x1 = xh[t - 1]; x2 = xh[t + 1]; xx = x[t]; }
+                else if (v == 2) { x0 = x[t]; x1 = x[t + 1]; x2 = x[t - 1]; xx = xh[t]; }
+                else { x0 = x[t + 1]; x1 = x[t]; x2 = x[t + 2]; xx = xh[t]; }
+                q.xi = (xx - x0) / (x1 - x0);
+                q.k = (x2 - x0) / (x1 - x0);
+                q.rk = 1.0 / q.k;
+                q.r1k = 1.0 / (1.0 - q.k);
+                q.rkm1 = 1.0 / (q.k - 1.0);
+                return q;
+            };
+            auto same = [](const QuickCoef& p, const QuickCoef& q) {
+                return p.xi == q.xi && p.k == q.k && p.rk == q.rk && p.r1k == q.r1k && p.rkm1 == q.rkm1;
+            };
+            for (int v = 0; v < 4; v++) {
+                const int t0 = v < 2 ? g : g - 1, t1 = v < 2 ? n + g : n + g - 1;
+                U->q[a][v] = coef(v, t0);
+                for (int t = t0 + 1; t <= t1 && uni; t++) uni = same(coef(v, t), U->q[a][v]);
+            }
+            U->d[a] = d[g];
+            U->dh[a] = dh[g];
+            // explicitMomDiff reads the metric one index beyond the interior
+            for (int t = g - 1; t <= n + g && uni; t++) uni = d[t] == d[g] && dh[t] == dh[g];
+            U->rd[a] = 1. / d[g];
+            U->rdh[a] = 1. / dh[g];
+        }
+        *uniform = uni;
+    }
+    return PARIS_OK;
+}
+
 int need(paris_ctx* c, std::initializer_list<int> fields) {
     for (int f : fields) PARIS_CHECK(ctx_alloc_field(c, f));
     return PARIS_OK;
@@ -321,10 +537,23 @@ extern "C" int paris_momentum_convection(paris_handle_t c, int32_t scheme) {
     }
     cudaSetDevice(c->dev);
     PARIS_CHECK(need(c, {PARIS_FIELD_U, PARIS_FIELD_V, PARIS_FIELD_W, PARIS_FIELD_DU, PARIS_FIELD_DV, PARIS_FIELD_DW}));
-    if (scheme == PARIS_CONV_QUICK)
-        PARIS_LAUNCH_N(c, "mom_convection", c->N, k_conv_quick, cgrid(c->L), cblock(), 0, vel(c), c->fld[PARIS_FIELD_DU],
-                       c->fld[PARIS_FIELD_DV], c->fld[PARIS_FIELD_DW], c->L, c->bnd, geo(c));
-    else
+    if (scheme == PARIS_CONV_QUICK) {
+        MomTab T;
+        QuickUniform U;
+        bool exact, uniform;
+        PARIS_CHECK(mom_tables(c, &T, &exact, &U, &uniform));
+        if (uniform)
+            PARIS_LAUNCH_N(c, "mom_convection", c->N, k_conv_quick_uniform, cgrid(c->L), cblock(), 0, vel(c),
+                           c->fld[PARIS_FIELD_DU], c->fld[PARIS_FIELD_DV], c->fld[PARIS_FIELD_DW], c->L, c->bnd, U);
+        else if (exact)
+            PARIS_LAUNCH_N(c, "mom_convection", c->N, k_conv_quick<true>, cgrid(c->L), cblock(), 0, vel(c),
+                           c->fld[PARIS_FIELD_DU], c->fld[PARIS_FIELD_DV], c->fld[PARIS_FIELD_DW], c->L, c->bnd, geo(c),
+                           T);
+        else
+            PARIS_LAUNCH_N(c, "mom_convection", c->N, k_conv_quick<false>, cgrid(c->L), cblock(), 0, vel(c),
+                           c->fld[PARIS_FIELD_DU], c->fld[PARIS_FIELD_DV], c->fld[PARIS_FIELD_DW], c->L, c->bnd, geo(c),
+                           T);
+    } else
         PARIS_LAUNCH_N(c, "mom_convection", c->N, k_conv_onedim, cgrid(c->L), cblock(), 0, vel(c),
                        c->fld[PARIS_FIELD_DU], c->fld[PARIS_FIELD_DV], c->fld[PARIS_FIELD_DW], c->L, c->bnd, geo(c),
                        scheme);
@@ -335,9 +564,18 @@ extern "C" int paris_explicit_mom_diff(paris_handle_t c) {
     if (!c) return PARIS_BAD_ARGS;
     cudaSetDevice(c->dev);
     PARIS_CHECK(need(c, {PARIS_FIELD_MU, PARIS_FIELD_DU, PARIS_FIELD_DV, PARIS_FIELD_DW}));
-    PARIS_LAUNCH_N(c, "mom_diffusion", c->N, k_mom_diff, cgrid(c->L), cblock(), 0, vel(c), c->fld[PARIS_FIELD_RHO],
-                   c->fld[PARIS_FIELD_MU], c->fld[PARIS_FIELD_DU], c->fld[PARIS_FIELD_DV], c->fld[PARIS_FIELD_DW], c->L,
-                   c->bnd, geo(c));
+    MomTab T;
+    QuickUniform U;
+    bool exact, uniform;
+    PARIS_CHECK(mom_tables(c, &T, &exact, &U, &uniform));
+    if (uniform)
+        PARIS_LAUNCH_N(c, "mom_diffusion", c->N, k_mom_diff<true>, cgrid(c->L), cblock(), 0, vel(c),
+                       c->fld[PARIS_FIELD_RHO], c->fld[PARIS_FIELD_MU], c->fld[PARIS_FIELD_DU], c->fld[PARIS_FIELD_DV],
+                       c->fld[PARIS_FIELD_DW], c->L, c->bnd, T, U);
+    else
+        PARIS_LAUNCH_N(c, "mom_diffusion", c->N, k_mom_diff<false>, cgrid(c->L), cblock(), 0, vel(c),
+                       c->fld[PARIS_FIELD_RHO], c->fld[PARIS_FIELD_MU], c->fld[PARIS_FIELD_DU], c->fld[PARIS_FIELD_DV],
+                       c->fld[PARIS_FIELD_DW], c->L, c->bnd, T, U);
     return PARIS_OK;
 }
 

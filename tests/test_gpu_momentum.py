@@ -9,8 +9,12 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def fields(capi, orc, n, bc, seed):
-    d = capi.make_desc((n, n + 4, n - 2), bc=bc, rho1=1.2, rho2=1000.0, mu1=1.7e-5, mu2=1e-3)
+def fields(capi, orc, n, bc, seed, grid="general"):
+    # "pow2": 16^3 on the unit cube, where the QUICK kernel multiplies by the
+    # exact reciprocals of its powers of two; "general": 16x20x14 (cells of
+    # 1/20 and 1/14 along y and z), where it divides
+    shape = (n, n, n) if grid == "pow2" else (n, n + 4, n - 2)
+    d = capi.make_desc(shape, bc=bc, rho1=1.2, rho2=1000.0, mu1=1.7e-5, mu2=1e-3)
     rng = np.random.default_rng(seed)
     u, v, w = (rng.standard_normal(orc.shape(d)) for _ in range(3))
     orc.set_velocity_bc(d, u, v, w)          # consistent ghosts (walls: reflected, periodic: images)
@@ -24,10 +28,11 @@ def upload(gpu, capi, **kw):
         gpu.upload(getattr(capi, "F_" + name.upper()), a)
 
 
+@pytest.mark.parametrize("grid", ["general", "pow2"])
 @pytest.mark.parametrize("bc", ["periodic", "wall"])
 @pytest.mark.parametrize("scheme", [0, 1, 2, 3])
-def test_convection_bitwise(gpu_lib, capi, runtime, orc, bc, scheme):
-    d, u, v, w, rho, mu = fields(capi, orc, 16, bc, 1)
+def test_convection_bitwise(gpu_lib, capi, runtime, orc, bc, scheme, grid):
+    d, u, v, w, rho, mu = fields(capi, orc, 16, bc, 1, grid)
     sentinel = [orc.zeros(d) + 7.0 + q for q in range(3)]   # entries the scheme leaves alone stay
     ref = [a.copy() for a in sentinel]
     assert orc.momentum_convection(d, scheme, u, v, w, *ref) == 0
@@ -40,9 +45,10 @@ def test_convection_bitwise(gpu_lib, capi, runtime, orc, bc, scheme):
         assert (b != s).any()
 
 
+@pytest.mark.parametrize("grid", ["general", "pow2"])
 @pytest.mark.parametrize("bc", ["periodic", "wall"])
-def test_diffusion_force_advance_bitwise(gpu_lib, capi, runtime, orc, bc):
-    d, u, v, w, rho, mu = fields(capi, orc, 16, bc, 2)
+def test_diffusion_force_advance_bitwise(gpu_lib, capi, runtime, orc, bc, grid):
+    d, u, v, w, rho, mu = fields(capi, orc, 16, bc, 2, grid)
     rng = np.random.default_rng(3)
     du, dv, dw = (rng.standard_normal(orc.shape(d)) for _ in range(3))
     ref = [a.copy() for a in (du, dv, dw)]

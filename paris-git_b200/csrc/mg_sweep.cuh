@@ -14,7 +14,8 @@
 // array is read from HBM once per sweep (the ring re-reads hit L2).  The
 // iterate is read from `xin` (nullptr: zero) and written to `xout`, never in
 // place, so blocks never see each other's new values and the sweep computes
-// exactly the two colour passes of k_fast_smooth.  With `xc`, the coarse-grid
+// the two colour passes of k_fast_smooth (in FP64 exactly; in FP32 with the
+// update arithmetic of SwUpd<float>).  With `xc`, the coarse-grid
 // correction (injection from the level below) is added to the iterate as it
 // arrives, fetched into registers one step ahead.  Ring-buffer slots rotate
 // with the step.
@@ -74,6 +75,32 @@ __device__ inline int sw_wrap(int a, int n, int per) {
     a %= n;
     return a < 0 ? a + n : a;
 }
+
+// The Gauss-Seidel update x = s / d of one cell.  FP32 (the inner cycle of
+// the mixed solver): the sums as trees of depth three instead of chains of
+// seven dependent adds, and the fast division (two ulps); the smoother only
+// has to reduce the error, the FP64 outer loop keeps the residual exact.
+// FP64: the sums in the order of A1..A6 and the IEEE division.
+template <typename T>
+struct SwUpd {
+    __device__ static inline bool apply(T a1, T a2, T a3, T a4, T a5, T a6, T x1, T x2, T x3, T x4, T x5, T x6, T b,
+                                        T& out) {
+        T d = a1 + a2 + a3 + a4 + a5 + a6;
+        T s = a1 * x1 + a2 * x2 + a3 * x3 + a4 * x4 + a5 * x5 + a6 * x6 + b;
+        if (d > (T)0) { out = s / d; return true; }
+        return false;
+    }
+};
+template <>
+struct SwUpd<float> {
+    __device__ static inline bool apply(float a1, float a2, float a3, float a4, float a5, float a6, float x1,
+                                        float x2, float x3, float x4, float x5, float x6, float b, float& out) {
+        const float d = ((a1 + a2) + (a3 + a4)) + (a5 + a6);
+        const float s = ((a1 * x1 + a2 * x2) + (a3 * x3 + a4 * x4)) + ((a5 * x5 + a6 * x6) + b);
+        if (d > 0.f) { out = __fdividef(s, d); return true; }
+        return false;
+    }
+};
 
 __device__ inline int sw_next(int s, int S) { return s + 1 == S ? 0 : s + 1; }
 // (s + d) mod S for |d| < S
@@ -245,9 +272,10 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
     auto update = [&](int r, T* xk, const T* xm, const T* xp, const T* cxk, const T* cyk, const T* bk,
                       const T* czk, const T* czm) {
         T a1 = cxk[r - 1], a2 = cxk[r], a3 = cyk[r - RX], a4 = cyk[r], a5 = czm[r], a6 = czk[r];
-        T d = a1 + a2 + a3 + a4 + a5 + a6;
-        T s = a1 * xk[r - 1] + a2 * xk[r + 1] + a3 * xk[r - RX] + a4 * xk[r + RX] + a5 * xm[r] + a6 * xp[r] + bk[r];
-        if (d > (T)0) xk[r] = s / d;
+        T out;
+        if (SwUpd<T>::apply(a1, a2, a3, a4, a5, a6, xk[r - 1], xk[r + 1], xk[r - RX], xk[r + RX], xm[r], xp[r], bk[r],
+                            out))
+            xk[r] = out;
     };
     // F at plane k (tile + ring) and S at plane k (tile) with its output; the
     // slot pointers of the planes involved are passed in

@@ -274,6 +274,29 @@ int paris_project_velocity(paris_handle_t h, double dt);
 int paris_calc_residuals_noalloc(int32_t nx, int32_t ny, int32_t nz, int32_t ng, const double* A_dev,
                                  const double* p_dev, double* out3, void* stream);
 
+/* ---- on-disk formats ---------------------------------------------------- */
+/* backup_VOF_write, vofmodules.f90:2033-2059: the restart text file of a VOF
+ * run (header FORMAT(es17.8e3,7I10) time, itimestep, imin..kmax, then
+ * FORMAT(5es25.16e3) u, v, w, p, cvof over k, j, i of the ghosted arrays)
+ * from the device fields; an existing file is first renamed <file>.old.   */
+int paris_backup_vof_write(paris_handle_t h, const char* filename, double time, int32_t itimestep);
+/* backup_VOF_read, vofmodules.f90:2063-2085, and the restart ghosts of
+ * paris.f90:3174-3178: loads u, v, w, p, cvof to the device, vof_flag from
+ * cvof (get_flags_and_clip), SetVOFBC and the periodic ghosts of cvof, the
+ * flags and the velocities.  A file of another grid returns PARIS_BAD_ARGS
+ * (the reference stops with "Error: backup_read").  time, itimestep may be
+ * NULL.                                                                   */
+int paris_backup_vof_read(paris_handle_t h, const char* filename, double* time, int32_t* itimestep);
+#define PARIS_VTK_STRUCTURED_GRID    2   /* output_format = 2, output_VOF_VTKSG */
+#define PARIS_VTK_STRUCTURED_POINTS  3   /* output_format = 3, output_VOF_VTKSP */
+/* output_VOF(nf,i1,i2,j1,j2,k1,k2), vofmodules.f90:1908-2031: one VTK file
+ * of cvof over the Fortran index box range = {i1,i2,j1,j2,k1,k2} (1-based,
+ * ghosts included: 1..N+2Ng), or NULL for is..ie+1, js..je+1, ks..ke+1 as
+ * the step loop writes it; filtered = output_filtered_VOF (27-point filter
+ * with weights 8, 4, 2, 1 / 64).                                          */
+int paris_output_vof_vtk(paris_handle_t h, const char* filename, int32_t format, double time, const int32_t* range,
+                         int32_t filtered);
+
 /* ---- projection adjoint.  No counterpart in the reference: the transpose
  *      of SetupPoisson (modules.f90:2722-2753) + NewSolver + project_velocity
  *      (paris.f90:898-909).  With B_f = 2/(rho_L + rho_R) on every face,

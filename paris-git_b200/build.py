@@ -29,6 +29,7 @@ SOURCES = {
     "st.cu": True,
     "momentum.cu": True,
     "stats.cu": True,
+    "io.cu": True,
 }
 
 

@@ -68,6 +68,7 @@ class SolveOpts(ctypes.Structure):
     ]
 
 
+VTK_STRUCTURED_GRID, VTK_STRUCTURED_POINTS = 2, 3
 NSTATS = 25
 STATS_RISING_BUBBLE, STATS_PHASE_INVERSION, STATS_TURB = 1, 2, 4
 
@@ -170,6 +171,9 @@ _PROTOS = {
     "paris_time_step_size": (_I, [_P, _D, _D, _D, _P, _P]),
     "paris_get_cfl_and_check": (_I, [_P, _D, _D, _P]),
     "paris_calc_stats": (_I, [_P, ctypes.POINTER(StatsOpts), _P]),
+    "paris_backup_vof_write": (_I, [_P, ctypes.c_char_p, _D, _I]),
+    "paris_backup_vof_read": (_I, [_P, ctypes.c_char_p, _P, _P]),
+    "paris_output_vof_vtk": (_I, [_P, ctypes.c_char_p, _I, _D, _P, _I]),
     "paris_setup_poisson": (_I, [_P, _D, _D]),
     "paris_setup_test_mg": (_I, [_P]),
     "paris_new_solver": (_I, [_P, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveResult)]),

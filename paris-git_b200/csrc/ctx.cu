@@ -63,45 +63,6 @@ int ctx_alloc_field(paris_ctx* c, int field) {
 }
 
 // ---- ghost fills ----------------------------------------------------------
-// Enumerates the ghost cells of a ghosted field in three disjoint regions
-// (x-slabs over all j,k; y-slabs over interior i, all k; z-slabs over interior
-// i,j).  A ghost cell copies the cell obtained by wrapping its out-of-range
-// periodic coordinates; walls are left untouched.  This equals ghost_x, then
-// ghost_y, then ghost_z of modules.f90:1821-1970 on one rank.
-__device__ inline bool ghost_cell(const Layout L, long t, int& i, int& j, int& k) {
-    const int g = L.ng;
-    const int tx = L.n[0] + 2 * g, ty = L.n[1] + 2 * g, tz = L.n[2] + 2 * g;
-    long rx = 2L * g * ty * tz, ry = (long)L.n[0] * 2 * g * tz, rz = (long)L.n[0] * L.n[1] * 2 * g;
-    if (t < rx) {
-        int a = (int)(t % (2 * g)); long r = t / (2 * g);
-        j = (int)(r % ty) - g; k = (int)(r / ty) - g;
-        i = a < g ? a - g : L.n[0] + (a - g);
-        return true;
-    }
-    t -= rx;
-    if (t < ry) {
-        i = (int)(t % L.n[0]); long r = t / L.n[0];
-        int a = (int)(r % (2 * g)); k = (int)(r / (2 * g)) - g;
-        j = a < g ? a - g : L.n[1] + (a - g);
-        return true;
-    }
-    t -= ry;
-    if (t < rz) {
-        i = (int)(t % L.n[0]); long r = t / L.n[0];
-        j = (int)(r % L.n[1]); int a = (int)(r / L.n[1]);
-        k = a < g ? a - g : L.n[2] + (a - g);
-        return true;
-    }
-    (void)tx;
-    return false;
-}
-
-__host__ __device__ inline long ghost_count(const Layout& L) {
-    const int g = L.ng;
-    long ty = L.n[1] + 2 * g, tz = L.n[2] + 2 * g;
-    return 2L * g * ty * tz + (long)L.n[0] * 2 * g * tz + (long)L.n[0] * L.n[1] * 2 * g;
-}
-
 template <typename T>
 __global__ void k_ghost_fill(T* __restrict__ f, const Layout L, const Bnd B) {
     long t = blockIdx.x * (long)blockDim.x + threadIdx.x;

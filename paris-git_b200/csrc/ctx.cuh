@@ -121,6 +121,9 @@ int ctx_ghost_fill_i8(paris_ctx* c, int8_t* f);
 int ctx_reduce_finish(paris_ctx* c, int nslots, double* out_host, int op_max = 0);
 int ctx_ensure_matrix(paris_ctx* c);
 
+// vof.cu: SetVOFBC on the ghosts of a volume fraction and its flags (dry
+// and wet walls fixed, periodic images, copies elsewhere), no clipping
+__global__ void k_init_ghosts(double* __restrict__ c, int8_t* __restrict__ flag, const Layout L, const Bnd B, long G);
 // poisson.cu
 int poisson_build_full_A(paris_ctx* c);
 // mg_ref.cu

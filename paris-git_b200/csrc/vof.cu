@@ -166,14 +166,13 @@ __global__ void k_vof_update(const SweepArgs a) {
 // x- y- z- x+ y+ z+ in that order, the last one writing a cell wins; 'outflow'
 // copies the boundary cell as it stood after the earlier orientations), then
 // the periodic wrap of do_all_ghost, then get_flags_and_clip.
-__device__ bool ghost_cell_v(const Layout L, long t, int& i, int& j, int& k);
 
 __global__ void k_vof_ghosts(double* __restrict__ c, int8_t* __restrict__ flag, const Layout L, const Bnd B,
                              long G, double epsc) {
     long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (t >= G) return;
     int i, j, k;
-    if (!ghost_cell_v(L, t, i, j, k)) return;
+    if (!ghost_cell(L, t, i, j, k)) return;
     int s[3] = {i, j, k};
     for (int d = 0; d < 3; d++)
         if (B.per[d]) {
@@ -201,40 +200,6 @@ __global__ void k_vof_ghosts(double* __restrict__ c, int8_t* __restrict__ flag, 
     long n = lidx(L, i, j, k);
     c[n] = val;
     flag[n] = fl;
-}
-
-// same enumeration of ghost cells as the generic ghost fill
-__device__ bool ghost_cell_v(const Layout L, long t, int& i, int& j, int& k) {
-    const int g = L.ng;
-    const int ty = L.n[1] + 2 * g, tz = L.n[2] + 2 * g;
-    long rx = 2L * g * ty * tz, ry = (long)L.n[0] * 2 * g * tz, rz = (long)L.n[0] * L.n[1] * 2 * g;
-    if (t < rx) {
-        int a = (int)(t % (2 * g)); long r = t / (2 * g);
-        j = (int)(r % ty) - g; k = (int)(r / ty) - g;
-        i = a < g ? a - g : L.n[0] + (a - g);
-        return true;
-    }
-    t -= rx;
-    if (t < ry) {
-        i = (int)(t % L.n[0]); long r = t / L.n[0];
-        int a = (int)(r % (2 * g)); k = (int)(r / (2 * g)) - g;
-        j = a < g ? a - g : L.n[1] + (a - g);
-        return true;
-    }
-    t -= ry;
-    if (t < rz) {
-        i = (int)(t % L.n[0]); long r = t / L.n[0];
-        j = (int)(r % L.n[1]); int a = (int)(r / L.n[1]);
-        k = a < g ? a - g : L.n[2] + (a - g);
-        return true;
-    }
-    return false;
-}
-
-static long ghost_total(const Layout& L) {
-    const int g = L.ng;
-    long ty = L.n[1] + 2 * g, tz = L.n[2] + 2 * g;
-    return 2L * g * ty * tz + (long)L.n[0] * 2 * g * tz + (long)L.n[0] * L.n[1] * 2 * g;
 }
 
 // c_mask(cvof, cbinary), vofmodules.f90:1295-1305 (whole ghosted array)
@@ -275,7 +240,7 @@ static int sweep(paris_ctx* c, int d, double dt) {
                    dim3(div_up(ext[0], 128), ext[1], ext[2]), 128, 0, a);
     PARIS_LAUNCH_N(c, "vof_mixed_flux", 0L, k_vof_mixed_flux, 148 * 16, 128, 0, a);
     PARIS_LAUNCH_N(c, "vof_sweep", c->N, k_vof_update, dim3(div_up(L.n[0], 128), L.n[1], L.n[2]), 128, 0, a);
-    long G = ghost_total(c->L);
+    long G = ghost_count(c->L);
     PARIS_LAUNCH_N(c, "vof_ghosts", G, k_vof_ghosts, div_up(G, 256), 256, 0, c->c2, c->flag, c->L, c->bnd, G,
                    c->d.epsc);
     double* t = c->fld[PARIS_FIELD_CVOF];
@@ -485,7 +450,7 @@ __global__ void k_init_ghosts(double* __restrict__ c, int8_t* __restrict__ flag,
     long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (t >= G) return;
     int i, j, k;
-    if (!ghost_cell_v(L, t, i, j, k)) return;
+    if (!ghost_cell(L, t, i, j, k)) return;
     int s[3] = {i, j, k};
     for (int d = 0; d < 3; d++)
         if (B.per[d]) {
@@ -530,7 +495,7 @@ extern "C" int paris_init_spheres(paris_handle_t c, int32_t nb, const double* xc
     PARIS_CUDA_TRY(c, cudaMalloc(&f2, c->L.total));
     PARIS_CUDA_TRY(c, cudaMemsetAsync(f2, 0, c->L.total, c->stream));
     dim3 grid(div_up(c->L.n[0], 64), c->L.n[1], c->L.n[2]);
-    long G = ghost_total(c->L);
+    long G = ghost_count(c->L);
     double* cv = c->fld[PARIS_FIELD_CVOF];
     // pass 1 (n1 = 1) into c2/f2, ghosts, then pass 2 into cvof/flag
     PARIS_LAUNCH(c, k_ls2vof, grid, 64, 0, S, c->L, c->xc, c->yc, c->zc, c->dx, c->dy, c->dz, 1, (const int8_t*)nullptr,

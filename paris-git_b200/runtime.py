@@ -10,6 +10,7 @@ that reaches maxit returns it = maxit+1 and warns, as NewSolverMG does
 (MGsolver.f90:402).
 """
 import ctypes
+import os
 import warnings
 
 import numpy as np
@@ -259,6 +260,26 @@ class ParisGpu:
         return out
 
     calcStats = calc_stats
+
+    # -- on-disk formats --------------------------------------------------------
+    def backup_vof_write(self, filename, time, itimestep):
+        """backup_VOF_write: the restart text file from the device fields."""
+        self._check(self.lib.paris_backup_vof_write(self.h, os.fsencode(filename), float(time), int(itimestep)),
+                    "backup_VOF_write")
+
+    def backup_vof_read(self, filename):
+        """backup_VOF_read (+ the restart ghosts): returns (time, itimestep)."""
+        t, it = ctypes.c_double(), ctypes.c_int32()
+        self._check(self.lib.paris_backup_vof_read(self.h, os.fsencode(filename), ctypes.byref(t), ctypes.byref(it)),
+                    "backup_VOF_read")
+        return t.value, it.value
+
+    def output_vof_vtk(self, filename, fmt=capi.VTK_STRUCTURED_GRID, time=0.0, index_range=None, filtered=False):
+        """output_VOF: one VTK file of cvof; index_range = (i1, i2, j1, j2,
+        k1, k2) in Fortran indices or None for is..ie+1 etc."""
+        rng = None if index_range is None else (ctypes.c_int32 * 6)(*[int(v) for v in index_range])
+        self._check(self.lib.paris_output_vof_vtk(self.h, os.fsencode(filename), int(fmt), float(time), rng,
+                                                  1 if filtered else 0), "output_VOF")
 
     def ns_step(self, itimestep, dt, scheme=capi.CONV_QUICK, gravity=(0.0, 0.0, 0.0), buoyancy=0, rho_ave=0.0,
                 dpdx=(0.0, 0.0, 0.0), wall_vel=None, solve=None):

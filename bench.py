@@ -218,10 +218,10 @@ def gpu_step(gpu, capi, k, dt, mode, pcg):
 
 
 # DRAM bytes per cell of the dominant kernel measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum of one 256^3 launch, 415.9 MB
-# over 16,777,216 cells): fills roofline.traffic, scaled by the cells a launch
-# processes
-NCU_DRAM_BYTES_PER_CELL = {"mg_sweep_f32": 415.9e6 / 16777216}
+# (dram__bytes_read.sum + dram__bytes_write.sum of one 256^3 launch,
+# 348.7 MB + 57.0 MB over 16,777,216 cells): fills roofline.traffic, scaled by
+# the cells a launch processes
+NCU_DRAM_BYTES_PER_CELL = {"mg_sweep_f32": (348.717568e6 + 57.026816e6) / 16777216}
 
 
 def roofline(report, peak):

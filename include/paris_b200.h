@@ -115,6 +115,23 @@ int paris_gpu_copy_field(paris_handle_t h, int32_t dst_field, int32_t src_field)
 int paris_gpu_fill_field(paris_handle_t h, int32_t field, double value);
 /* Block until all work queued on the handle's stream has finished. */
 int paris_gpu_sync(paris_handle_t h);
+/* Asynchronous transfers of real(8) fields, for drivers that overlap their
+ * host I/O with the steps.  paris_gpu_upload_async starts copying the host
+ * array (pin it for the copy to run concurrently) into a device staging copy
+ * of the field on a transfer stream and returns; paris_gpu_upload_commit is
+ * the point in the handle's work from which the field holds those values
+ * (the handle's stream waits there for the copy).  Issue the upload early
+ * and the commit late to overlap the copy with the work in between.
+ * paris_gpu_download_async snapshots the field as the handle's work issued
+ * before the call left it and copies it to the host on a second transfer
+ * stream.  Host arrays must stay valid, and a download's must not be read,
+ * until paris_gpu_sync_transfers returns.  No counterpart in the reference
+ * (its arrays live on the host).  Flags, A and heights are transferred with
+ * the synchronous calls only (PARIS_BAD_ARGS here).                        */
+int paris_gpu_upload_async(paris_handle_t h, int32_t field, const void* host);
+int paris_gpu_upload_commit(paris_handle_t h, int32_t field);
+int paris_gpu_download_async(paris_handle_t h, int32_t field, void* host);
+int paris_gpu_sync_transfers(paris_handle_t h);
 /* The cudaStream_t the handle issues all work on (as void*). */
 void* paris_gpu_stream(paris_handle_t h);
 /* Device pointer of a field (interior-only, i fastest; A: 8 components). */

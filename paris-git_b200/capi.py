@@ -149,6 +149,10 @@ _PROTOS = {
     "paris_gpu_upload": (_I, [_P, _I, _P]),
     "paris_gpu_download": (_I, [_P, _I, _P]),
     "paris_gpu_sync": (_I, [_P]),
+    "paris_gpu_upload_async": (_I, [_P, _I, _P]),
+    "paris_gpu_upload_commit": (_I, [_P, _I]),
+    "paris_gpu_download_async": (_I, [_P, _I, _P]),
+    "paris_gpu_sync_transfers": (_I, [_P]),
     "paris_gpu_copy_field": (_I, [_P, _I, _I]),
     "paris_gpu_fill_field": (_I, [_P, _I, _D]),
     "paris_gpu_profile": (_I, [_P, _I]),

@@ -102,10 +102,11 @@ __global__ void k_reduce_slots(const double* __restrict__ part, double* out, int
     if (threadIdx.x == 0) out[slot] = v;
 }
 
+// The reduced scalars are written by the kernel straight into mapped pinned
+// host memory: a small device-to-host copy would queue on the copy engine
+// behind any field download in flight on the transfer stream.
 int ctx_reduce_finish(paris_ctx* c, int nslots, double* out_host, int op_max) {
-    PARIS_LAUNCH(c, k_reduce_slots, nslots, 256, 0, c->red_part, c->red_out, op_max, c->red_nb);
-    PARIS_CUDA_TRY(c, cudaMemcpyAsync(c->red_host, c->red_out, nslots * sizeof(double),
-                                      cudaMemcpyDeviceToHost, c->stream));
+    PARIS_LAUNCH(c, k_reduce_slots, nslots, 256, 0, c->red_part, c->red_host_dev, op_max, c->red_nb);
     PARIS_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     for (int s = 0; s < nslots; s++) out_host[s] = c->red_host[s];
     return PARIS_OK;
@@ -199,8 +200,8 @@ extern "C" int paris_gpu_init(const paris_grid_desc* desc, paris_handle_t* out) 
     if (!s) s = upload_vec(c, &c->yh, c->h_yh);
     if (!s) s = upload_vec(c, &c->zh, c->h_zh);
     if (!s && cudaMalloc(&c->red_part, 8L * kRedBlocks * sizeof(double)) != cudaSuccess) s = PARIS_CUDA_ERROR;
-    if (!s && cudaMalloc(&c->red_out, 8 * sizeof(double)) != cudaSuccess) s = PARIS_CUDA_ERROR;
-    if (!s && cudaMallocHost(&c->red_host, 8 * sizeof(double)) != cudaSuccess) s = PARIS_CUDA_ERROR;
+    if (!s && cudaHostAlloc(&c->red_host, 8 * sizeof(double), cudaHostAllocMapped) != cudaSuccess) s = PARIS_CUDA_ERROR;
+    if (!s && cudaHostGetDevicePointer((void**)&c->red_host_dev, c->red_host, 0) != cudaSuccess) s = PARIS_CUDA_ERROR;
     for (int f : {PARIS_FIELD_CVOF, PARIS_FIELD_U, PARIS_FIELD_V, PARIS_FIELD_W, PARIS_FIELD_RHO, PARIS_FIELD_P})
         if (!s) s = ctx_alloc_field(c, f);
     if (!s) s = ctx_alloc_field(c, PARIS_FIELD_VOF_FLAG);
@@ -227,11 +228,21 @@ extern "C" int paris_gpu_finalize(paris_handle_t c) {
     for (void* p : {(void*)c->dx, (void*)c->dxh, (void*)c->dy, (void*)c->dyh, (void*)c->dz, (void*)c->dzh,
                     (void*)c->xc, (void*)c->yc, (void*)c->zc, (void*)c->xh, (void*)c->yh, (void*)c->zh, (void*)c->c2, (void*)c->flag, (void*)c->cg,
                     (void*)c->height, (void*)c->i32stage, (void*)c->cx, (void*)c->cy, (void*)c->cz,
-                    (void*)c->rhs, (void*)c->A, (void*)c->red_part, (void*)c->red_out, (void*)c->fast_r64,
+                    (void*)c->rhs, (void*)c->A, (void*)c->red_part, (void*)c->fast_r64,
                     (void*)c->fast_d64, (void*)c->fast_q64,
                     (void*)c->vflux, (void*)c->mixlist, (void*)c->mixcount, (void*)c->kflag, (void*)c->st_list,
                     (void*)c->st_count, (void*)c->adj, (void*)c->stats_part, (void*)c->stats_out, (void*)c->mom_tab})
         free_ptr(p);
+    if (c->s_h2d) cudaStreamSynchronize(c->s_h2d);
+    if (c->s_d2h) cudaStreamSynchronize(c->s_d2h);
+    for (int f = 0; f < PARIS_NFIELDS; f++) {
+        free_ptr(c->stage_in[f]);
+        free_ptr(c->stage_out[f]);
+        for (cudaEvent_t e : {c->ev_in_done[f], c->ev_in_free[f], c->ev_out_ready[f], c->ev_out_free[f]})
+            if (e) cudaEventDestroy(e);
+    }
+    if (c->s_h2d) cudaStreamDestroy(c->s_h2d);
+    if (c->s_d2h) cudaStreamDestroy(c->s_d2h);
     for (auto& l : c->ref) { free_ptr(l.K); free_ptr(l.p); free_ptr(l.e); }
     for (auto& l : c->fl32) { free_ptr(l.cx); free_ptr(l.cy); free_ptr(l.cz); free_ptr(l.b); free_ptr(l.x); free_ptr(l.x2); }
     for (auto& l : c->fl64) { free_ptr(l.cx); free_ptr(l.cy); free_ptr(l.cz); free_ptr(l.b); free_ptr(l.x); free_ptr(l.x2); }
@@ -330,13 +341,94 @@ static bool real_field(int f) {
            f != PARIS_FIELD_HEIGHT && f != PARIS_FIELD_VOF_PHASE;
 }
 
+// Device-to-device copy of n doubles on the handle's stream by the SMs, so
+// that the copy engines stay free for the host transfers.
+__global__ void k_copy(double* __restrict__ dst, const double* __restrict__ src, long n) {
+    const long n2 = n >> 1;
+    const double2* s2 = reinterpret_cast<const double2*>(src);
+    double2* d2 = reinterpret_cast<double2*>(dst);
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n2; t += (long)gridDim.x * blockDim.x)
+        d2[t] = s2[t];
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) dst[n - 1] = src[n - 1];
+}
+
+int ctx_copy(paris_ctx* c, double* dst, const double* src, long n) {
+    PARIS_LAUNCH(c, k_copy, (unsigned)(c->nsm * 8), 256, 0, dst, src, n);
+    return PARIS_OK;
+}
+
+// ---- asynchronous transfers --------------------------------------------------
+// An upload fills a device staging copy of the field on the H2D stream; a
+// commit makes the handle's stream wait for that copy at the point of the
+// commit and move it into the field.  A download copies the field into its own
+// staging buffer at the point of issue, and the D2H stream moves that to the
+// host while the handle's stream runs on.  Each staging buffer is refilled
+// only after the transfer before it has finished with it.
+static int async_setup(paris_ctx* c, int f, bool in) {
+    if (!c->s_h2d) {
+        PARIS_CUDA_TRY(c, cudaStreamCreateWithFlags(&c->s_h2d, cudaStreamNonBlocking));
+        PARIS_CUDA_TRY(c, cudaStreamCreateWithFlags(&c->s_d2h, cudaStreamNonBlocking));
+    }
+    double** buf = in ? &c->stage_in[f] : &c->stage_out[f];
+    if (!*buf) {
+        PARIS_CUDA_TRY(c, cudaMalloc(buf, c->L.total * sizeof(double)));
+        cudaEvent_t* e0 = in ? &c->ev_in_done[f] : &c->ev_out_ready[f];
+        cudaEvent_t* e1 = in ? &c->ev_in_free[f] : &c->ev_out_free[f];
+        PARIS_CUDA_TRY(c, cudaEventCreateWithFlags(e0, cudaEventDisableTiming));
+        PARIS_CUDA_TRY(c, cudaEventCreateWithFlags(e1, cudaEventDisableTiming));
+    }
+    return PARIS_OK;
+}
+
+extern "C" int paris_gpu_upload_async(paris_handle_t c, int32_t field, const void* host) {
+    if (!c || !host || !real_field(field)) return PARIS_BAD_ARGS;
+    cudaSetDevice(c->dev);
+    PARIS_CHECK(ctx_alloc_field(c, field));
+    PARIS_CHECK(async_setup(c, field, true));
+    const size_t bytes = (size_t)c->L.total * sizeof(double);
+    PARIS_CUDA_TRY(c, cudaStreamWaitEvent(c->s_h2d, c->ev_in_free[field], 0));
+    PARIS_CUDA_TRY(c, cudaMemcpyAsync(c->stage_in[field], host, bytes, cudaMemcpyHostToDevice, c->s_h2d));
+    PARIS_CUDA_TRY(c, cudaEventRecord(c->ev_in_done[field], c->s_h2d));
+    return PARIS_OK;
+}
+
+extern "C" int paris_gpu_upload_commit(paris_handle_t c, int32_t field) {
+    if (!c || !real_field(field) || !c->stage_in[field]) return PARIS_BAD_ARGS;
+    cudaSetDevice(c->dev);
+    PARIS_CUDA_TRY(c, cudaStreamWaitEvent(c->stream, c->ev_in_done[field], 0));
+    PARIS_CHECK(ctx_copy(c, c->fld[field], c->stage_in[field], c->L.total));
+    PARIS_CUDA_TRY(c, cudaEventRecord(c->ev_in_free[field], c->stream));
+    return PARIS_OK;
+}
+
+extern "C" int paris_gpu_download_async(paris_handle_t c, int32_t field, void* host) {
+    if (!c || !host || !real_field(field)) return PARIS_BAD_ARGS;
+    if (!c->fld[field]) return PARIS_BAD_ARGS;
+    cudaSetDevice(c->dev);
+    PARIS_CHECK(async_setup(c, field, false));
+    const size_t bytes = (size_t)c->L.total * sizeof(double);
+    PARIS_CUDA_TRY(c, cudaStreamWaitEvent(c->stream, c->ev_out_free[field], 0));
+    PARIS_CHECK(ctx_copy(c, c->stage_out[field], c->fld[field], c->L.total));
+    PARIS_CUDA_TRY(c, cudaEventRecord(c->ev_out_ready[field], c->stream));
+    PARIS_CUDA_TRY(c, cudaStreamWaitEvent(c->s_d2h, c->ev_out_ready[field], 0));
+    PARIS_CUDA_TRY(c, cudaMemcpyAsync(host, c->stage_out[field], bytes, cudaMemcpyDeviceToHost, c->s_d2h));
+    PARIS_CUDA_TRY(c, cudaEventRecord(c->ev_out_free[field], c->s_d2h));
+    return PARIS_OK;
+}
+
+extern "C" int paris_gpu_sync_transfers(paris_handle_t c) {
+    if (!c) return PARIS_BAD_ARGS;
+    cudaSetDevice(c->dev);
+    if (c->s_h2d) PARIS_CUDA_TRY(c, cudaStreamSynchronize(c->s_h2d));
+    if (c->s_d2h) PARIS_CUDA_TRY(c, cudaStreamSynchronize(c->s_d2h));
+    return PARIS_OK;
+}
+
 extern "C" int paris_gpu_copy_field(paris_handle_t c, int32_t dst, int32_t src) {
     if (!c || !real_field(dst) || !real_field(src) || !c->fld[src]) return PARIS_BAD_ARGS;
     cudaSetDevice(c->dev);
     PARIS_CHECK(ctx_alloc_field(c, dst));
-    PARIS_CUDA_TRY(c, cudaMemcpyAsync(c->fld[dst], c->fld[src], c->L.total * sizeof(double), cudaMemcpyDeviceToDevice,
-                                      c->stream));
-    return PARIS_OK;
+    return ctx_copy(c, c->fld[dst], c->fld[src], c->L.total);
 }
 
 __global__ void k_fill(double* __restrict__ f, double v, long n) {

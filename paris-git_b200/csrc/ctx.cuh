@@ -63,8 +63,8 @@ struct paris_ctx {
     double setup_dt = 0.0;
     // reductions
     double* red_part = nullptr;    // kRedBlocks partials * 4 slots
-    double* red_out = nullptr;     // device scalars
-    double* red_host = nullptr;    // pinned
+    double* red_host = nullptr;    // pinned and mapped
+    double* red_host_dev = nullptr;   // its device address
     int red_nb = kRedBlocks;       // blocks of the last reduction launch
     int nsm = 148;
     std::vector<std::pair<const void*, int>> red_occ;   // kernel -> resident blocks per SM
@@ -78,6 +78,13 @@ struct paris_ctx {
     double* fast_d64 = nullptr;
     double* fast_q64 = nullptr;
     double* adj = nullptr;         // projection adjoint: 10 ghosted fields + N (allocated on first use)
+    // asynchronous transfers: one stream per direction, a device staging copy
+    // of each transferred field and the events that order them against `stream`
+    cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
+    double* stage_in[PARIS_NFIELDS] = {};
+    double* stage_out[PARIS_NFIELDS] = {};
+    cudaEvent_t ev_in_done[PARIS_NFIELDS] = {}, ev_in_free[PARIS_NFIELDS] = {};
+    cudaEvent_t ev_out_ready[PARIS_NFIELDS] = {}, ev_out_free[PARIS_NFIELDS] = {};
     double* mom_tab = nullptr;     // momentum predictor: per-index QUICK coefficients and metric reciprocals
     int mom_tab_exact = 0;         // their reciprocals of k, 1-k, k-1, dx, dxh are exact (powers of two)
     double* stats_part = nullptr;  // calcStats: PARIS_NSTATS slots of kRedBlocks partials (on first use)
@@ -120,6 +127,7 @@ int ctx_ghost_fill(paris_ctx* c, double* f);         // do_all_ghost (periodic w
 int ctx_ghost_fill_i8(paris_ctx* c, int8_t* f);
 int ctx_reduce_finish(paris_ctx* c, int nslots, double* out_host, int op_max = 0);
 int ctx_ensure_matrix(paris_ctx* c);
+int ctx_copy(paris_ctx* c, double* dst, const double* src, long n);   // device copy by a kernel
 
 // vof.cu: SetVOFBC on the ghosts of a volume fraction and its flags (dry
 // and wet walls fixed, periodic images, copies elsewhere), no clipping

@@ -104,6 +104,25 @@ class ParisGpu:
         assert arr.dtype == np.float64 and arr.shape == self.shape and arr.flags.c_contiguous
         self._check(self.lib.paris_gpu_upload(self.h, field, _ptr(arr)), "upload")
 
+    def upload_async(self, field, arr):
+        """Start copying a real(8) field to the device (arr: contiguous float64,
+        ideally pinned, kept alive and unchanged until sync_transfers); the
+        field takes the values at upload_commit."""
+        assert arr.dtype == np.float64 and arr.shape == self.shape and arr.flags.c_contiguous
+        self._check(self.lib.paris_gpu_upload_async(self.h, field, _ptr(arr)), "upload_async")
+
+    def upload_commit(self, field):
+        self._check(self.lib.paris_gpu_upload_commit(self.h, field), "upload_commit")
+
+    def download_async(self, field, out):
+        """Asynchronous download into out (contiguous float64, ideally pinned);
+        read it only after sync_transfers."""
+        assert out.dtype == np.float64 and out.shape == self.shape and out.flags.c_contiguous
+        self._check(self.lib.paris_gpu_download_async(self.h, field, _ptr(out)), "download_async")
+
+    def sync_transfers(self):
+        self._check(self.lib.paris_gpu_sync_transfers(self.h), "sync_transfers")
+
     def copy_field(self, dst, src):
         self._check(self.lib.paris_gpu_copy_field(self.h, dst, src), "copy_field")
 

@@ -115,7 +115,7 @@ static inline dim3 row_grid(long n0, int n1, int n2) { return dim3(div_up(n0, 12
 // right-hand side of level L0 are loaded, the cycle runs, and the iterate of
 // level L0 is written back.
 template <typename T>
-__global__ void __launch_bounds__(512) k_fast_coarse_cycle(const LVSet<T> G, int L0, int nl, const Bnd B, int nu1,
+__global__ void __launch_bounds__(1024) k_fast_coarse_cycle(const LVSet<T> G, int L0, int nl, const Bnd B, int nu1,
                                                             int nu2, int in_smem) {
     const int tid = threadIdx.x, nt = blockDim.x;
     extern __shared__ __align__(16) unsigned char cc_raw[];
@@ -560,7 +560,7 @@ static int vcycle(paris_ctx* c, int nu1, int nu2, T** x0) {
                                                (int)csm));
         csm_set = csm;
     }
-    PARIS_LAUNCH_N(c, kname<T>("mg_coarse_cycle"), lv[Lc].N, k_fast_coarse_cycle<T>, 1, 512, csm, S, Lc, nl, c->bnd, nu1, nu2,
+    PARIS_LAUNCH_N(c, kname<T>("mg_coarse_cycle"), lv[Lc].N, k_fast_coarse_cycle<T>, 1, 1024, csm, S, Lc, nl, c->bnd, nu1, nu2,
                    in_smem);
     cur[Lc] = lv[Lc].x;
     for (int L = Lc - 1; L >= 0; L--) {

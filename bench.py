@@ -45,8 +45,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="projection", choices=["projection", "rising_bubble"])
-    ap.add_argument("--n", type=int, default=None,
-                    help="cells per direction (projection: 256; rising_bubble: 512 across, twice that in z)")
+    ap.add_argument("--grid", "--n", dest="n", type=int, default=None,
+                    help="cells per direction (projection: 256; rising_bubble: 512 across, twice that in z); "
+                         "under torchrun use --grid, which its own options cannot be confused with")
     ap.add_argument("--pcg", type=int, default=1, help="1: FP64 flexible CG preconditioned by the V-cycle, 0: defect correction")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")

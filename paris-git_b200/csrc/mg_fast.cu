@@ -629,8 +629,13 @@ static int solve_dc(paris_ctx* c, const paris_solve_opts* o, paris_solve_result*
     return done ? PARIS_OK : PARIS_NOT_CONVERGED;
 }
 
+// a PCG vector, zero on allocation: the first direction d = z + 0*d must not
+// read uninitialised memory (0 * NaN is NaN)
 static int alloc_vec(paris_ctx* c, double** p) {
-    if (!*p) PARIS_CUDA_TRY(c, cudaMalloc(p, c->N * sizeof(double)));
+    if (!*p) {
+        PARIS_CUDA_TRY(c, cudaMalloc(p, c->N * sizeof(double)));
+        PARIS_CUDA_TRY(c, cudaMemsetAsync(*p, 0, c->N * sizeof(double), c->stream));
+    }
     return PARIS_OK;
 }
 

@@ -291,6 +291,17 @@ int paris_project_velocity(paris_handle_t h, double dt);
 int paris_calc_residuals_noalloc(int32_t nx, int32_t ny, int32_t nz, int32_t ng, const double* A_dev,
                                  const double* p_dev, double* out3, void* stream);
 
+/* clean_debris, vofmodules.f90:2087-2234 (clean_debris_method, with
+ * clean_debris_neighbours <= Ng): 1 sets the interior cells with no cell of
+ * the other phase (cvof > 0.5) within `neighbours` cells to their pure phase;
+ * 2 sets cells below 0.1 with a neighbourhood sum below 0.3 to 0 and cells
+ * above 0.9 within 0.3 of a full neighbourhood to 1; 3 cleans the mixed cells
+ * with fewer than 6 mixed cells among their 27 to their phase, in sweeps
+ * with the ghosts, flags and clipping refreshed between them (up to 11).
+ * Methods 1 and 2 change cvof only, as the reference does; method 3 cvof and
+ * vof_flag.  sweeps (may be NULL) gets the number of sweeps run.            */
+int paris_clean_debris(paris_handle_t h, int32_t method, int32_t neighbours, int32_t* sweeps);
+
 /* ---- on-disk formats ---------------------------------------------------- */
 /* backup_VOF_write, vofmodules.f90:2033-2059: the restart text file of a VOF
  * run (header FORMAT(es17.8e3,7I10) time, itimestep, imin..kmax, then

@@ -76,6 +76,7 @@ def lib():
             "og_projection_forward_B": (I, [G, D, P, P, P, P, P, P, P, P, P, P, D, I]),
             "og_projection_adjoint": (I, [G, D, P, P, P, P, P, P, P, P, P, P, P, P, P, D, I]),
             "og_time_step_size": (I, [G, P, P, P, D, D, D, P, P]),
+            "og_clean_debris": (I, [G, P, P, I, I, P]),
             "og_get_cfl_and_check": (I, [G, P, P, P, D, D, P]),
             "og_calc_stats": (I, [G, P, P, P, P, P, P, P, P, ctypes.POINTER(capi.StatsOpts), P, P]),
         }
@@ -381,3 +382,12 @@ def calc_stats(desc, u, v, w, rho, p, cvof, mu, flag, opts=None):
                              ctypes.byref(opts) if opts is not None else None, _p(out), _p(ab))
     assert st == 0, st
     return out, ab
+
+
+def clean_debris(desc, cvof, flag, method=1, neighbours=2):
+    """clean_debris on cvof (float64) and flag (int32) in place; returns the sweeps run."""
+    assert cvof.dtype == np.float64 and flag.dtype == np.int32
+    n = ctypes.c_int()
+    st = lib().og_clean_debris(ctypes.byref(desc), _p(cvof), _p(flag), method, neighbours, ctypes.byref(n))
+    assert st == 0, st
+    return n.value

@@ -30,6 +30,7 @@ SOURCES = {
     "momentum.cu": True,
     "stats.cu": True,
     "io.cu": True,
+    "debris.cu": True,
 }
 
 

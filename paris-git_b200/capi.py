@@ -175,6 +175,7 @@ _PROTOS = {
     "paris_time_step_size": (_I, [_P, _D, _D, _D, _P, _P]),
     "paris_get_cfl_and_check": (_I, [_P, _D, _D, _P]),
     "paris_calc_stats": (_I, [_P, ctypes.POINTER(StatsOpts), _P]),
+    "paris_clean_debris": (_I, [_P, _I, _I, _P]),
     "paris_backup_vof_write": (_I, [_P, ctypes.c_char_p, _D, _I]),
     "paris_backup_vof_read": (_I, [_P, ctypes.c_char_p, _P, _P]),
     "paris_output_vof_vtk": (_I, [_P, ctypes.c_char_p, _I, _D, _P, _I]),

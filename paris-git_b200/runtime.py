@@ -280,6 +280,14 @@ class ParisGpu:
 
     calcStats = calc_stats
 
+    def clean_debris(self, method=1, neighbours=2):
+        """clean_debris (clean_debris_method, clean_debris_neighbours);
+        returns the number of sweeps run."""
+        n = ctypes.c_int32()
+        self._check(self.lib.paris_clean_debris(self.h, int(method), int(neighbours), ctypes.byref(n)),
+                    "clean_debris")
+        return n.value
+
     # -- on-disk formats --------------------------------------------------------
     def backup_vof_write(self, filename, time, itimestep):
         """backup_VOF_write: the restart text file from the device fields."""

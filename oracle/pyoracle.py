@@ -323,7 +323,7 @@ def set_velocity_bc(desc, u, v, w, wall_vel=None):
 
 
 def ns_step(desc, st, itimestep, dt, scheme=0, gravity=(0.0, 0.0, 0.0), buoyancy=0, rho_ave=0.0,
-            dpdx=(0.0, 0.0, 0.0), wall_vel=None, max_error=1e-12, maxit=2000, rel_tol=None):
+            dpdx=(0.0, 0.0, 0.0), wall_vel=None, max_error=1e-12, maxit=2000, rel_tol=None, clean_debris=None):
     """The step loop of paris.f90:281-656 (explicit, two-phase VOF, no front
     tracking, no free surface) on the oracle; st: dict of ghosted arrays
     cvof, flag, u, v, w, p, rho, mu (updated in place).  The pressure is
@@ -336,6 +336,8 @@ def ns_step(desc, st, itimestep, dt, scheme=0, gravity=(0.0, 0.0, 0.0), buoyancy
     mu = linfunc(desc, st["cvof"], desc.mu1, desc.mu2, desc.visc_mean)
     momentum_convection(desc, scheme, u, v, w, du, dv, dw)
     vofsweeps(desc, itimestep, dt, st["cvof"], st["flag"], u, v, w)
+    if clean_debris is not None and itimestep % clean_debris[2] == 0:   # paris.f90:310-314
+        globals()["clean_debris"](desc, st["cvof"], st["flag"], clean_debris[0], clean_debris[1])
     H = get_all_heights(desc, st["cvof"], st["flag"])
     rho = linfunc(desc, st["cvof"], desc.rho1, desc.rho2, desc.dens_mean)
     if desc.sigma > 0.0:

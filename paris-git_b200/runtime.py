@@ -309,7 +309,7 @@ class ParisGpu:
                                                   1 if filtered else 0), "output_VOF")
 
     def ns_step(self, itimestep, dt, scheme=capi.CONV_QUICK, gravity=(0.0, 0.0, 0.0), buoyancy=0, rho_ave=0.0,
-                dpdx=(0.0, 0.0, 0.0), wall_vel=None, solve=None):
+                dpdx=(0.0, 0.0, 0.0), wall_vel=None, solve=None, clean_debris=None):
         """One explicit time step in the order of the PARIS step loop
         (paris.f90:281-656: itime_scheme 1, two-phase VOF, no front
         tracking, no free surface): property update, momentum convection,
@@ -317,8 +317,10 @@ class ParisGpu:
         viscous diffusion, volume force, u += dt*du, velocity BCs, then the
         projection (SetupPoisson, NewSolver, project_velocity, velocity BCs)
         and the property update.  `solve`: keyword arguments of new_solver
-        (default: the B200 mixed solver to ||r||/||b|| < 1e-10).  Returns the
-        solver's result."""
+        (default: the B200 mixed solver to ||r||/||b|| < 1e-10).
+        clean_debris: (method, neighbours, nsteps) to run clean_debris after
+        the VOF sweeps of every nsteps-th step (do_clean_debris), or None.
+        Returns the solver's result."""
         solve = dict(solve or {"max_error": 0.0, "rel_tol": 1e-10, "maxit": 200, "mode": capi.MG_MIXED, "pcg": 1})
         for f in (capi.F_DU, capi.F_DV, capi.F_DW):
             self.fill_field(f, 0.0)
@@ -326,6 +328,8 @@ class ParisGpu:
         self.linfunc(capi.F_MU)
         self.momentum_convection(scheme)
         self.vof_sweeps(itimestep, dt)
+        if clean_debris is not None and itimestep % clean_debris[2] == 0:
+            self.clean_debris(clean_debris[0], clean_debris[1])
         self.get_all_heights()
         self.linfunc(capi.F_RHO)
         if self.desc.sigma > 0.0:

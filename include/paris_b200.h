@@ -97,7 +97,9 @@ typedef struct paris_ctx* paris_handle_t;
 #define PARIS_FIELD_USTAR    15   /* caller scratch face fields, e.g. the predicted  */
 #define PARIS_FIELD_VSTAR    16   /* velocity u* kept on the device between steps    */
 #define PARIS_FIELD_WSTAR    17
-#define PARIS_NFIELDS        18
+#define PARIS_FIELD_MOMENTUM 18   /* momentum of the momentum-conserving sweeps (DoMOMCONS), */
+                                  /* zero when first used, kept between calls               */
+#define PARIS_NFIELDS        19
 
 /* ---- life cycle (replaces the allocations of initialize/initialize_VOF,
  *      paris.f90:3016-3031 and init_MG, MGsolver.f90:34-65) --------------- */
@@ -190,6 +192,22 @@ int paris_advance_velocity(paris_handle_t h, double dt);
  * (1 x-, 2 x+, 3 y-, 4 y+, 5 z-, 6 z+) component c at (f-1)+6*(c-1);
  * NULL for resting walls.  Other boundary types return PARIS_BAD_ARGS.    */
 int paris_set_velocity_bc(paris_handle_t h, const double* wall_vel);
+/* vofandmomsweepsstaggered(tswap, t), vofmodules.f90:1536-1692 (DoMOMCONS,
+ * called before vofsweeps, paris.f90:303-305): for each velocity component,
+ * the momentum is formed on a staggered (staggered = 1: get_momentum_staggered,
+ * :1396-1449) or centred (0: get_momentum_centered, :1363-1394) control
+ * volume, advected with a copy of the volume fraction by the three split
+ * CIAM or Weymouth-Yue sweeps in the order of MOD(tswap,3) (swpmom_stg/swp_stg,
+ * vofnonmodule.f90:50-116,239-631,757-1139, or swpmom/swp), and DU/DV/DW are
+ * replaced by (mom/rho - u)/dt where the advected fraction is mixed
+ * (get_velocity_from_momentum_*, vofmodules.f90:1451-1534).  lin_interp:
+ * LinInterp (linear momentum profile across the flux volumes, staggered
+ * only); scheme: PARIS_CONV_* of AdvectionScheme for interpole3.  CVOF and
+ * VOF_FLAG are read, MOMENTUM is kept.  Boundaries: periodic and walls
+ * (SetMomentumBC, modules.f90:1329-1625; wall_vel as for
+ * paris_set_velocity_bc); others return PARIS_BAD_ARGS.                  */
+int paris_vof_mom_sweeps(paris_handle_t h, int32_t tswap, double dt, int32_t staggered, int32_t lin_interp,
+                         int32_t scheme, const double* wall_vel);
 
 /* ---- time-step control and flow statistics ---------------------------- */
 /* TimeStepSize(dt, vof_phase), paris.f90:968-1041, for a run without a free

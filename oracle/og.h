@@ -63,5 +63,17 @@ void og_area_centroid(const double nr[3], double cc, double xc0[3]);
 void og_mycs(const double c[27], double m[3]);
 void og_fd32(const double c[27], double m[3]);
 void og_youngs(const double c[27], double m[3]);
+/* FLUX_CENTROID, vof_functions.f90:619-752 */
+void og_flux_centroid(const double nr[3], double alpha, const double x0[3], const double dx[3], double xc0[3]);
+
+/* og_vof.c pieces shared with the momentum-conserving sweeps */
+void og_setvofbc(const og_grid* g, double* cv, int32_t* fl);          /* SetVOFBC */
+void og_flags_and_clip(const og_grid* g, double* c, int32_t* f);      /* get_flags_and_clip */
+void og_stencil(const og_grid* g, const double* c, long n, double st[27]);
+int og_fit_plane_new(double vof, int d, double a1, double a2, const double st[27], double m[3], double* alpha);
+/* swp (vofnonmodule.f90:27-48) along d (0..2) with face velocity us; w2 is
+ * the c_mask of the Weymouth-Yue sweep; phase may be NULL */
+void og_swp(const og_grid* g, const double* us, double* c, int32_t* f, int d, double dt, double* w1, double* w2,
+            double* w3, int32_t* phase);
 
 #endif

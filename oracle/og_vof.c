@@ -8,7 +8,7 @@
 #include "og.h"
 
 /* SetVOFBC, vofmodules.f90:1694-1825 ('dry' 0, 'wet' 1, 'periodic', 'outflow') */
-static void og_setvofbc(const og_grid* g, double* cv, int32_t* fl) {
+void og_setvofbc(const og_grid* g, double* cv, int32_t* fl) {
     for (int orient = 0; orient < 6; orient++) {
         int cond = g->d.vofbdry_cond[orient];
         int d = orient % 3;
@@ -38,7 +38,7 @@ static void og_setvofbc(const og_grid* g, double* cv, int32_t* fl) {
 }
 
 /* get_flags_and_clip, vofmodules.f90:549-571 (all cells, ghosts included) */
-static void og_flags_and_clip(const og_grid* g, double* c, int32_t* f) {
+void og_flags_and_clip(const og_grid* g, double* c, int32_t* f) {
     double epsc = g->d.epsc;
     for (long n = 0; n < g->ntot; n++) {
         if (c[n] <= epsc) {
@@ -57,7 +57,7 @@ void og_vof_phase(const og_grid* g, const double* c, int32_t* phase) {
     for (long n = 0; n < g->ntot; n++) phase[n] = c[n] < (0.5 - epsc) ? 0 : 1;
 }
 
-static void og_stencil(const og_grid* g, const double* c, long n, double st[27]) {
+void og_stencil(const og_grid* g, const double* c, long n, double st[27]) {
     for (int i1 = -1; i1 <= 1; i1++)
         for (int j1 = -1; j1 <= 1; j1++)
             for (int k1 = -1; k1 <= 1; k1++)
@@ -65,7 +65,7 @@ static void og_stencil(const og_grid* g, const double* c, long n, double st[27])
 }
 
 /* fit_plane_new, vofnonmodule.f90:633-655; returns 1 on error (zero normal) */
-static int og_fit_plane_new(double vof, int d, double a1, double a2, const double st[27],
+int og_fit_plane_new(double vof, int d, double a1, double a2, const double st[27],
                             double m[3], double* alpha) {
     og_mycs(st, m);
     if (m[0] == 0.0 && m[1] == 0.0 && m[2] == 0.0) return 1;
@@ -183,7 +183,7 @@ static void og_swpr(const og_grid* g, const double* us, double* c, int32_t* f, i
 }
 
 /* swp, vofnonmodule.f90:27-48 */
-static void og_swp(const og_grid* g, const double* us, double* c, int32_t* f, int d, double dt,
+void og_swp(const og_grid* g, const double* us, double* c, int32_t* f, int d, double dt,
                    double* w1, double* w2, double* w3, int32_t* phase) {
     if (g->d.vof_advect == PARIS_ADVECT_WY)
         og_swpr(g, us, c, f, d, dt, w1, w2, w3);

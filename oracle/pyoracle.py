@@ -77,6 +77,8 @@ def lib():
             "og_projection_adjoint": (I, [G, D, P, P, P, P, P, P, P, P, P, P, P, P, P, D, I]),
             "og_time_step_size": (I, [G, P, P, P, D, D, D, P, P]),
             "og_clean_debris": (I, [G, P, P, I, I, P]),
+            "og_vof_mom_sweeps": (I, [G, I, D, I, I, I, P, P, P, P, P, P, P, P, P, P]),
+            "og_flux_centroid": (None, [P, D, P, P, P]),
             "og_get_cfl_and_check": (I, [G, P, P, P, D, D, P]),
             "og_calc_stats": (I, [G, P, P, P, P, P, P, P, P, ctypes.POINTER(capi.StatsOpts), P, P]),
         }
@@ -322,19 +324,50 @@ def set_velocity_bc(desc, u, v, w, wall_vel=None):
     return lib().og_set_velocity_bc(ctypes.byref(desc), _p(u), _p(v), _p(w), _p(wv))
 
 
+def vof_mom_sweeps(desc, tswap, dt, cvof, flag, u, v, w, du, dv, dw, mom, staggered=True, lin_interp=False,
+                   scheme=0, wall_vel=None):
+    """vofandmomsweepsstaggered (DoMOMCONS): advects the momentum of each
+    component with the split VOF fluxes and overwrites du, dv, dw where the
+    advected (staggered) fraction is mixed; mom is the persistent momentum
+    array (in/out).  cvof and flag are read only."""
+    wv = None if wall_vel is None else np.ascontiguousarray(np.asarray(wall_vel, dtype=np.float64).reshape(6, 3).T)
+    f32 = np.ascontiguousarray(flag, dtype=np.int32)
+    st = lib().og_vof_mom_sweeps(ctypes.byref(desc), tswap, dt, 1 if staggered else 0, 1 if lin_interp else 0, scheme,
+                                 _p(wv), _p(cvof), _p(f32), _p(u), _p(v), _p(w), _p(du), _p(dv), _p(dw), _p(mom))
+    assert st == 0, st
+
+
+def flux_centroid(nr, alpha, x0, dx):
+    out = np.zeros(3)
+    lib().og_flux_centroid(_p(np.ascontiguousarray(nr, dtype=np.float64)), alpha,
+                           _p(np.ascontiguousarray(x0, dtype=np.float64)),
+                           _p(np.ascontiguousarray(dx, dtype=np.float64)), _p(out))
+    return out
+
+
 def ns_step(desc, st, itimestep, dt, scheme=0, gravity=(0.0, 0.0, 0.0), buoyancy=0, rho_ave=0.0,
-            dpdx=(0.0, 0.0, 0.0), wall_vel=None, max_error=1e-12, maxit=2000, rel_tol=None, clean_debris=None):
+            dpdx=(0.0, 0.0, 0.0), wall_vel=None, max_error=1e-12, maxit=2000, rel_tol=None, clean_debris=None,
+            momcons=None):
     """The step loop of paris.f90:281-656 (explicit, two-phase VOF, no front
     tracking, no free surface) on the oracle; st: dict of ghosted arrays
     cvof, flag, u, v, w, p, rho, mu (updated in place).  The pressure is
     solved by the reference multigrid to the absolute RMS residual
     max_error, or, with rel_tol, to rel_tol times the RMS of the right-hand
-    side (||r||_2/||b||_2 < rel_tol).  Returns the solver's cycle count."""
+    side (||r||_2/||b||_2 < rel_tol).  momcons: None, or the keyword
+    arguments staggered / lin_interp of vof_mom_sweeps to run the
+    momentum-conserving sweeps before vofsweeps (DoMOMCONS, paris.f90:303-305);
+    st["mom"] then holds the persistent momentum array.  Returns the
+    solver's cycle count."""
     u, v, w = st["u"], st["v"], st["w"]
     du, dv, dw = (zeros(desc) for _ in range(3))
     rho = linfunc(desc, st["cvof"], desc.rho1, desc.rho2, desc.dens_mean)
     mu = linfunc(desc, st["cvof"], desc.mu1, desc.mu2, desc.visc_mean)
     momentum_convection(desc, scheme, u, v, w, du, dv, dw)
+    if momcons is not None:
+        if "mom" not in st:
+            st["mom"] = zeros(desc)
+        vof_mom_sweeps(desc, itimestep, dt, st["cvof"], st["flag"], u, v, w, du, dv, dw, st["mom"], scheme=scheme,
+                       wall_vel=wall_vel, **momcons)
     vofsweeps(desc, itimestep, dt, st["cvof"], st["flag"], u, v, w)
     if clean_debris is not None and itimestep % clean_debris[2] == 0:   # paris.f90:310-314
         globals()["clean_debris"](desc, st["cvof"], st["flag"], clean_debris[0], clean_debris[1])

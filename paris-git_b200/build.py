@@ -31,6 +31,7 @@ SOURCES = {
     "stats.cu": True,
     "io.cu": True,
     "debris.cu": True,
+    "momcons.cu": True,
 }
 
 

@@ -23,7 +23,7 @@ MEAN_ARITH, MEAN_HARM = 101, 102
 
 # fields
 (F_CVOF, F_U, F_V, F_W, F_RHO, F_P, F_DU, F_DV, F_DW, F_KAPPA, F_MU, F_VOF_FLAG,
- F_A, F_HEIGHT, F_VOF_PHASE, F_USTAR, F_VSTAR, F_WSTAR) = range(18)
+ F_A, F_HEIGHT, F_VOF_PHASE, F_USTAR, F_VSTAR, F_WSTAR, F_MOMENTUM) = range(19)
 
 # solver modes
 MG_REFERENCE, MG_FP64, MG_MIXED = 0, 1, 2
@@ -176,6 +176,7 @@ _PROTOS = {
     "paris_get_cfl_and_check": (_I, [_P, _D, _D, _P]),
     "paris_calc_stats": (_I, [_P, ctypes.POINTER(StatsOpts), _P]),
     "paris_clean_debris": (_I, [_P, _I, _I, _P]),
+    "paris_vof_mom_sweeps": (_I, [_P, _I, _D, _I, _I, _I, _P]),
     "paris_backup_vof_write": (_I, [_P, ctypes.c_char_p, _D, _I]),
     "paris_backup_vof_read": (_I, [_P, ctypes.c_char_p, _P, _P]),
     "paris_output_vof_vtk": (_I, [_P, ctypes.c_char_p, _I, _D, _P, _I]),

@@ -231,7 +231,9 @@ extern "C" int paris_gpu_finalize(paris_handle_t c) {
                     (void*)c->rhs, (void*)c->A, (void*)c->red_part, (void*)c->fast_r64,
                     (void*)c->fast_d64, (void*)c->fast_q64,
                     (void*)c->vflux, (void*)c->mixlist, (void*)c->mixcount, (void*)c->kflag, (void*)c->st_list,
-                    (void*)c->st_count, (void*)c->adj, (void*)c->stats_part, (void*)c->stats_out, (void*)c->mom_tab})
+                    (void*)c->st_count, (void*)c->adj, (void*)c->stats_part, (void*)c->stats_out, (void*)c->mom_tab,
+                    (void*)c->mc_tmp, (void*)c->mc_tmp2, (void*)c->mc_work, (void*)c->mc_fv, (void*)c->mc_flag,
+                    (void*)c->mc_cg})
         free_ptr(p);
     if (c->s_h2d) cudaStreamSynchronize(c->s_h2d);
     if (c->s_d2h) cudaStreamSynchronize(c->s_d2h);

@@ -87,6 +87,12 @@ struct paris_ctx {
     cudaEvent_t ev_out_ready[PARIS_NFIELDS] = {}, ev_out_free[PARIS_NFIELDS] = {};
     double* mom_tab = nullptr;     // momentum predictor: per-index QUICK coefficients and metric reciprocals
     int mom_tab_exact = 0;         // their reciprocals of k, 1-k, k-1, dx, dxh are exact (powers of two)
+    double* mc_tmp = nullptr;      // momentum-conserving sweeps: advected fraction (two buffers),
+    double* mc_tmp2 = nullptr;
+    double* mc_work = nullptr;     // 3 ghosted work arrays (half fractions, momentum fluxes),
+    double* mc_fv = nullptr;       // face velocity of a sweep, and flags / c_mask of the fraction
+    int8_t* mc_flag = nullptr;
+    uint8_t* mc_cg = nullptr;
     double* stats_part = nullptr;  // calcStats: PARIS_NSTATS slots of kRedBlocks partials (on first use)
     double* stats_out = nullptr;
     int64_t launches = 0;
@@ -132,6 +138,13 @@ int ctx_copy(paris_ctx* c, double* dst, const double* src, long n);   // device 
 // vof.cu: SetVOFBC on the ghosts of a volume fraction and its flags (dry
 // and wet walls fixed, periodic images, copies elsewhere), no clipping
 __global__ void k_init_ghosts(double* __restrict__ c, int8_t* __restrict__ flag, const Layout L, const Bnd B, long G);
+// vof.cu: one split sweep (swpz or swpr, then SetVOFBC, get_flags_and_clip
+// and the ghosts) along d of the volume fraction src into dst with its flags;
+// us: the face velocity of the sweep, cg: c_mask for the Weymouth-Yue sweep
+int vof_sweep_dir(paris_ctx* c, int d, double dt, const double* src, double* dst, int8_t* flag, const double* us,
+                  const uint8_t* cg);
+// vof.cu: c_mask (vofmodules.f90:1295-1305) over total cells
+__global__ void k_c_mask(const double* __restrict__ c, uint8_t* __restrict__ cg, long total);
 // poisson.cu
 int poisson_build_full_A(paris_ctx* c);
 // mg_ref.cu

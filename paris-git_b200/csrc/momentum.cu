@@ -14,6 +14,7 @@
 #include <cmath>
 
 #include "ctx.cuh"
+#include "limiter.cuh"
 
 namespace {
 
@@ -193,26 +194,6 @@ __global__ void __launch_bounds__(256) k_conv_quick_uniform(Vel V, double* __res
             - (0.5 * ((v[n] + v[n + sz]) * w2 - (v[n - sy] + v[n - sy + sz]) * w2m)) * Q.rd[1]
             - (a * a - b * b) * Q.rdh[2];
     }
-}
-
-// minabs / maxabs (paris.f90:3450-3475) and slope_lim (modules.f90:177-197)
-__device__ inline double minabs(double a, double b) { return fabs(a) < fabs(b) ? a : b; }
-__device__ inline double maxabs(double a, double b) { return fabs(a) > fabs(b) ? a : b; }
-__device__ inline double slope_lim(double v1, double v2, double v3, int scheme) {
-    if (scheme == PARIS_CONV_SUPERBEE) {
-        double a1 = minabs(v3 - v2, 2.0 * (v2 - v1));
-        double a2 = minabs(2.0 * (v3 - v2), v2 - v1);
-        return maxabs(a1, a2);
-    } else if (scheme == PARIS_CONV_ENO) {
-        return minabs(v3 - v2, v2 - v1);
-    } else if (scheme == PARIS_CONV_WENO) {
-        double d1 = v2 - v1, d2 = v3 - v2;
-        double a1 = 1.0 / (d1 * d1 + 1.e-16);
-        double a2 = 1.0 / (d2 * d2 + 1.e-16);
-        double a = a1 + a2;
-        return (a1 * (v2 - v1) + a2 * (v3 - v2)) / a;
-    }
-    return 0.0;
 }
 
 // work(p, a) of momentumConvection_onedim for the component phi of

@@ -303,4 +303,91 @@ __device__ inline void mycs(const double c[27], double mxyz[3]) {
 }
 #undef PC
 
+// FLUX_CENTROID, vof_functions.f90:619-752: the centroid of the part of the
+// box [x0, x0 + dx] below the plane nr.x = alpha.  The box goes onto the unit
+// cube with positive, sorted coefficients; the centroid below the plane (or
+// that of the complement when more than half the box is filled) follows from
+// the plane's position in five cases, and is mapped back.
+__device__ inline void flux_centroid(const double nr[3], double alpha, const double x0[3], const double dx[3],
+                                     double xc0[3]) {
+    double al = alpha - nr[0] * x0[0] - nr[1] * x0[1] - nr[2] * x0[2];
+    al = al + dmax1(0.0, -nr[0] * dx[0]) + dmax1(0.0, -nr[1] * dx[1]) + dmax1(0.0, -nr[2] * dx[2]);
+    double np1 = fabs(nr[0]), np2 = fabs(nr[1]), np3 = fabs(nr[2]);
+    const double almax = np1 * dx[0] + np2 * dx[1] + np3 * dx[2];
+    al = dmax1(0.0, dmin1(1.0, al / almax));
+    const double alh = dmin1(al, 1.0 - al);
+    const double alr = dmax1(alh, kEps0);
+    np1 = np1 * dx[0] / almax;
+    np2 = np2 * dx[1] / almax;
+    np3 = np3 * dx[2] / almax;
+    double m1, m2, m3, ctd0[3], frac;
+    int ind[3];
+    if (np1 <= np2) { m1 = np1; m3 = np2; ind[0] = 0; ind[2] = 1; }
+    else { m1 = np2; m3 = np1; ind[0] = 1; ind[2] = 0; }
+    if (np3 < m1) { m2 = m1; m1 = np3; ind[1] = ind[0]; ind[0] = 2; }
+    else if (np3 >= m3) { m2 = m3; m3 = np3; ind[1] = ind[2]; ind[2] = 2; }
+    else { m2 = np3; ind[1] = 2; }
+    const double m12 = m1 + m2;
+    const double mm = dmin1(m12, m3);
+    const double denom = dmax1(6.0 * m1 * m2 * m3, kEps0);
+    if (alr <= m1) {
+        const double q = 0.25 * alh;
+        ctd0[0] = q / m1;
+        ctd0[1] = q / m2;
+        ctd0[2] = q / m3;
+        frac = alh * alh * alh / denom;
+    } else if (alr <= m2) {
+        const double t1 = (2.0 * alh - m1);
+        double t2 = (2.0 * alh * alh - 2.0 * alh * m1 + m1 * m1);
+        const double b = 4.0 * (3.0 * alr * alr - 3.0 * alh * m1 + m1 * m1);
+        t2 = t1 * t2 / b;
+        ctd0[0] = 0.5 - m1 * t1 / b;
+        ctd0[1] = t2 / m2;
+        ctd0[2] = t2 / m3;
+        frac = 0.5 * alh * (alh - m1) / (m2 * m3) + m1 * m1 * m1 / denom;
+    } else if (alr <= mm) {
+        const double a2 = alh * alh;
+        const double t1 = (alh - m1) * (alh - m1) * (alh - m1);
+        const double t2 = (alh - m2) * (alh - m2) * (alh - m2);
+        const double b = 4.0 * (a2 * alh - t1 - t2);
+        ctd0[0] = (a2 * a2 - t1 * (alh + 3.0 * m1) - t2 * (alh - m2)) / (m1 * b);
+        ctd0[1] = (a2 * a2 - t1 * (alh - m1) - t2 * (alh + 3.0 * m2)) / (m2 * b);
+        ctd0[2] = (a2 * a2 - t1 * (alh - m1) - t2 * (alh - m2)) / (m3 * b);
+        const double t3 = alh * alh * (3.0 * m12 - alh) + m1 * m1 * (m1 - 3.0 * alh);
+        frac = (t3 + m2 * m2 * (m2 - 3.0 * alh)) / denom;
+    } else if (m12 <= m3) {
+        const double b = dmax1((2.0 * alh - m12), kEps0);
+        ctd0[0] = 0.5 - m1 / (6.0 * b);
+        ctd0[1] = 0.5 - m2 / (6.0 * b);
+        ctd0[2] = ((3.0 * alh - 2.0 * m12) * b + alh * m12 - m1 * m2) / (6.0 * m3 * b);
+        frac = (alh - 0.5 * m12) / m3;
+    } else {
+        const double s1 = m1 + m2 + m3;
+        const double s2 = m1 * m1 + m2 * m2 + m3 * m3;
+        const double s3 = m1 * m1 * m1 + m2 * m2 * m2 + m3 * m3 * m3;
+        const double s4 = m1 * m1 * m1 * m1 + m2 * m2 * m2 * m2 + m3 * m3 * m3 * m3;
+        const double a2 = alh * alh;
+        const double b = 4.0 * (2.0 * a2 * alh - 3.0 * a2 * s1 + 3.0 * alh * s2 - s3);
+        const double t = 2.0 * a2 * a2 - 4.0 * a2 * alh * s1 + 6.0 * a2 * s2 - 4.0 * alh * s3 + s4;
+        ctd0[0] = (t + 4.0 * m1 * (alh - m1) * (alh - m1) * (alh - m1)) / (m1 * b);
+        ctd0[1] = (t + 4.0 * m2 * (alh - m2) * (alh - m2) * (alh - m2)) / (m2 * b);
+        ctd0[2] = (t + 4.0 * m3 * (alh - m3) * (alh - m3) * (alh - m3)) / (m3 * b);
+        const double u1 = alh * alh * (3.0 - 2.0 * alh) + m1 * m1 * (m1 - 3.0 * alh);
+        frac = (u1 + m2 * m2 * (m2 - 3.0 * alh) + m3 * m3 * (m3 - 3.0 * alh)) / denom;
+    }
+    if (al > 0.5) {
+        ctd0[0] = (0.5 - frac * (1.0 - ctd0[0])) / (1.0 - frac);
+        ctd0[1] = (0.5 - frac * (1.0 - ctd0[1])) / (1.0 - frac);
+        ctd0[2] = (0.5 - frac * (1.0 - ctd0[2])) / (1.0 - frac);
+    }
+    double r[3];
+    r[ind[0]] = ctd0[0];
+    r[ind[1]] = ctd0[1];
+    r[ind[2]] = ctd0[2];
+    for (int a = 0; a < 3; a++) {
+        if (nr[a] < 0.0) r[a] = 1.0 - r[a];
+        xc0[a] = x0[a] + r[a] * dx[a];
+    }
+}
+
 }  // namespace plic

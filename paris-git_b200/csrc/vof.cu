@@ -208,7 +208,8 @@ __global__ void k_c_mask(const double* __restrict__ c, uint8_t* __restrict__ cg,
     if (t < total) cg[t] = c[t] > 0.5 ? 1 : 0;
 }
 
-static int sweep(paris_ctx* c, int d, double dt) {
+int vof_sweep_dir(paris_ctx* c, int d, double dt, const double* src, double* dst, int8_t* flag, const double* us,
+                  const uint8_t* cg) {
     const Layout& L = c->L;
     if (!c->vflux) {
         PARIS_CUDA_TRY(c, cudaMalloc(&c->vflux, 3 * L.total * sizeof(double)));
@@ -216,11 +217,11 @@ static int sweep(paris_ctx* c, int d, double dt) {
         PARIS_CUDA_TRY(c, cudaMalloc(&c->mixcount, sizeof(int)));
     }
     SweepArgs a;
-    a.c = c->fld[PARIS_FIELD_CVOF];
-    a.cn = c->c2;
-    a.flag = c->flag;
-    a.us = c->fld[PARIS_FIELD_U + d];
-    a.cg = c->cg;
+    a.c = src;
+    a.cn = dst;
+    a.flag = flag;
+    a.us = us;
+    a.cg = cg;
     a.v1 = c->vflux;
     a.v2 = c->vflux + L.total;
     a.v3 = c->vflux + 2 * L.total;
@@ -241,8 +242,13 @@ static int sweep(paris_ctx* c, int d, double dt) {
     PARIS_LAUNCH_N(c, "vof_mixed_flux", 0L, k_vof_mixed_flux, 148 * 16, 128, 0, a);
     PARIS_LAUNCH_N(c, "vof_sweep", c->N, k_vof_update, dim3(div_up(L.n[0], 128), L.n[1], L.n[2]), 128, 0, a);
     long G = ghost_count(c->L);
-    PARIS_LAUNCH_N(c, "vof_ghosts", G, k_vof_ghosts, div_up(G, 256), 256, 0, c->c2, c->flag, c->L, c->bnd, G,
+    PARIS_LAUNCH_N(c, "vof_ghosts", G, k_vof_ghosts, div_up(G, 256), 256, 0, dst, flag, c->L, c->bnd, G,
                    c->d.epsc);
+    return PARIS_OK;
+}
+
+static int sweep(paris_ctx* c, int d, double dt) {
+    PARIS_CHECK(vof_sweep_dir(c, d, dt, c->fld[PARIS_FIELD_CVOF], c->c2, c->flag, c->fld[PARIS_FIELD_U + d], c->cg));
     double* t = c->fld[PARIS_FIELD_CVOF];
     c->fld[PARIS_FIELD_CVOF] = c->c2;
     c->c2 = t;

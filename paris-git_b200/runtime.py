@@ -254,6 +254,17 @@ class ParisGpu:
             wv = np.ascontiguousarray(np.asarray(wall_vel, dtype=np.float64).reshape(6, 3).T)   # Fortran order
             self._check(self.lib.paris_set_velocity_bc(self.h, _ptr(wv)), "SetVelocityBC")
 
+    def vof_mom_sweeps(self, tswap, dt, staggered=True, lin_interp=False, scheme=capi.CONV_QUICK, wall_vel=None):
+        """vofandmomsweepsstaggered (DoMOMCONS): the momentum of each component
+        advected with the split VOF fluxes of its control volume; DU/DV/DW
+        replaced where the advected fraction is mixed.  The MOMENTUM field
+        is kept between calls."""
+        wv = None if wall_vel is None else np.ascontiguousarray(
+            np.asarray(wall_vel, dtype=np.float64).reshape(6, 3).T)
+        self._check(self.lib.paris_vof_mom_sweeps(self.h, int(tswap), float(dt), 1 if staggered else 0,
+                                                  1 if lin_interp else 0, int(scheme), _ptr(wv) if wv is not None
+                                                  else None), "vofandmomsweepsstaggered")
+
     # -- time-step control and statistics ------------------------------------
     def time_step_size(self, cfl, max_dt, u_inject=0.0):
         """TimeStepSize (no free surface): returns (dt, vmax)."""
@@ -309,7 +320,7 @@ class ParisGpu:
                                                   1 if filtered else 0), "output_VOF")
 
     def ns_step(self, itimestep, dt, scheme=capi.CONV_QUICK, gravity=(0.0, 0.0, 0.0), buoyancy=0, rho_ave=0.0,
-                dpdx=(0.0, 0.0, 0.0), wall_vel=None, solve=None, clean_debris=None):
+                dpdx=(0.0, 0.0, 0.0), wall_vel=None, solve=None, clean_debris=None, momcons=None):
         """One explicit time step in the order of the PARIS step loop
         (paris.f90:281-656: itime_scheme 1, two-phase VOF, no front
         tracking, no free surface): property update, momentum convection,
@@ -320,6 +331,8 @@ class ParisGpu:
         (default: the B200 mixed solver to ||r||/||b|| < 1e-10).
         clean_debris: (method, neighbours, nsteps) to run clean_debris after
         the VOF sweeps of every nsteps-th step (do_clean_debris), or None.
+        momcons: None, or the keyword arguments staggered / lin_interp of
+        vof_mom_sweeps, run before the VOF sweeps (DoMOMCONS).
         Returns the solver's result."""
         solve = dict(solve or {"max_error": 0.0, "rel_tol": 1e-10, "maxit": 200, "mode": capi.MG_MIXED, "pcg": 1})
         for f in (capi.F_DU, capi.F_DV, capi.F_DW):
@@ -327,6 +340,8 @@ class ParisGpu:
         self.linfunc(capi.F_RHO)
         self.linfunc(capi.F_MU)
         self.momentum_convection(scheme)
+        if momcons is not None:
+            self.vof_mom_sweeps(itimestep, dt, scheme=scheme, wall_vel=wall_vel, **momcons)
         self.vof_sweeps(itimestep, dt)
         if clean_debris is not None and itimestep % clean_debris[2] == 0:
             self.clean_debris(clean_debris[0], clean_debris[1])

@@ -10,6 +10,8 @@
 // defect correction p += V(b - A p), or CG preconditioned by the V-cycle.
 // Levels at or below kCoarseCells cells run in one single-block kernel.
 #include <string.h>
+#include <type_traits>
+
 #include "ctx.cuh"
 
 static constexpr long kCoarseCells = 4096;   // 16^3
@@ -97,6 +99,70 @@ template <typename T>
 __global__ void k_fast_restrict(const LV<T> f, const LV<T> c, const Bnd B) {
     int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
     if (i < c.n0) restrict_cell(f, c, B, i, j, k);
+}
+
+// Residual and restriction with one warp per 32 coarse cells of a fine row:
+// threadIdx.y = dj + 2 dk picks the fine row of the 2x2x2 block, and each
+// lane computes the residuals of its fine pair (2i, 2i+1) from pair loads
+// (x, the east/north/top coefficients, b, and the rows and planes around),
+// the west neighbours of the pair by a shuffle from the lane to its left
+// (scalar loads at the tile edge).  The four rows of a coarse cell are summed
+// in shared memory.  Needs an even fine n0 (every level above the coarsest).
+template <typename T>
+__global__ void __launch_bounds__(128) k_fast_restrict2(const LV<T> f, const LV<T> c, const Bnd B) {
+    using V2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+    __shared__ T part[4][32];
+    const int lane = threadIdx.x, ty = threadIdx.y;
+    const int ci = blockIdx.x * 32 + lane, cj = blockIdx.y, ck = blockIdx.z;
+    const int n0 = f.n0, n1 = f.n1, n2 = f.n2;
+    const long sy = n0, sz = (long)n0 * n1;
+    const int i0 = 2 * ci, j = 2 * cj + (ty & 1), k = 2 * ck + (ty >> 1);
+    const bool ok = ci < c.n0;
+    const long m = i0 + sy * j + sz * k;
+    auto ld2 = [&](const T* a, long q) { return *reinterpret_cast<const V2*>(a + q); };
+    const V2 zero2 = {(T)0, (T)0};
+    V2 X = zero2, CX = zero2, CY = zero2, CZ = zero2, BB = zero2, XS = zero2, XN = zero2, XB = zero2, XT = zero2,
+       CYS = zero2, CZB = zero2;
+    if (ok) {
+        X = ld2(f.x, m);
+        CX = ld2(f.cx, m);
+        CY = ld2(f.cy, m);
+        CZ = ld2(f.cz, m);
+        BB = ld2(f.b, m);
+        if (j > 0) { XS = ld2(f.x, m - sy); CYS = ld2(f.cy, m - sy); }
+        else if (B.per[1]) { XS = ld2(f.x, m + sy * (n1 - 1)); CYS = ld2(f.cy, m + sy * (n1 - 1)); }
+        if (j < n1 - 1) XN = ld2(f.x, m + sy);
+        else if (B.per[1]) XN = ld2(f.x, m - sy * (n1 - 1));
+        if (k > 0) { XB = ld2(f.x, m - sz); CZB = ld2(f.cz, m - sz); }
+        else if (B.per[2]) { XB = ld2(f.x, m + sz * (n2 - 1)); CZB = ld2(f.cz, m + sz * (n2 - 1)); }
+        if (k < n2 - 1) XT = ld2(f.x, m + sz);
+        else if (B.per[2]) XT = ld2(f.x, m - sz * (n2 - 1));
+    }
+    // west of the pair: x and cx of fine cell i0-1; east: x of fine cell i0+2
+    T xw = __shfl_up_sync(0xffffffffu, X.y, 1), a1w = __shfl_up_sync(0xffffffffu, CX.y, 1);
+    T xe = __shfl_down_sync(0xffffffffu, X.x, 1);
+    if (ok && (lane == 0 || i0 == 0)) {
+        if (i0 > 0) { xw = f.x[m - 1]; a1w = f.cx[m - 1]; }
+        else if (B.per[0]) { xw = f.x[m + n0 - 1]; a1w = f.cx[m + n0 - 1]; }
+        else { xw = (T)0; a1w = (T)0; }
+    }
+    if (ok && (lane == 31 || ci == c.n0 - 1)) {
+        if (i0 + 2 < n0) xe = f.x[m + 2];
+        else xe = B.per[0] ? f.x[m + 2 - n0] : (T)0;
+    }
+    T s = (T)0;
+    if (ok) {
+        // the fine cell i0, then i0+1 (the arithmetic of resid_cell)
+        T d = a1w + CX.x + CYS.x + CY.x + CZB.x + CZ.x;
+        const T rA = BB.x - d * X.x + a1w * xw + CX.x * X.y + CYS.x * XS.x + CY.x * XN.x + CZB.x * XB.x + CZ.x * XT.x;
+        d = CX.x + CX.y + CYS.y + CY.y + CZB.y + CZ.y;
+        const T rB = BB.y - d * X.y + CX.x * X.x + CX.y * xe + CYS.y * XS.y + CY.y * XN.y + CZB.y * XB.y + CZ.y * XT.y;
+        s = rA + rB;
+    }
+    part[ty][lane] = s;
+    __syncthreads();
+    if (ty == 0 && ok)
+        c.b[cidx(c.n0, c.n1, ci, cj, ck)] = (T)0.125 * (((part[0][lane] + part[1][lane]) + part[2][lane]) + part[3][lane]);
 }
 
 template <typename T>
@@ -545,8 +611,8 @@ static int vcycle(paris_ctx* c, int nu1, int nu2, T** x0) {
             cur[L] = l.x;
         }
         LV<T> cv = view(lv[L + 1]);
-        PARIS_LAUNCH_N(c, kname<T>("mg_restrict"), l.N, k_fast_restrict<T>, row_grid(cv.n0, cv.n1, cv.n2), 128, 0,
-                       view_x(l, cur[L]), cv, c->bnd);
+        PARIS_LAUNCH_N(c, kname<T>("mg_restrict"), l.N, k_fast_restrict2<T>, dim3(div_up(cv.n0, 32), cv.n1, cv.n2),
+                       dim3(32, 4), 0, view_x(l, cur[L]), cv, c->bnd);
     }
     LVSet<T> S;
     for (int L = 0; L < nl; L++) S.l[L] = view(lv[L]);

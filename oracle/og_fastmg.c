@@ -108,7 +108,8 @@ static void resid_##SUF(const fm_mg* mg, fm_level* l, const T* b, const T* x, T*
             }                                                                                \
 }                                                                                            \
 /* r = b - A x in flux form, b + sum_f a_f (x_f - x_c): the FP64 outer loop */               \
-static void resid_flux_##SUF(const fm_mg* mg, fm_level* l, const T* b, const T* x, T* r) {   \
+static __attribute__((unused)) void resid_flux_##SUF(const fm_mg* mg, fm_level* l, const T* b, const T* x, \
+                                                      T* r) {                                \
     const int* per = mg->per;                                                                \
     for (int k = 0; k < l->n[2]; k++)                                                        \
         for (int j = 0; j < l->n[1]; j++)                                                    \

@@ -285,22 +285,26 @@ static double og_ls2vof_in_cell(const double st[27], int* nflag) {
 typedef struct {
     int nb;
     const double *xc, *yc, *zc, *rad;
+    double cdir[3];   /* 1/(1 + excentricity), 0 along a cylinder's axis */
+    int prune;        /* spheres (cdir = 1): candidate bubbles per cell */
     int ncand;
     int cand[4096];
 } og_spheres;
 
-/* shapes2ls with excentricity 0 and ipar 0 (spheres), vofmodules.f90:973-993:
- * max over bubbles of rad^2 - |x - xc|^2.  The max runs over the candidate
- * bubbles of the current cell only; og_candidates() keeps every bubble that
- * can reach the max anywhere in the cell's stencil region, so the value is
- * the same as the max over all bubbles. */
+/* shapes2ls, vofmodules.f90:973-993: max over bubbles of rad^2 -
+ * sum_a cdir(a) (x_a - xc_a)^2, cdir = 1/(1 + excentricity) with the
+ * cylinder axis (ipar < 0) zeroed.  For spheres the max runs over the
+ * candidate bubbles of the current cell only; og_candidates() keeps every
+ * bubble that can reach the max anywhere in the cell's stencil region, so the
+ * value is the same as the max over all bubbles. */
 static double og_shapes2ls(const og_spheres* s, double xx, double yy, double zz) {
     double r = -2.0e6;
     for (int q = 0; q < s->ncand; q++) {
         int ib = s->cand[q];
         double v = s->rad[ib] * s->rad[ib] -
-                   (1.0 * ((xx - s->xc[ib]) * (xx - s->xc[ib])) + 1.0 * ((yy - s->yc[ib]) * (yy - s->yc[ib])) +
-                    1.0 * ((zz - s->zc[ib]) * (zz - s->zc[ib])));
+                   (s->cdir[0] * ((xx - s->xc[ib]) * (xx - s->xc[ib])) +
+                    s->cdir[1] * ((yy - s->yc[ib]) * (yy - s->yc[ib])) +
+                    s->cdir[2] * ((zz - s->zc[ib]) * (zz - s->zc[ib])));
         r = r > v ? r : v;
     }
     return r;
@@ -355,7 +359,7 @@ static void og_ls2vof_refined(const og_grid* g, og_spheres* s, int n1, double* c
                 }
                 if (n1 == 1 || refinethis) {
                     double dx1 = g->dx[i] / n1, dy1 = g->dy[j] / n1, dz1 = g->dz[k] / n1;
-                    {   /* stencil points lie within half a cell plus one sub-cell of the centre */
+                    if (s->prune) {   /* stencil points lie within half a cell plus one sub-cell of the centre */
                         double hx = 0.5 * g->dx[i] + dx1, hy = 0.5 * g->dy[j] + dy1, hz = 0.5 * g->dz[k] + dz1;
                         og_candidates(s, g->x[i], g->y[j], g->z[k], 1.000001 * sqrt(hx * hx + hy * hy + hz * hz));
                     }
@@ -398,12 +402,38 @@ static void og_ls2vof_refined(const og_grid* g, og_spheres* s, int n1, double* c
 
 /* levelset2vof(shapes2ls, 0) without VOFI (vofmodules.f90:1048-1109) followed by
  * the end of initconditions_VOF (:788-792): ghosts, SetVOFBC, phase. */
+static int og_init_shapes_impl(const paris_grid_desc* desc, int nb, const double* xc, const double* yc,
+                               const double* zc, const double* rad, const double* excentricity, int ipar,
+                               int refinement, int jacobi, double* cvof, int32_t* flag, int32_t* phase);
+
 int og_init_spheres(const paris_grid_desc* desc, int nb, const double* xc, const double* yc,
                     const double* zc, const double* rad, int refinement, int jacobi,
                     double* cvof, int32_t* flag, int32_t* phase) {
+    return og_init_shapes_impl(desc, nb, xc, yc, zc, rad, NULL, 0, refinement, jacobi, cvof, flag, phase);
+}
+
+/* levelset2vof(shapes2ls, ipar) with the excentricity of module_2phase:
+ * ipar = 0 spheres, -1/-2/-3 a cylinder along x/y/z (one bubble). */
+int og_init_shapes(const paris_grid_desc* desc, int nb, const double* xc, const double* yc, const double* zc,
+                   const double* rad, const double* excentricity, int ipar, int refinement, double* cvof,
+                   int32_t* flag, int32_t* phase) {
+    if (ipar < -3 || ipar > 0 || (ipar < 0 && nb != 1)) return PARIS_BAD_ARGS;
+    return og_init_shapes_impl(desc, nb, xc, yc, zc, rad, excentricity, ipar, refinement, 0, cvof, flag, phase);
+}
+
+static int og_init_shapes_impl(const paris_grid_desc* desc, int nb, const double* xc, const double* yc,
+                               const double* zc, const double* rad, const double* excentricity, int ipar,
+                               int refinement, int jacobi, double* cvof, int32_t* flag, int32_t* phase) {
     og_grid* g = og_grid_new(desc);
     og_spheres s;
     s.nb = nb; s.xc = xc; s.yc = yc; s.zc = zc; s.rad = rad; s.ncand = 0;
+    for (int a = 0; a < 3; a++) s.cdir[a] = 1.0 / (1.0 + (excentricity ? excentricity[a] : 0.0));
+    if (ipar < 0) s.cdir[-ipar - 1] = 0.0;
+    s.prune = s.cdir[0] == 1.0 && s.cdir[1] == 1.0 && s.cdir[2] == 1.0;
+    if (!s.prune) {
+        s.ncand = nb < 4096 ? nb : 4096;
+        for (int q = 0; q < s.ncand; q++) s.cand[q] = q;
+    }
     og_ls2vof_refined(g, &s, 1, cvof, flag, flag);
     og_do_all_ighost(g, flag);
     og_do_all_ghost(g, cvof);

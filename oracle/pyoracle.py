@@ -78,6 +78,7 @@ def lib():
             "og_time_step_size": (I, [G, P, P, P, D, D, D, P, P]),
             "og_clean_debris": (I, [G, P, P, I, I, P]),
             "og_vof_mom_sweeps": (I, [G, I, D, I, I, I, P, P, P, P, P, P, P, P, P, P]),
+            "og_init_shapes": (I, [G, I, P, P, P, P, P, I, I, P, P, P]),
             "og_flux_centroid": (None, [P, D, P, P, P]),
             "og_get_cfl_and_check": (I, [G, P, P, P, D, D, P]),
             "og_calc_stats": (I, [G, P, P, P, P, P, P, P, P, ctypes.POINTER(capi.StatsOpts), P, P]),
@@ -157,6 +158,22 @@ def linfunc(desc, cvof, a1, a2, meanflag):
     field = zeros(desc)
     lib().og_linfunc(ctypes.byref(desc), _p(field), _p(cvof), a1, a2, meanflag)
     return field
+
+
+def init_shapes(desc, centers, radii, excentricity=(0.0, 0.0, 0.0), ipar=0, refinement=8):
+    """levelset2vof(shapes2ls, ipar): spheres (ipar 0) or one cylinder along
+    x/y/z (ipar -1/-2/-3), with the excentricity of the bubbles."""
+    c = np.ascontiguousarray(np.asarray(centers, dtype=np.float64).reshape(-1, 3))
+    r = np.ascontiguousarray(np.asarray(radii, dtype=np.float64).reshape(-1))
+    xc, yc, zc = (np.ascontiguousarray(c[:, a]) for a in range(3))
+    e = np.ascontiguousarray(np.asarray(excentricity, dtype=np.float64))
+    cvof = zeros(desc)
+    flag = zeros(desc, np.int32)
+    phase = zeros(desc, np.int32)
+    st = lib().og_init_shapes(ctypes.byref(desc), len(r), _p(xc), _p(yc), _p(zc), _p(r), _p(e), ipar, refinement,
+                              _p(cvof), _p(flag), _p(phase))
+    assert st == 0, st
+    return cvof, flag, phase
 
 
 def init_spheres(desc, centers, radii, refinement=8, jacobi=False):

@@ -4,6 +4,8 @@ are committed so that the tests need no reference tree).
 
   Tests/VOF/volumeref.txt        -> vof_volumeref.txt
   Tests/VOF/centerofmassref.txt  -> vof_centerofmassref.txt
+  Tests/CylinderAdvection/reference.txt -> cylinder_advection_cvof.txt
+      (cvof of the mid plane after 3800 steps, i outer and j inner, 16 x 16)
 """
 import os
 import sys
@@ -22,6 +24,15 @@ def main(ref_root):
             for r in rows:
                 f.write(f"{float(r[0]):.6e} {float(r[1]):.6e}\n")
         print("wrote", dst, len(rows), "rows")
+    src, dst = "Tests/CylinderAdvection/reference.txt", "cylinder_advection_cvof.txt"
+    with open(os.path.join(ref_root, src)) as f:
+        vals = [line.strip() for line in f if line.strip()]
+    with open(os.path.join(HERE, dst), "w") as f:
+        f.write(f"# {src} of slitvinov/paris-git: cvof(i, j, (ks+ke)/2) at step 3800, i outer, j inner, "
+                "as printed (E14.5)\n")
+        for v in vals:
+            f.write(v + "\n")
+    print("wrote", dst, len(vals), "values")
 
 
 if __name__ == "__main__":

@@ -95,12 +95,6 @@ __global__ void k_fast_smooth(const LV<T> v, const Bnd B, int color) {
     if (i < v.n0) smooth_cell(v, B, i, j, k);
 }
 
-template <typename T>
-__global__ void k_fast_restrict(const LV<T> f, const LV<T> c, const Bnd B) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-    if (i < c.n0) restrict_cell(f, c, B, i, j, k);
-}
-
 // Residual and restriction with one warp per 32 coarse cells of a fine row:
 // threadIdx.y = dj + 2 dk picks the fine row of the 2x2x2 block, and each
 // lane computes the residuals of its fine pair (2i, 2i+1) from pair loads

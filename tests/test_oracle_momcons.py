@@ -95,3 +95,25 @@ def test_rejects_unsupported_boundaries(capi, orc):
     du, dv, dw = (orc.zeros(d) for _ in range(3))
     with pytest.raises(AssertionError):
         orc.vof_mom_sweeps(d, 0, 1e-3, cvof, flag, u, v, w, du, dv, dw, orc.zeros(d))
+
+
+def test_init_shapes_cylinders_and_spheres(capi, orc):
+    """levelset2vof(shapes2ls, ipar): a cylinder along each axis with an
+    excentricity has the area pi a b of its ellipse per unit length (to the
+    refinement's accuracy), and spheres without excentricity are the
+    init_spheres fields bit for bit."""
+    n = 32
+    d = capi.make_desc((n, n, n))
+    g = d.ng
+    for axis in range(3):
+        exc = [0.0, 0.0, 0.0]
+        exc[(axis + 1) % 3] = 1.0   # semi-axis sqrt(2) R along the next axis
+        cvof, flag, _ = orc.init_shapes(d, [(0.5, 0.5, 0.5)], [0.2], excentricity=exc, ipar=-(axis + 1))
+        vol = cvof[g:-g, g:-g, g:-g].sum() / n ** 3
+        assert abs(vol - np.pi * 0.2 * 0.2 * np.sqrt(2.0)) < 2e-3, (axis, vol)
+        c = cvof[g:-g, g:-g, g:-g]
+        assert np.array_equal(c, np.moveaxis(np.moveaxis(c, 2 - axis, 0)[[0] * n], 0, 2 - axis)), axis
+    cen = [(0.3, 0.4, 0.5), (0.7, 0.6, 0.45)]
+    a = orc.init_shapes(d, cen, [0.12, 0.1])
+    b = orc.init_spheres(d, cen, [0.12, 0.1])
+    assert all(np.array_equal(x, y) for x, y in zip(a, b))

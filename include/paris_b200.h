@@ -54,7 +54,8 @@ extern "C" {
 
 /* ---- grid and physical parameters -------------------------------------- */
 typedef struct paris_grid_desc {
-    int32_t nx, ny, nz;          /* Nx, Ny, Nz: interior cells (one rank, no MPI split) */
+    int32_t nx, ny, nz;          /* Nx, Ny, Nz: interior cells (one rank, no MPI split); at
+                                    least 4 each, or Nz = 2 for a two-dimensional run    */
     int32_t ng;                  /* Ng of the host arrays; must be 2 (modules.f90 Ng) */
     int32_t bdry_cond[6];        /* PARIS_BC_*, order x- y- z- x+ y+ z+ */
     int32_t vofbdry_cond[6];     /* PARIS_VOFBC_* */

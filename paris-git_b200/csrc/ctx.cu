@@ -139,7 +139,9 @@ __global__ void k_phase_i32(const double* __restrict__ c, int32_t* __restrict__ 
 // ---- exported life cycle --------------------------------------------------
 static int validate(const paris_grid_desc* d) {
     if (!d) return PARIS_BAD_ARGS;
-    if (d->nx < 4 || d->ny < 4 || d->nz < 4 || d->ng != 2) return PARIS_BAD_ARGS;
+    // at least four cells across, or Nz = 2: the reference's two-dimensional
+    // runs (one cell of depth and its periodic image)
+    if (d->nx < 4 || d->ny < 4 || (d->nz < 4 && d->nz != 2) || d->ng != 2) return PARIS_BAD_ARGS;
     if (d->nx > 32767 || d->ny > 32767 || d->nz > 32767) return PARIS_BAD_ARGS;
     for (int a = 0; a < 3; a++) {
         int lo = d->bdry_cond[a], hi = d->bdry_cond[a + 3];

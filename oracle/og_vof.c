@@ -287,6 +287,8 @@ typedef struct {
     const double *xc, *yc, *zc, *rad;
     double cdir[3];   /* 1/(1 + excentricity), 0 along a cylinder's axis */
     int prune;        /* spheres (cdir = 1): candidate bubbles per cell */
+    int wave;         /* wave2ls instead of shapes2ls */
+    double hdir[3], vdir[3], len[3], amp, shift, nsign;
     int ncand;
     int cand[4096];
 } og_spheres;
@@ -297,7 +299,19 @@ typedef struct {
  * candidate bubbles of the current cell only; og_candidates() keeps every
  * bubble that can reach the max anywhere in the cell's stencil region, so the
  * value is the same as the max over all bubbles. */
+/* wave2ls, vofmodules.f90:997-1034: a cosine interface normal to vdir,
+ * varying along hdir, with amplitude 0.5*A_h*dx(nx/2+2) */
+static double og_wave2ls(const og_spheres* s, double xx, double yy, double zz) {
+    const double PI = 3.14159265359;   /* module_grid PI */
+    double w = s->vdir[2] * (-zz + s->len[2] / 2.0) + s->vdir[1] * (-yy + s->len[1] / 2.0) +
+               s->vdir[0] * (-xx + s->len[0] / 2.0) +
+               s->amp * cos(2.0 * PI * (s->hdir[0] * xx / s->len[0] + s->hdir[1] * yy / s->len[1] +
+                                        s->hdir[2] * zz / s->len[2]));
+    return w * s->nsign + s->shift;
+}
+
 static double og_shapes2ls(const og_spheres* s, double xx, double yy, double zz) {
+    if (s->wave) return og_wave2ls(s, xx, yy, zz);
     double r = -2.0e6;
     for (int q = 0; q < s->ncand; q++) {
         int ib = s->cand[q];
@@ -421,12 +435,40 @@ int og_init_shapes(const paris_grid_desc* desc, int nb, const double* xc, const 
     return og_init_shapes_impl(desc, nb, xc, yc, zc, rad, excentricity, ipar, refinement, 0, cvof, flag, phase);
 }
 
+static int og_levelset2vof(og_grid* g, og_spheres* s, int refinement, int jacobi, double* cvof, int32_t* flag,
+                           int32_t* phase);
+
+/* levelset2vof(wave2ls, ipar) (vofmodules.f90:683-689, 997-1034): ipar 1, 2
+ * or 3 puts the interface normal to z, z or y and varying along y, x, x;
+ * A_h = 2, normal_up and hshift as in the reference's namelist. */
+int og_init_wave(const paris_grid_desc* desc, int ipar, int normal_up, double hshift, int refinement, double* cvof,
+                 int32_t* flag, int32_t* phase) {
+    if (ipar < 1 || ipar > 3) return PARIS_BAD_ARGS;
+    og_grid* g = og_grid_new(desc);
+    og_spheres s;
+    memset(&s, 0, sizeof(s));
+    s.wave = 1;
+    const int hpar = ipar == 1 ? 2 : 1, vpar = ipar == 3 ? 2 : 3;   /* 1-based */
+    for (int a = 0; a < 3; a++) {
+        s.hdir[a] = a + 1 == hpar ? 1.0 : 0.0;
+        s.vdir[a] = a + 1 == vpar ? 1.0 : 0.0;
+    }
+    s.len[0] = desc->xlength; s.len[1] = desc->ylength; s.len[2] = desc->zlength;
+    const double A_h = 2.0;
+    const double dxm = g->dx[g->nx / 2 + 2 - 1];   /* dx(nx/2+2) */
+    s.amp = 0.5 * A_h * dxm;
+    s.nsign = normal_up ? 1.0 : -1.0;
+    s.shift = hshift * dxm;
+    return og_levelset2vof(g, &s, refinement, 0, cvof, flag, phase);
+}
+
 static int og_init_shapes_impl(const paris_grid_desc* desc, int nb, const double* xc, const double* yc,
                                const double* zc, const double* rad, const double* excentricity, int ipar,
                                int refinement, int jacobi, double* cvof, int32_t* flag, int32_t* phase) {
     og_grid* g = og_grid_new(desc);
     og_spheres s;
     s.nb = nb; s.xc = xc; s.yc = yc; s.zc = zc; s.rad = rad; s.ncand = 0;
+    s.wave = 0;
     for (int a = 0; a < 3; a++) s.cdir[a] = 1.0 / (1.0 + (excentricity ? excentricity[a] : 0.0));
     if (ipar < 0) s.cdir[-ipar - 1] = 0.0;
     s.prune = s.cdir[0] == 1.0 && s.cdir[1] == 1.0 && s.cdir[2] == 1.0;
@@ -434,6 +476,15 @@ static int og_init_shapes_impl(const paris_grid_desc* desc, int nb, const double
         s.ncand = nb < 4096 ? nb : 4096;
         for (int q = 0; q < s.ncand; q++) s.cand[q] = q;
     }
+    return og_levelset2vof(g, &s, refinement, jacobi, cvof, flag, phase);
+}
+
+/* levelset2vof without VOFI (vofmodules.f90:1048-1109) followed by the end of
+ * initconditions_VOF (:788-792): a first pass at refinement 1, ghosts and
+ * SetVOFBC, the refined pass, ghosts, SetVOFBC, phase.  Frees g. */
+static int og_levelset2vof(og_grid* g, og_spheres* sp, int refinement, int jacobi, double* cvof, int32_t* flag,
+                           int32_t* phase) {
+    og_spheres s = *sp;
     og_ls2vof_refined(g, &s, 1, cvof, flag, flag);
     og_do_all_ighost(g, flag);
     og_do_all_ghost(g, cvof);

@@ -147,9 +147,11 @@ static int validate(const paris_grid_desc* d) {
         int lo = d->bdry_cond[a], hi = d->bdry_cond[a + 3];
         if (lo < 0 || lo > 2 || hi < 0 || hi > 2) return PARIS_BAD_ARGS;
         if ((lo == PARIS_BC_PERIODIC) != (hi == PARIS_BC_PERIODIC)) return PARIS_BAD_ARGS;
+        // a periodic volume fraction needs a periodic velocity; a periodic
+        // velocity may carry dry / wet / outflow VOF ghosts (SetVOFBC after the wrap)
         int vlo = d->vofbdry_cond[a], vhi = d->vofbdry_cond[a + 3];
-        if ((vlo == PARIS_VOFBC_PERIODIC) != (lo == PARIS_BC_PERIODIC)) return PARIS_BAD_ARGS;
-        if ((vhi == PARIS_VOFBC_PERIODIC) != (hi == PARIS_BC_PERIODIC)) return PARIS_BAD_ARGS;
+        if (vlo == PARIS_VOFBC_PERIODIC && lo != PARIS_BC_PERIODIC) return PARIS_BAD_ARGS;
+        if (vhi == PARIS_VOFBC_PERIODIC && hi != PARIS_BC_PERIODIC) return PARIS_BAD_ARGS;
         for (int v : {vlo, vhi})
             if (v != 0 && v != 1 && v != 3 && v != 4) return PARIS_BAD_ARGS;
     }

@@ -165,7 +165,9 @@ __global__ void k_vof_update(const SweepArgs a) {
 // ghost cells of the new cvof and flags: SetVOFBC on walls (orientations
 // x- y- z- x+ y+ z+ in that order, the last one writing a cell wins; 'outflow'
 // copies the boundary cell as it stood after the earlier orientations), then
-// the periodic wrap of do_all_ghost, then get_flags_and_clip.
+// the periodic wrap of do_all_ghost, then get_flags_and_clip.  In swp the
+// exchange of do_all_ghost comes after SetVOFBC, so where the velocity is
+// periodic the wrap wins over a dry/wet/outflow VOF condition.
 
 __global__ void k_vof_ghosts(double* __restrict__ c, int8_t* __restrict__ flag, const Layout L, const Bnd B,
                              long G, double epsc) {
@@ -451,7 +453,11 @@ __global__ void k_ls2vof(const Spheres S, const Layout L, const double* __restri
     fout[n] = fl;
 }
 
-// walls of the initial field: SetVOFBC without the clipping of the sweeps
+// walls of the initial field, without the clipping of the sweeps: the
+// ghosts of levelset2vof (vofmodules.f90:1098-1106), the periodic exchange
+// where the velocity is periodic, then SetVOFBC on every face whose VOF
+// condition is not periodic, over the exchanged value (a direction may be
+// periodic for the velocity and dry/wet for the volume fraction)
 __global__ void k_init_ghosts(double* __restrict__ c, int8_t* __restrict__ flag, const Layout L, const Bnd B, long G) {
     long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (t >= G) return;
@@ -466,11 +472,12 @@ __global__ void k_init_ghosts(double* __restrict__ c, int8_t* __restrict__ flag,
     double val = 0.0;
     int8_t fl = 0;
     bool fixed = false;
+    const int gc[3] = {i, j, k};
     for (int o = 5; o >= 0 && !fixed; o--) {
         int d = o % 3;
         bool lo = o < 3;
-        if (B.per[d]) continue;
-        bool out = lo ? s[d] < 0 : s[d] >= L.n[d];
+        if (B.vofbc[o] == PARIS_VOFBC_PERIODIC) continue;
+        bool out = lo ? gc[d] < 0 : gc[d] >= L.n[d];   // a ghost row of this face (over the periodic image)
         if (!out) continue;
         int cond = B.vofbc[o];
         if (cond == PARIS_VOFBC_DRY) { val = 0.0; fl = 0; fixed = true; }

@@ -6,6 +6,9 @@ are committed so that the tests need no reference tree).
   Tests/VOF/centerofmassref.txt  -> vof_centerofmassref.txt
   Tests/CylinderAdvection/reference.txt -> cylinder_advection_cvof.txt
       (cvof of the mid plane after 3800 steps, i outer and j inner, 16 x 16)
+  Tests/CapWave/prosperetti      -> capwave_prosperetti.txt
+      (Prosperetti's amplitude of the capillary wave against omega_0 t,
+      the initial amplitude scaled to 0.01)
 """
 import os
 import sys
@@ -33,6 +36,14 @@ def main(ref_root):
         for v in vals:
             f.write(v + "\n")
     print("wrote", dst, len(vals), "values")
+    src, dst = "Tests/CapWave/prosperetti", "capwave_prosperetti.txt"
+    with open(os.path.join(ref_root, src)) as f:
+        rows = [line.split() for line in f if line.strip()]
+    with open(os.path.join(HERE, dst), "w") as f:
+        f.write(f"# {src} of slitvinov/paris-git: omega_0 t, amplitude (initial 0.01)\n")
+        for r in rows:
+            f.write(f"{r[0]} {r[1]}\n")
+    print("wrote", dst, len(rows), "rows")
 
 
 if __name__ == "__main__":

@@ -29,7 +29,8 @@ def test_cylinder_advection_matches_the_reference_output(capi, orc):
     st = {"cvof": cvof, "flag": flag, "u": np.full(orc.shape(d), 0.01), "v": np.full(orc.shape(d), 0.01),
           "w": orc.zeros(d), "p": orc.zeros(d)}
     for k in range(1, 3801):
-        orc.ns_step(d, st, k, 0.1, max_error=1e-5, maxit=2000, momcons={"staggered": True, "lin_interp": False})
+        orc.ns_step(d, st, k, 0.1, max_error=1e-5, maxit=2000, momcons={"staggered": True, "lin_interp": False},
+                    solver="fast")
     g = d.ng
     out = st["cvof"][g, g:-g, g:-g].T   # plane (ks+ke)/2 = ks, indexed (i, j)
     ref = golden()

@@ -62,3 +62,28 @@ def test_init_without_device_fails_cleanly(capi):
     st = lib.paris_gpu_init(ctypes.byref(d), ctypes.byref(h))
     assert st in (capi.NO_DEVICE, capi.BAD_ARGS)
     assert not h.value
+
+
+def test_descriptor_validation_rules(capi):
+    """The checks of paris_gpu_init that run before any device call: at least
+    four cells across except Nz = 2 (two-dimensional runs); a periodic volume
+    fraction needs a periodic velocity, while a periodic velocity may carry
+    dry/wet VOF ghosts (the capillary-wave setup).  Accepted descriptors get
+    as far as the device (NO_DEVICE here, OK on a GPU)."""
+    lib = capi.load_library()
+
+    def status(d):
+        h = ctypes.c_void_p()
+        st = lib.paris_gpu_init(ctypes.byref(d), ctypes.byref(h))
+        if h.value:
+            lib.paris_gpu_finalize(h)
+        return st
+
+    accepted = (capi.OK, capi.NO_DEVICE)
+    assert status(capi.make_desc((16, 16, 2))) in accepted
+    assert status(capi.make_desc((16, 16, 3))) == capi.BAD_ARGS
+    assert status(capi.make_desc((16, 2, 16))) == capi.BAD_ARGS
+    vb = [capi.VOFBC_PERIODIC, capi.VOFBC_WET, capi.VOFBC_WET, capi.VOFBC_PERIODIC, capi.VOFBC_DRY, capi.VOFBC_DRY]
+    assert status(capi.make_desc((32, 96, 2), length=(1.0, 3.0, 0.0625), vofbc=vb)) in accepted
+    walls_periodic_vof = capi.make_desc((16, 16, 16), bc="wall", vofbc=[capi.VOFBC_PERIODIC] * 6)
+    assert status(walls_periodic_vof) == capi.BAD_ARGS

@@ -137,27 +137,11 @@ def load_pkg():
     return __graft_entry__.load_package()
 
 
-def smoothed_faces(n, seed=1, sweeps=3, ng=2):
-    """u*, v*, w*: i.i.d. N(0,1) per face, `sweeps` Jacobi sweeps
-    u <- (u + 6 face neighbours)/7 on the periodic grid; ghosted arrays."""
-    rng = np.random.default_rng(seed)
-    out = []
-    for _ in range(3):
-        u = rng.standard_normal((n, n, n))
-        for _ in range(sweeps):
-            p = np.pad(u, 1, mode="wrap")
-            u = (p[1:-1, 1:-1, 1:-1] + p[:-2, 1:-1, 1:-1] + p[2:, 1:-1, 1:-1] + p[1:-1, :-2, 1:-1]
-                 + p[1:-1, 2:, 1:-1] + p[1:-1, 1:-1, :-2] + p[1:-1, 1:-1, 2:]) / 7.0
-        a = np.pad(u, ng, mode="wrap")
-        out.append(np.ascontiguousarray(a))
-    return out
-
-
 def workload(pkg, n, device=0):
     capi, wl = pkg.capi, pkg.workloads
     desc = capi.make_desc((n, n, n), rho1=1.0, rho2=1000.0, device=device)
     cen, rad = wl.drop_layout(64, rmin=0.03, rmax=0.08, seed=0, h=1.0 / n)
-    us = smoothed_faces(n, seed=1)
+    us = wl.smoothed_gaussian_faces((n, n, n), seed=1)
     umax = max(float(np.abs(a).max()) for a in us)
     dt = 0.25 * (1.0 / n) / umax
     return desc, cen, rad, us, dt

@@ -11,8 +11,8 @@
  * A(is:ie, js:je, ks:ke, 8) (modules.f90:2729).  Fields live on the device
  * between calls; upload/download move them to and from the Fortran arrays.
  *
- * A Fortran driver binds these with ISO_C_BINDING; the interface module that
- * keeps the original subroutine names is shown in INTEGRATION.md.
+ * A Fortran driver binds these with ISO_C_BINDING, through an interface
+ * module that keeps the original subroutine names and signatures.
  */
 #ifndef PARIS_B200_H
 #define PARIS_B200_H
@@ -41,8 +41,12 @@ extern "C" {
 /* vofbdry_cond of &VOFPARAMETERS (SetVOFBC, vofmodules.f90:1694-1825).      */
 #define PARIS_VOFBC_DRY       0
 #define PARIS_VOFBC_WET       1
+#define PARIS_VOFBC_JET       2   /* 'jet': x- only; the first ghost layer is inject(j,k) of the
+                                     inject_type below, the second keeps its value (vofmodules.f90:1716-1718,1758-1760,1797-1811) */
 #define PARIS_VOFBC_PERIODIC  3
 #define PARIS_VOFBC_OUTFLOW   4
+#define PARIS_VOFBC_90DEG     5   /* '90deg': the first ghost layer copies the adjacent cell, the
+                                     second keeps its value (vofmodules.f90:1719-1720,1771-1790) */
 
 /* VOF_advect of &VOFPARAMETERS */
 #define PARIS_ADVECT_CIAM  0   /* 'CIAM'      -> swpz (vofnonmodule.f90:126)  */
@@ -74,7 +78,15 @@ typedef struct paris_grid_desc {
     int32_t mixed_heights;       /* mixed_heights flag of the curvature (default 1) */
     int32_t use_full_heights;    /* use_full_heights flag (default 1) */
     int32_t do_rotation;         /* do_rotation flag of the paraboloid fit (default 0) */
-    int32_t reserved[4];
+    int32_t inject_type;         /* inject_type of &PARAMETERS (modules.f90:872); with a 'jet' VOF
+                                    condition the first ghost layer at x- is liquid where
+                                    2 or 4: (y-jetcenter_yc)^2 + (z-jetcenter_zc)^2 < radius_liq_inject^2,
+                                    3: y-jetcenter_yc <= radius_liq_inject,
+                                    5: radius_gas_inject < y-jetcenter_yc < radius_liq_inject,
+                                    and gas otherwise (vofmodules.f90:1797-1811)                  */
+    int32_t reserved[3];
+    double  jetcenter_yc, jetcenter_zc;           /* modules.f90:397 */
+    double  radius_liq_inject, radius_gas_inject; /* modules.f90:395 */
 } paris_grid_desc;
 
 typedef struct paris_ctx* paris_handle_t;
@@ -107,9 +119,8 @@ typedef struct paris_ctx* paris_handle_t;
 int paris_gpu_init(const paris_grid_desc* desc, paris_handle_t* out);
 int paris_gpu_finalize(paris_handle_t h);
 /* Copy one field between the device mirror and a host array in the reference
- * layout (ghost layers included; only the interior is transferred, ghosts are
- * rebuilt on the device from the boundary conditions).  VOF_FLAG/VOF_PHASE
- * take int32 arrays, every other field real(8).                           */
+ * layout, ghost layers included, as they stand.  VOF_FLAG/VOF_PHASE take
+ * int32 arrays, every other field real(8).                                 */
 int paris_gpu_upload(paris_handle_t h, int32_t field, const void* host);
 int paris_gpu_download(paris_handle_t h, int32_t field, void* host);
 /* Device-to-device copy of one real(8) field into another (ghosts included). */
@@ -304,9 +315,11 @@ int paris_project_velocity(paris_handle_t h, double dt);
  * Linf as calcResiduals.  stream: a cudaStream_t or NULL.  Scratch is a fixed
  * 1.5 MiB device array held by every GPU that loads the library: grids above
  * 16,777,216 interior cells are rejected (PARIS_BAD_ARGS).  All calls share
- * that array, so calls that overlap on the GPU race.  The first call on a
- * device looks up the array's device address; make it before any stream
- * capture. */
+ * that array, so calls that overlap on the GPU race.  Every call looks up the
+ * array's device address in the current context (no allocation); with lazy
+ * module loading the first call on a device may load the library's module
+ * and place the array then, so make a first call at set-up time.  All
+ * interior cells count (ExcludeBoundCellCalcRes = F, the reference default). */
 int paris_calc_residuals_noalloc(int32_t nx, int32_t ny, int32_t nz, int32_t ng, const double* A_dev,
                                  const double* p_dev, double* out3, void* stream);
 

@@ -7,7 +7,25 @@
 #include <string.h>
 #include "og.h"
 
-/* SetVOFBC, vofmodules.f90:1694-1825 ('dry' 0, 'wet' 1, 'periodic', 'outflow') */
+/* inject(j,k) of SetVOFBC, vofmodules.f90:1797-1811 (j,k ghosted C indices) */
+static int og_inject(const og_grid* g, int j, int k) {
+    const paris_grid_desc* d = &g->d;
+    double yy = g->y[j] - d->jetcenter_yc, zz = g->z[k] - d->jetcenter_zc;
+    if (d->inject_type == 2 || d->inject_type == 4) {
+        if (yy * yy + zz * zz < d->radius_liq_inject * d->radius_liq_inject) return 1;
+    } else if (d->inject_type == 3) {
+        if (yy <= d->radius_liq_inject) return 1;
+    } else if (d->inject_type == 5) {
+        if (yy > d->radius_gas_inject && yy < d->radius_liq_inject) return 1;
+    }
+    return 0;
+}
+
+/* SetVOFBC, vofmodules.f90:1694-1825: orientations x- y- z- x+ y+ z+ in
+ * turn, each over the whole ghosted extent of the other two directions.
+ * 'dry'/'wet' set both ghost layers, 'outflow' copies the boundary cell into
+ * both; 'jet' (x- only) sets the first layer to inject(j,k) and '90deg' the
+ * first layer to the adjacent cell, leaving the second layer as it was. */
 void og_setvofbc(const og_grid* g, double* cv, int32_t* fl) {
     for (int orient = 0; orient < 6; orient++) {
         int cond = g->d.vofbdry_cond[orient];
@@ -23,15 +41,21 @@ void og_setvofbc(const og_grid* g, double* cv, int32_t* fl) {
                 long base = l * st[t2] + m * st[t3];
                 long g1 = base + (long)(lim + sign) * st[d];
                 long g2 = base + (long)(lim + 2 * sign) * st[d];
+                long in = base + (long)lim * st[d];
                 if (cond == PARIS_VOFBC_DRY || cond == PARIS_VOFBC_WET) {
                     int flag = cond == PARIS_VOFBC_WET ? 1 : 0;
                     cv[g1] = (double)flag; fl[g1] = flag;
                     cv[g2] = (double)flag; fl[g2] = flag;
+                } else if (cond == PARIS_VOFBC_JET) {
+                    /* c(2) = l, c(3) = m: t2 = y, t3 = z for the x- face */
+                    int inj = og_inject(g, l, m);
+                    cv[g1] = (double)inj; fl[g1] = inj;
                 } else if (cond == PARIS_VOFBC_OUTFLOW) {
-                    long in = base + (long)lim * st[d];
                     double cvh = cv[in]; int32_t flh = fl[in];
                     cv[g1] = cvh; fl[g1] = flh;
                     cv[g2] = cvh; fl[g2] = flh;
+                } else if (cond == PARIS_VOFBC_90DEG) {
+                    cv[g1] = cv[in]; fl[g1] = fl[in];
                 }
             }
     }
@@ -485,10 +509,18 @@ static int og_init_shapes_impl(const paris_grid_desc* desc, int nb, const double
 static int og_levelset2vof(og_grid* g, og_spheres* sp, int refinement, int jacobi, double* cvof, int32_t* flag,
                            int32_t* phase) {
     og_spheres s = *sp;
+    /* initialize_VOF: cvof = 0, vof_flag = 3 (vofmodules.f90:436-437) */
+    for (long n = 0; n < g->ntot; n++) { cvof[n] = 0.0; flag[n] = 3; }
     og_ls2vof_refined(g, &s, 1, cvof, flag, flag);
     og_do_all_ighost(g, flag);
     og_do_all_ghost(g, cvof);
     og_setvofbc(g, cvof, flag);
+    /* the second pass stops with "bad flag" unless the largest flag is 2
+     * (vofmodules.f90:1220-1231); a 'jet' or '90deg' face leaves its second
+     * ghost layer at 3 */
+    int32_t fmax = -2147483647;
+    for (long n = 0; n < g->ntot; n++) fmax = flag[n] > fmax ? flag[n] : fmax;
+    if (refinement > 1 && fmax != 2) { og_grid_free(g); return PARIS_BAD_ARGS; }
     /* jacobi = 1: pass 2 reads the flags of pass 1 only (the order-free variant
      * computed by the device); 0: the reference's in-place loop order. */
     int32_t* f1 = NULL;
@@ -502,6 +534,14 @@ static int og_levelset2vof(og_grid* g, og_spheres* sp, int refinement, int jacob
     og_do_all_ighost(g, flag);
     og_setvofbc(g, cvof, flag);
     if (phase) og_vof_phase(g, cvof, phase);
+    og_grid_free(g);
+    return 0;
+}
+
+/* SetVOFBC on host arrays, for the tests */
+int og_setvofbc_host(const paris_grid_desc* desc, double* cv, int32_t* fl) {
+    og_grid* g = og_grid_new(desc);
+    og_setvofbc(g, cv, fl);
     og_grid_free(g);
     return 0;
 }

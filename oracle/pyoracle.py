@@ -54,6 +54,7 @@ def lib():
             "og_fill_ghosts": (None, [G, P]),
             "og_vofsweeps": (I, [G, I, D, P, P, P, P, P, P]),
             "og_flags_clip": (I, [G, P, P]),
+            "og_setvofbc_host": (I, [G, P, P]),
             "og_linfunc": (I, [G, P, P, D, D, I]),
             "og_init_spheres": (I, [G, I, P, P, P, P, I, I, P, P, P]),
             "og_fastmg_solve": (I, [G, P, P, D, I, I, I, I, I, P]),
@@ -155,6 +156,11 @@ def flags_clip(desc, c, f):
     return lib().og_flags_clip(ctypes.byref(desc), _p(c), _p(f))
 
 
+def setvofbc(desc, cvof, flag):
+    """SetVOFBC(cvof, vof_flag) in place (vofmodules.f90:1694-1825)."""
+    return lib().og_setvofbc_host(ctypes.byref(desc), _p(cvof), _p(flag))
+
+
 def linfunc(desc, cvof, a1, a2, meanflag):
     field = zeros(desc)
     lib().og_linfunc(ctypes.byref(desc), _p(field), _p(cvof), a1, a2, meanflag)
@@ -198,8 +204,10 @@ def init_spheres(desc, centers, radii, refinement=8, jacobi=False):
     cvof = zeros(desc)
     flag = zeros(desc, np.int32)
     phase = zeros(desc, np.int32)
-    lib().og_init_spheres(ctypes.byref(desc), len(r), _p(xc), _p(yc), _p(zc), _p(r), refinement,
-                          1 if jacobi else 0, _p(cvof), _p(flag), _p(phase))
+    st = lib().og_init_spheres(ctypes.byref(desc), len(r), _p(xc), _p(yc), _p(zc), _p(r), refinement,
+                               1 if jacobi else 0, _p(cvof), _p(flag), _p(phase))
+    if st:
+        raise ValueError("ls2vof_refined: bad flag (largest vof_flag after the first pass is not 2)")
     return cvof, flag, phase
 
 

@@ -17,7 +17,7 @@ STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "NAN_DETECTED", 3: "BAD_ARGS",
 
 # boundary conditions
 BC_WALL, BC_PERIODIC, BC_SHEAR = 0, 1, 2
-VOFBC_DRY, VOFBC_WET, VOFBC_PERIODIC, VOFBC_OUTFLOW = 0, 1, 3, 4
+VOFBC_DRY, VOFBC_WET, VOFBC_JET, VOFBC_PERIODIC, VOFBC_OUTFLOW, VOFBC_90DEG = 0, 1, 2, 3, 4, 5
 ADVECT_CIAM, ADVECT_WY = 0, 1
 MEAN_ARITH, MEAN_HARM = 101, 102
 
@@ -50,7 +50,10 @@ class GridDesc(ctypes.Structure):
         ("mixed_heights", ctypes.c_int32),
         ("use_full_heights", ctypes.c_int32),
         ("do_rotation", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 4),
+        ("inject_type", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 3),
+        ("jetcenter_yc", ctypes.c_double), ("jetcenter_zc", ctypes.c_double),
+        ("radius_liq_inject", ctypes.c_double), ("radius_gas_inject", ctypes.c_double),
     ]
 
 
@@ -103,11 +106,13 @@ class SolveResult(ctypes.Structure):
 def make_desc(n, length=(1.0, 1.0, 1.0), bc="periodic", vofbc=None, advect=ADVECT_CIAM,
               rho1=1.0, rho2=1.0, mu1=0.0, mu2=0.0, sigma=0.0, epsc=1e-12, nrelax=3,
               sym_mg=0, nfilter=0, dens_mean=MEAN_ARITH, visc_mean=MEAN_ARITH, device=0,
-              mixed_heights=1, use_full_heights=1, do_rotation=0):
+              mixed_heights=1, use_full_heights=1, do_rotation=0, jet=None):
     """Grid descriptor with the reference's namelist defaults.
 
     bc: "periodic", "wall", or a 6-sequence of BDRY_COND codes (x- y- z- x+ y+ z+).
     vofbc: None (periodic where bc is periodic, 'dry' at walls) or 6 codes.
+    jet: None or (inject_type, jetcenter_yc, jetcenter_zc, radius_liq_inject,
+    radius_gas_inject) for a 'jet' VOF face.
     """
     d = GridDesc()
     d.nx, d.ny, d.nz = (int(v) for v in n)
@@ -129,6 +134,9 @@ def make_desc(n, length=(1.0, 1.0, 1.0), bc="periodic", vofbc=None, advect=ADVEC
     d.rho1, d.rho2, d.mu1, d.mu2, d.sigma, d.epsc = rho1, rho2, mu1, mu2, sigma, epsc
     d.nrelax, d.sym_mg, d.device = nrelax, sym_mg, device
     d.mixed_heights, d.use_full_heights, d.do_rotation = mixed_heights, use_full_heights, do_rotation
+    if jet is not None:
+        d.inject_type = int(jet[0])
+        d.jetcenter_yc, d.jetcenter_zc, d.radius_liq_inject, d.radius_gas_inject = (float(v) for v in jet[1:5])
     return d
 
 

@@ -44,6 +44,76 @@ struct Bnd {
     int vofbc[6];     // vofbdry_cond
 };
 
+// The inflow of a 'jet' VOF condition (x- face): inject(j,k) of SetVOFBC,
+// vofmodules.f90:1797-1811, from the cell centres y(j), z(k).
+struct VofJet {
+    int type;                  // inject_type
+    double yc, zc, rliq, rgas; // jetcenter_yc, jetcenter_zc, radius_liq_inject, radius_gas_inject
+    const double* y;           // cell centres, ghosted index j + Ng
+    const double* z;
+};
+
+__device__ inline int vof_inject(const VofJet& J, int ng, int j, int k) {
+    const double yy = J.y[j + ng] - J.yc, zz = J.z[k + ng] - J.zc;
+    if (J.type == 2 || J.type == 4) return yy * yy + zz * zz < J.rliq * J.rliq ? 1 : 0;
+    if (J.type == 3) return yy <= J.rliq ? 1 : 0;
+    if (J.type == 5) return (yy > J.rgas && yy < J.rliq) ? 1 : 0;
+    return 0;
+}
+
+// SetVOFBC (vofmodules.f90:1694-1825) at ghost cell (i,j,k), together with the
+// periodic wrap of do_all_ghost.  The orientations x- y- z- x+ y+ z+ write in
+// that order, so the cell's value is found walking them backwards: the last
+// one that writes the cell decides it.  'dry'/'wet' (both layers) and 'jet'
+// (first layer at x-) fix the value; 'outflow' (both layers) and '90deg'
+// (first layer) copy the adjacent cell as it stood after the orientations
+// before them, so the walk continues from that cell.
+//   SWEEP = true: swp's order, SetVOFBC then the wrap, which wins wherever the
+//   velocity is periodic.  SWEEP = false: initconditions_VOF's order, the wrap
+//   then SetVOFBC, which wins on every face whose VOF condition is not
+//   periodic.
+// Returns true with v set when a condition fixes the value.  Otherwise the
+// ghost takes the value of cell s: an interior cell, or a ghost cell that no
+// orientation writes (the second layer of a 'jet' or '90deg' face), which
+// keeps the value it held.
+template <bool SWEEP>
+__device__ inline bool vof_ghost_rule(const Layout& L, const Bnd& B, const VofJet& J, int i, int j, int k, int s[3],
+                                      double& v) {
+    const int gc[3] = {i, j, k};
+    s[0] = i; s[1] = j; s[2] = k;
+    for (int d = 0; d < 3; d++)
+        if (B.per[d]) {
+            if (s[d] < 0) s[d] += L.n[d];
+            else if (s[d] >= L.n[d]) s[d] -= L.n[d];
+        }
+    for (int o = 5; o >= 0; o--) {
+        const int d = o % 3;
+        const bool lo = o < 3;
+        const int cond = B.vofbc[o];
+        if (SWEEP ? B.per[d] != 0 : cond == PARIS_VOFBC_PERIODIC) continue;
+        const int a = SWEEP ? s[d] : gc[d];
+        const bool out = lo ? a < 0 : a >= L.n[d];
+        if (!out) continue;
+        const bool first = lo ? a == -1 : a == L.n[d];
+        if (cond == PARIS_VOFBC_DRY || cond == PARIS_VOFBC_WET) {
+            v = cond == PARIS_VOFBC_WET ? 1.0 : 0.0;
+            return true;
+        }
+        if (cond == PARIS_VOFBC_JET) {
+            if (!first) continue;
+            v = (double)vof_inject(J, L.ng, s[1], s[2]);
+            return true;
+        }
+        if (cond == PARIS_VOFBC_90DEG && !first) continue;
+        s[d] = lo ? 0 : L.n[d] - 1;   // outflow, or the first layer of 90deg
+    }
+    return false;
+}
+
+__device__ inline bool vof_interior(const Layout& L, const int s[3]) {
+    return s[0] >= 0 && s[0] < L.n[0] && s[1] >= 0 && s[1] < L.n[1] && s[2] >= 0 && s[2] < L.n[2];
+}
+
 // ---- ghost cells ---------------------------------------------------------
 // Enumerates the ghost cells of a ghosted field in three disjoint regions
 // (x-slabs over all j,k; y-slabs over interior i, all k; z-slabs over interior

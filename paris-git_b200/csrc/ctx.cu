@@ -153,8 +153,11 @@ static int validate(const paris_grid_desc* d) {
         if (vlo == PARIS_VOFBC_PERIODIC && lo != PARIS_BC_PERIODIC) return PARIS_BAD_ARGS;
         if (vhi == PARIS_VOFBC_PERIODIC && hi != PARIS_BC_PERIODIC) return PARIS_BAD_ARGS;
         for (int v : {vlo, vhi})
-            if (v != 0 && v != 1 && v != 3 && v != 4) return PARIS_BAD_ARGS;
+            if (v < PARIS_VOFBC_DRY || v > PARIS_VOFBC_90DEG) return PARIS_BAD_ARGS;
+        // SetVOFBC: "jet only at x-" (vofmodules.f90:1717)
+        if (vhi == PARIS_VOFBC_JET || (a > 0 && vlo == PARIS_VOFBC_JET)) return PARIS_BAD_ARGS;
     }
+    if (d->inject_type < 0 || d->inject_type > 5) return PARIS_BAD_ARGS;
     if (d->xlength <= 0 || d->ylength <= 0 || d->zlength <= 0) return PARIS_BAD_ARGS;
     return PARIS_OK;
 }
@@ -204,6 +207,7 @@ extern "C" int paris_gpu_init(const paris_grid_desc* desc, paris_handle_t* out) 
     if (!s) s = upload_vec(c, &c->yh, c->h_yh);
     if (!s) s = upload_vec(c, &c->zh, c->h_zh);
     if (!s && cudaMalloc(&c->red_part, 8L * kRedBlocks * sizeof(double)) != cudaSuccess) s = PARIS_CUDA_ERROR;
+    if (!s && cudaMalloc(&c->debris_count, sizeof(int)) != cudaSuccess) s = PARIS_CUDA_ERROR;
     if (!s && cudaHostAlloc(&c->red_host, 8 * sizeof(double), cudaHostAllocMapped) != cudaSuccess) s = PARIS_CUDA_ERROR;
     if (!s && cudaHostGetDevicePointer((void**)&c->red_host_dev, c->red_host, 0) != cudaSuccess) s = PARIS_CUDA_ERROR;
     for (int f : {PARIS_FIELD_CVOF, PARIS_FIELD_U, PARIS_FIELD_V, PARIS_FIELD_W, PARIS_FIELD_RHO, PARIS_FIELD_P})
@@ -235,7 +239,7 @@ extern "C" int paris_gpu_finalize(paris_handle_t c) {
                     (void*)c->rhs, (void*)c->A, (void*)c->red_part, (void*)c->fast_r64,
                     (void*)c->fast_d64, (void*)c->fast_q64,
                     (void*)c->vflux, (void*)c->mixlist, (void*)c->mixcount, (void*)c->kflag, (void*)c->st_list,
-                    (void*)c->st_count, (void*)c->adj, (void*)c->stats_part, (void*)c->stats_out, (void*)c->mom_tab,
+                    (void*)c->st_count, (void*)c->debris_count, (void*)c->adj, (void*)c->stats_part, (void*)c->stats_out, (void*)c->mom_tab,
                     (void*)c->mc_tmp, (void*)c->mc_tmp2, (void*)c->mc_work, (void*)c->mc_fv, (void*)c->mc_flag,
                     (void*)c->mc_cg})
         free_ptr(p);

@@ -53,6 +53,7 @@ struct paris_ctx {
     int8_t* kflag = nullptr;       // kappaflag of the curvature passes
     int* st_list = nullptr;        // interior mixed cells of the curvature passes
     int* st_count = nullptr;
+    int* debris_count = nullptr;   // cells cleaned by a sweep of clean_debris method 3
     int32_t* i32stage = nullptr;   // staging for int32 host transfers
     // pressure equation, compact interior arrays (N each)
     double *cx = nullptr, *cy = nullptr, *cz = nullptr, *rhs = nullptr;
@@ -137,7 +138,20 @@ int ctx_copy(paris_ctx* c, double* dst, const double* src, long n);   // device 
 
 // vof.cu: SetVOFBC on the ghosts of a volume fraction and its flags (dry
 // and wet walls fixed, periodic images, copies elsewhere), no clipping
-__global__ void k_init_ghosts(double* __restrict__ c, int8_t* __restrict__ flag, const Layout L, const Bnd B, long G);
+__global__ void k_init_ghosts(double* __restrict__ c, int8_t* __restrict__ flag, const Layout L, const Bnd B,
+                              const VofJet J, long G, double epsc);
+// the 'jet' inflow parameters of the handle's descriptor
+inline VofJet ctx_vof_jet(const paris_ctx* c) {
+    VofJet J;
+    J.type = c->d.inject_type;
+    J.yc = c->d.jetcenter_yc;
+    J.zc = c->d.jetcenter_zc;
+    J.rliq = c->d.radius_liq_inject;
+    J.rgas = c->d.radius_gas_inject;
+    J.y = c->yc;
+    J.z = c->zc;
+    return J;
+}
 // vof.cu: one split sweep (swpz or swpr, then SetVOFBC, get_flags_and_clip
 // and the ghosts) along d of the volume fraction src into dst with its flags;
 // us: the face velocity of the sweep, cg: c_mask for the Weymouth-Yue sweep

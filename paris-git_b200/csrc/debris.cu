@@ -5,9 +5,12 @@
 // second cvof buffer and a copy puts them back.  Method 3 cleans the mixed
 // cells in place in the reference's k, j, i order: a cell sees the cells
 // cleaned before it in the same sweep.  The sweep runs exactly in parallel
-// by wavefronts t = i + 2j + 4k: every neighbour that comes earlier in
-// that order has a smaller t, every later one a larger t, and no two
-// neighbours share a t, so the cells of one wavefront are independent and
+// by wavefronts t = i + 2j + 4k: no neighbour of a cell (offsets of at most
+// one in each index) lies on the cell's own wavefront, and a neighbour that
+// comes earlier in the k, j, i order has a smaller t, a later one a larger t
+// (|di + 2 dj| < 4, so the sign of the t difference is that of dk, then dj,
+// then di).  Two neighbours of a cell may share a wavefront with each other,
+// but never with the cell, so the cells of one wavefront are independent and
 // the wavefronts in increasing t reproduce the sequential sweep.  One block
 // walks them, with a barrier between wavefronts.  Ghost cells keep their
 // values during a sweep (the reference refreshes them only between sweeps).
@@ -128,8 +131,7 @@ extern "C" int paris_clean_debris(paris_handle_t c, int32_t method, int32_t neig
         PARIS_LAUNCH(c, k_debris_copy_back, g, 128, 0, cv, c->c2, L);
         nsw = 1;
     } else {
-        int* d_cleaned = nullptr;
-        PARIS_CUDA_TRY(c, cudaMalloc(&d_cleaned, sizeof(int)));
+        int* d_cleaned = c->debris_count;   // written by every sweep
         int cleaned_mix = 0;
         bool all_clean = false;
         int st = PARIS_OK;
@@ -152,7 +154,6 @@ extern "C" int paris_clean_debris(paris_handle_t c, int32_t method, int32_t neig
                              c->d.epsc);
             }
         }
-        cudaFree(d_cleaned);
         if (st != PARIS_OK) {
             ctx_set_error(c, "clean_debris: a device transfer failed");
             return st;

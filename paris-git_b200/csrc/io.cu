@@ -204,7 +204,7 @@ extern "C" int paris_backup_vof_read(paris_handle_t c, const char* filename, dou
     PARIS_LAUNCH(c, k_flags_clip, dim3(div_up(L.n[0], 128), L.n[1], L.n[2]), 128, 0, cv, c->flag, L, c->d.epsc);
     const long G = ghost_count(L);
     // SetVOFBC + do_all_ghost / do_all_ighost of the restart path (paris.f90:3174-3178)
-    PARIS_LAUNCH(c, k_init_ghosts, div_up(G, 256), 256, 0, cv, c->flag, L, c->bnd, G);
+    PARIS_LAUNCH(c, k_init_ghosts, div_up(G, 256), 256, 0, cv, c->flag, L, c->bnd, ctx_vof_jet(c), G, c->d.epsc);
     for (int q = 0; q < 3; q++) PARIS_CHECK(ctx_ghost_fill(c, c->fld[fields[q]]));
     PARIS_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     if (time) *time = hdr[0];

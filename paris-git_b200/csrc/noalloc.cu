@@ -13,10 +13,14 @@
 //  - every call on a device shares g_na_part / g_na_out and leaves its sums
 //    there; each call overwrites every slot it reads, so nothing needs to be
 //    cleared, but calls whose kernels overlap on the GPU race on the arrays;
-//  - the first call on a device looks up the device addresses of the arrays
-//    (cudaGetSymbolAddress with that device current); make that first call
-//    before any stream capture.
-#include <mutex>
+//  - every call looks up the device addresses of the arrays for the current
+//    device and context (cudaGetSymbolAddress, which allocates nothing), so a
+//    device reset or another context is followed; with lazy module loading
+//    (the CUDA default) the first call on a device may load this module and
+//    place the arrays at that moment, so make a first call at set-up time;
+//  - all cells count, as calcResiduals with ExcludeBoundCellCalcRes = F (the
+//    reference's default); the variant that skips the cells next to walls
+//    (modules.f90:3347-3359) is not provided.
 #include "ctx.cuh"
 
 static constexpr int kNaThreads = 256;
@@ -25,17 +29,6 @@ static constexpr long kNaMaxCells = kNaThreads * kNaMaxBlocks;
 
 static __device__ __align__(256) double g_na_part[3 * kNaMaxBlocks];   // 1.5 MiB
 static __device__ __align__(256) double g_na_out[3];
-
-namespace {
-struct NaDevice {
-    double* part = nullptr;
-    double* out = nullptr;
-    bool ready = false;
-};
-constexpr int kNaMaxDevices = 64;
-NaDevice g_na_dev[kNaMaxDevices];
-std::mutex g_na_mutex;
-}  // namespace
 
 // |r| of every interior cell, one cell per thread; block sums of |r|, r^2, max|r|
 __global__ void __launch_bounds__(kNaThreads) k_na_residuals(const double* __restrict__ A, const double* __restrict__ p,
@@ -79,22 +72,14 @@ __global__ void k_na_finish(const double* __restrict__ part, long nblocks, doubl
     if (threadIdx.x == 0) out[slot] = v;
 }
 
-// Device addresses of the scratch arrays for the current device (set-up on
-// the first call per device).
-static int na_setup(int dev, NaDevice** out) {
-    if (dev < 0 || dev >= kNaMaxDevices) return PARIS_BAD_ARGS;
-    std::lock_guard<std::mutex> lock(g_na_mutex);
-    NaDevice& d = g_na_dev[dev];
-    if (!d.ready) {
-        void* pp = nullptr;
-        void* po = nullptr;
-        if (cudaGetSymbolAddress(&pp, g_na_part) != cudaSuccess) return PARIS_CUDA_ERROR;
-        if (cudaGetSymbolAddress(&po, g_na_out) != cudaSuccess) return PARIS_CUDA_ERROR;
-        d.part = (double*)pp;
-        d.out = (double*)po;
-        d.ready = true;
-    }
-    *out = &d;
+// Device addresses of the scratch arrays in the current device's context.
+static int na_scratch(double** part, double** out) {
+    void* pp = nullptr;
+    void* po = nullptr;
+    if (cudaGetSymbolAddress(&pp, g_na_part) != cudaSuccess) return PARIS_CUDA_ERROR;
+    if (cudaGetSymbolAddress(&po, g_na_out) != cudaSuccess) return PARIS_CUDA_ERROR;
+    *part = (double*)pp;
+    *out = (double*)po;
     return PARIS_OK;
 }
 
@@ -105,17 +90,18 @@ extern "C" int paris_calc_residuals_noalloc(int32_t nx, int32_t ny, int32_t nz, 
     if (N > kNaMaxCells) return PARIS_BAD_ARGS;   // scratch holds kNaMaxBlocks partial sums
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess) return PARIS_NO_DEVICE;
-    NaDevice* d = nullptr;
-    int st = na_setup(dev, &d);
+    double* part = nullptr;
+    double* dout = nullptr;
+    int st = na_scratch(&part, &dout);
     if (st != PARIS_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
     long nblocks = (N + kNaThreads - 1) / kNaThreads;
-    k_na_residuals<<<(unsigned)nblocks, kNaThreads, 0, s>>>(A_dev, p_dev, nx, ny, nz, ng, d->part, nblocks);
+    k_na_residuals<<<(unsigned)nblocks, kNaThreads, 0, s>>>(A_dev, p_dev, nx, ny, nz, ng, part, nblocks);
     if (cudaGetLastError() != cudaSuccess) return PARIS_CUDA_ERROR;
-    k_na_finish<<<3, 256, 0, s>>>(d->part, nblocks, d->out);
+    k_na_finish<<<3, 256, 0, s>>>(part, nblocks, dout);
     if (cudaGetLastError() != cudaSuccess) return PARIS_CUDA_ERROR;
     double sums[3];
-    if (cudaMemcpyAsync(sums, d->out, sizeof(sums), cudaMemcpyDeviceToHost, s) != cudaSuccess) return PARIS_CUDA_ERROR;
+    if (cudaMemcpyAsync(sums, dout, sizeof(sums), cudaMemcpyDeviceToHost, s) != cudaSuccess) return PARIS_CUDA_ERROR;
     if (cudaStreamSynchronize(s) != cudaSuccess) return PARIS_CUDA_ERROR;
     out3[0] = sums[0] / (double)nx / (double)ny / (double)nz;
     out3[1] = sqrt(sums[1] / (double)nx / (double)ny / (double)nz);

@@ -162,39 +162,24 @@ __global__ void k_vof_update(const SweepArgs a) {
     a.flag[n] = fl;
 }
 
-// ghost cells of the new cvof and flags: SetVOFBC on walls (orientations
-// x- y- z- x+ y+ z+ in that order, the last one writing a cell wins; 'outflow'
-// copies the boundary cell as it stood after the earlier orientations), then
-// the periodic wrap of do_all_ghost, then get_flags_and_clip.  In swp the
-// exchange of do_all_ghost comes after SetVOFBC, so where the velocity is
-// periodic the wrap wins over a dry/wet/outflow VOF condition.
-
-__global__ void k_vof_ghosts(double* __restrict__ c, int8_t* __restrict__ flag, const Layout L, const Bnd B,
-                             long G, double epsc) {
+// ghost cells of the new cvof and flags: SetVOFBC (x- y- z- x+ y+ z+ in that
+// order), then the periodic wrap of do_all_ghost, then get_flags_and_clip.
+// In swp the exchange of do_all_ghost comes after SetVOFBC, so where the
+// velocity is periodic the wrap wins over the VOF condition.  A ghost that
+// no condition writes (second layer of 'jet' or '90deg') keeps the value it
+// held before the sweep, which is in the source buffer `old`.
+__global__ void k_vof_ghosts(double* __restrict__ c, const double* __restrict__ old, int8_t* __restrict__ flag,
+                             const Layout L, const Bnd B, const VofJet J, long G, double epsc) {
     long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (t >= G) return;
     int i, j, k;
     if (!ghost_cell(L, t, i, j, k)) return;
-    int s[3] = {i, j, k};
-    for (int d = 0; d < 3; d++)
-        if (B.per[d]) {
-            if (s[d] < 0) s[d] += L.n[d];
-            else if (s[d] >= L.n[d]) s[d] -= L.n[d];
-        }
-    double val = 0.0;
-    bool fixed = false;
-    for (int o = 5; o >= 0 && !fixed; o--) {
-        int d = o % 3;
-        bool lo = o < 3;
-        if (B.per[d]) continue;
-        bool out = lo ? s[d] < 0 : s[d] >= L.n[d];
-        if (!out) continue;
-        int cond = B.vofbc[o];
-        if (cond == PARIS_VOFBC_DRY) { val = 0.0; fixed = true; }
-        else if (cond == PARIS_VOFBC_WET) { val = 1.0; fixed = true; }
-        else s[d] = lo ? 0 : L.n[d] - 1;   // outflow
+    int s[3];
+    double val;
+    if (!vof_ghost_rule<true>(L, B, J, i, j, k, s, val)) {
+        const long q = lidx(L, s[0], s[1], s[2]);
+        val = vof_interior(L, s) ? c[q] : old[q];
     }
-    if (!fixed) val = c[lidx(L, s[0], s[1], s[2])];
     int8_t fl;
     if (val <= epsc) { fl = 0; val = 0.0; }
     else if (val >= 1.0 - epsc) { fl = 1; val = 1.0; }
@@ -244,8 +229,8 @@ int vof_sweep_dir(paris_ctx* c, int d, double dt, const double* src, double* dst
     PARIS_LAUNCH_N(c, "vof_mixed_flux", 0L, k_vof_mixed_flux, 148 * 16, 128, 0, a);
     PARIS_LAUNCH_N(c, "vof_sweep", c->N, k_vof_update, dim3(div_up(L.n[0], 128), L.n[1], L.n[2]), 128, 0, a);
     long G = ghost_count(c->L);
-    PARIS_LAUNCH_N(c, "vof_ghosts", G, k_vof_ghosts, div_up(G, 256), 256, 0, dst, flag, c->L, c->bnd, G,
-                   c->d.epsc);
+    PARIS_LAUNCH_N(c, "vof_ghosts", G, k_vof_ghosts, div_up(G, 256), 256, 0, dst, src, flag, c->L, c->bnd,
+                   ctx_vof_jet(c), G, c->d.epsc);
     return PARIS_OK;
 }
 
@@ -457,37 +442,25 @@ __global__ void k_ls2vof(const Spheres S, const Layout L, const double* __restri
 // ghosts of levelset2vof (vofmodules.f90:1098-1106), the periodic exchange
 // where the velocity is periodic, then SetVOFBC on every face whose VOF
 // condition is not periodic, over the exchanged value (a direction may be
-// periodic for the velocity and dry/wet for the volume fraction)
-__global__ void k_init_ghosts(double* __restrict__ c, int8_t* __restrict__ flag, const Layout L, const Bnd B, long G) {
+// periodic for the velocity and dry/wet for the volume fraction).  Fixed
+// values carry their flag, copies the flag of their source; a ghost that no
+// condition writes keeps its value, with the flag of get_flags_and_clip.
+__global__ void k_init_ghosts(double* __restrict__ c, int8_t* __restrict__ flag, const Layout L, const Bnd B,
+                              const VofJet J, long G, double epsc) {
     long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (t >= G) return;
     int i, j, k;
     if (!ghost_cell(L, t, i, j, k)) return;
-    int s[3] = {i, j, k};
-    for (int d = 0; d < 3; d++)
-        if (B.per[d]) {
-            if (s[d] < 0) s[d] += L.n[d];
-            else if (s[d] >= L.n[d]) s[d] -= L.n[d];
-        }
-    double val = 0.0;
-    int8_t fl = 0;
-    bool fixed = false;
-    const int gc[3] = {i, j, k};
-    for (int o = 5; o >= 0 && !fixed; o--) {
-        int d = o % 3;
-        bool lo = o < 3;
-        if (B.vofbc[o] == PARIS_VOFBC_PERIODIC) continue;
-        bool out = lo ? gc[d] < 0 : gc[d] >= L.n[d];   // a ghost row of this face (over the periodic image)
-        if (!out) continue;
-        int cond = B.vofbc[o];
-        if (cond == PARIS_VOFBC_DRY) { val = 0.0; fl = 0; fixed = true; }
-        else if (cond == PARIS_VOFBC_WET) { val = 1.0; fl = 1; fixed = true; }
-        else s[d] = lo ? 0 : L.n[d] - 1;
-    }
-    if (!fixed) {
-        long src = lidx(L, s[0], s[1], s[2]);
-        val = c[src];
-        fl = flag[src];
+    int s[3];
+    double val;
+    int8_t fl;
+    if (vof_ghost_rule<false>(L, B, J, i, j, k, s, val)) {
+        fl = (int8_t)val;
+    } else {
+        const long q = lidx(L, s[0], s[1], s[2]);
+        val = c[q];
+        if (vof_interior(L, s)) fl = flag[q];
+        else fl = val <= epsc ? 0 : (val >= 1.0 - epsc ? 1 : 2);
     }
     long n = lidx(L, i, j, k);
     c[n] = val;
@@ -497,6 +470,16 @@ __global__ void k_init_ghosts(double* __restrict__ c, int8_t* __restrict__ flag,
 extern "C" int paris_init_spheres(paris_handle_t c, int32_t nb, const double* xc, const double* yc, const double* zc,
                                   const double* rad, int32_t refinement) {
     if (!c || nb <= 0 || !xc || !yc || !zc || !rad || refinement < 1) return PARIS_BAD_ARGS;
+    // ls2vof_refined stops with "bad flag" when a 'jet' or '90deg' face is
+    // present: its second ghost layer still holds the vof_flag = 3 of the
+    // allocation (vofmodules.f90:436-437,1222-1231).  Such runs start from an
+    // uploaded field or a restart file.
+    for (int o = 0; o < 6; o++)
+        if (c->d.vofbdry_cond[o] == PARIS_VOFBC_JET || c->d.vofbdry_cond[o] == PARIS_VOFBC_90DEG) {
+            ctx_set_error(c, "ls2vof_refined: bad flag (a 'jet' or '90deg' VOF face leaves vof_flag = 3 "
+                             "in its second ghost layer)");
+            return PARIS_BAD_ARGS;
+        }
     cudaSetDevice(c->dev);
     double* dbuf = nullptr;
     PARIS_CUDA_TRY(c, cudaMalloc(&dbuf, 4L * nb * sizeof(double)));
@@ -513,10 +496,11 @@ extern "C" int paris_init_spheres(paris_handle_t c, int32_t nb, const double* xc
     // pass 1 (n1 = 1) into c2/f2, ghosts, then pass 2 into cvof/flag
     PARIS_LAUNCH(c, k_ls2vof, grid, 64, 0, S, c->L, c->xc, c->yc, c->zc, c->dx, c->dy, c->dz, 1, (const int8_t*)nullptr,
                  (const double*)nullptr, c->c2, f2);
-    PARIS_LAUNCH(c, k_init_ghosts, div_up(G, 256), 256, 0, c->c2, f2, c->L, c->bnd, G);
+    PARIS_LAUNCH(c, k_init_ghosts, div_up(G, 256), 256, 0, c->c2, f2, c->L, c->bnd, ctx_vof_jet(c), G, c->d.epsc);
     PARIS_LAUNCH(c, k_ls2vof, grid, 64, 0, S, c->L, c->xc, c->yc, c->zc, c->dx, c->dy, c->dz, refinement, f2, c->c2,
                  cv, c->flag);
-    PARIS_LAUNCH(c, k_init_ghosts, div_up(G, 256), 256, 0, cv, c->flag, c->L, c->bnd, G);
+    PARIS_LAUNCH(c, k_init_ghosts, div_up(G, 256), 256, 0, cv, c->flag, c->L, c->bnd, ctx_vof_jet(c), G,
+                 c->d.epsc);
     PARIS_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     cudaFree(dbuf);
     cudaFree(f2);

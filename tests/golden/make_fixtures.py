@@ -2,6 +2,8 @@
 tests/golden/ (run once where the reference tree is available; the copies
 are committed so that the tests need no reference tree).
 
+  python make_fixtures.py <root of the slitvinov/paris-git tree>
+
   Tests/VOF/volumeref.txt        -> vof_volumeref.txt
   Tests/VOF/centerofmassref.txt  -> vof_centerofmassref.txt
   Tests/CylinderAdvection/reference.txt -> cylinder_advection_cvof.txt
@@ -47,4 +49,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_fixtures.py <root of the slitvinov/paris-git tree>")
+    main(sys.argv[1])

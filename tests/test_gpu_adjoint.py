@@ -15,7 +15,8 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 ORACLE_RTOL = 1e-8     # GPU adjoint vs oracle adjoint (both FP64, solves to 1e-12 / 1e-15)
-FD_RTOL = 1e-6         # adjoint vs central differences, eps = 1e-6 (relative for rho)
+FD_RTOL = 1e-6         # adjoint vs central differences, eps = 1e-6 (relative for rho), per entry
+FD_FLOOR = 0.05        # entries checked per entry: |gradient| >= FD_FLOOR * the largest sampled one
 
 
 def faces_of(orc, d):
@@ -151,14 +152,20 @@ def test_adjoint_finite_differences_128(gpu_lib, capi, runtime, orc):
                 res.append(fd_forward(gpu, capi, dt, us, p0))
             fd = loss_diff(w, m, res[0], res[1]) / (2 * eps)
             errs_r.append((fd, gr[q]))
-    rels = {}
+    # per entry: |fd - ad| / |ad| over the entries whose |ad| is at least
+    # FD_FLOOR of the largest sampled one.  The central difference carries an
+    # absolute error (rounding of the forward solves over eps), so entries far
+    # below the largest one are checked against that absolute level instead.
     for name, e in (("u*", np.array(errs_u)), ("rho", np.array(errs_r))):
         fd, ad = e[:, 0], e[:, 1]
-        rels[name] = np.abs(fd - ad).max() / np.abs(ad).max()
-        print(f"adjoint vs FD ({name}, {len(e)} entries): max rel {rels[name]:.3e}, "
-              f"l2 rel {np.linalg.norm(fd - ad) / np.linalg.norm(ad):.3e}")
-    for name, rel in rels.items():
-        assert rel < FD_RTOL, name
+        big = np.abs(ad) >= FD_FLOOR * np.abs(ad).max()
+        rel = np.abs(fd[big] - ad[big]) / np.abs(ad[big])
+        absl = np.abs(fd[~big] - ad[~big]).max(initial=0.0) / np.abs(ad).max()
+        print(f"adjoint vs FD ({name}): {big.sum()} of {len(e)} entries above the floor, per-entry rel max "
+              f"{rel.max():.3e} median {np.median(rel):.3e}; below the floor max |fd-ad|/max|ad| {absl:.3e}")
+        assert big.sum() >= len(e) // 2, name
+        assert rel.max() < FD_RTOL, name
+        assert absl < FD_RTOL * FD_FLOOR, name
     assert np.abs(np.concatenate([a.ravel() for a in u0])).max() > 0
 
 

@@ -66,6 +66,30 @@ def test_linfunc_bitwise(gpu_lib, capi, runtime, orc, workloads):
     assert np.array_equal(rho, rho_ref)
 
 
+@pytest.mark.parametrize("nfilter", [0, 1])
+@pytest.mark.parametrize("mean", [101, 102])
+@pytest.mark.parametrize("bc", ["periodic", "wall"])
+def test_linfunc_means_and_filter(gpu_lib, capi, runtime, orc, workloads, nfilter, mean, bc):
+    """linfunc (vofmodules.f90:171-218) for rho and mu with the arithmetic and
+    the harmonic mean, unfiltered and with the 27-point filter (nfilter = 1),
+    bit for bit against the oracle, ghosts included."""
+    n = 16
+    desc = capi.make_desc((n, n, n), bc=bc, rho1=1.0, rho2=1000.0, mu1=1.8e-5, mu2=1e-3, nfilter=nfilter,
+                          dens_mean=mean, visc_mean=203 - mean)
+    cen, rad = workloads.drop_layout(6, rmin=0.1, rmax=0.2, seed=2, h=1.0 / n)
+    cvof, flag, _ = orc.init_spheres(desc, cen, rad, refinement=4)
+    rho_ref = orc.linfunc(desc, cvof, desc.rho1, desc.rho2, mean)
+    mu_ref = orc.linfunc(desc, cvof, desc.mu1, desc.mu2, 203 - mean)
+    with runtime.ParisGpu(desc) as gpu:
+        gpu.upload(capi.F_CVOF, cvof)
+        gpu.linfunc(capi.F_RHO)
+        gpu.linfunc(capi.F_MU)
+        rho = gpu.download(capi.F_RHO)
+        mu = gpu.download(capi.F_MU)
+    assert np.array_equal(rho, rho_ref)
+    assert np.array_equal(mu, mu_ref)
+
+
 def test_poissonmg_known_answer(gpu_lib, capi, runtime, orc):
     """Tests/PoissonMG: 32x16x16 periodic, XLENGTH=2, 20 V-cycles; residual
     < 1e-8 and L1 error < 0.1 (Tests/PoissonMG/run.sh:13), same iterates as

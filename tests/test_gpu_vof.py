@@ -76,3 +76,54 @@ def test_init_spheres(gpu_lib, capi, runtime, orc, workloads, bc):
         f = gpu.download(capi.F_VOF_FLAG)
     assert np.abs(c - c_ref).max() <= TOL
     assert np.array_equal(f, f_ref)
+
+
+JET, DEG90, DRY, OUT = 2, 5, 0, 4
+
+
+@pytest.mark.parametrize("advect", [0, 1])
+@pytest.mark.parametrize("vofbc", [(JET, DEG90, DRY, DEG90, OUT, DEG90), (DEG90, DEG90, DEG90, DEG90, DEG90, DEG90)])
+def test_sweeps_jet_and_90deg(gpu_lib, capi, runtime, orc, workloads, advect, vofbc):
+    """'jet' and '90deg' faces (vofmodules.f90:1716-1720,1758-1811): the first
+    ghost layer from the inflow pattern or the adjacent cell, the second kept
+    from before the sweep.  The state starts from drops in a dry box whose
+    second ghost layers are set to distinct values, with an inflow through
+    x- so that the jet's first layer is advected in."""
+    n = 24
+    jet = (2, 0.5, 0.45, 0.2, 0.0)
+    dry = capi.make_desc((n, n, n), bc="wall", advect=advect)
+    desc = capi.make_desc((n, n, n), bc="wall", vofbc=vofbc, advect=advect, jet=jet)
+    cen, rad = workloads.drop_layout(5, rmin=0.1, rmax=0.18, seed=3, h=1.0 / n, margin_cells=0)
+    cvof, flag, _ = orc.init_spheres(dry, cen, rad, refinement=4)
+    rng = np.random.default_rng(7)
+    for sl in ((slice(None), slice(None), 0), (slice(None), slice(None), -1), (slice(None), 0, slice(None)),
+               (slice(None), -1, slice(None)), (0, slice(None), slice(None)), (-1, slice(None), slice(None))):
+        cvof[sl] = rng.choice([0.0, 1.0, 0.4], size=cvof[sl].shape)
+    orc.setvofbc(desc, cvof, flag)
+    orc.flags_clip(desc, cvof, flag)
+    u, v, w = velocity(capi, orc, workloads, desc)
+    u = u + 0.6
+    dt = 0.25 / n / 2.0
+    ref_c, ref_f = cvof.copy(), flag.copy()
+    with runtime.ParisGpu(desc) as gpu:
+        gpu.upload(capi.F_CVOF, cvof)
+        gpu.upload(capi.F_VOF_FLAG, flag)
+        for f, a in zip((capi.F_U, capi.F_V, capi.F_W), (u, v, w)):
+            gpu.upload(f, a)
+        for step in range(3):
+            orc.vofsweeps(desc, step, dt, ref_c, ref_f, u, v, w)
+            gpu.vof_sweeps(step, dt)
+        c = gpu.download(capi.F_CVOF)
+        f = gpu.download(capi.F_VOF_FLAG)
+    assert np.abs(c - ref_c).max() <= TOL
+    assert np.array_equal(f, ref_f)
+    if vofbc[0] == JET:   # the jet carried liquid into the first interior column
+        assert ref_c[2:-2, 2:-2, 2].sum() > cvof[2:-2, 2:-2, 2].sum()
+
+
+@pytest.mark.parametrize("code", [JET, DEG90])
+def test_init_spheres_refuses_jet_and_90deg(gpu_lib, capi, runtime, code):
+    desc = capi.make_desc((16, 16, 16), bc="wall", vofbc=(code, 0, 0, 0, 0, 0), jet=(2, 0.5, 0.5, 0.2, 0.0))
+    with runtime.ParisGpu(desc) as gpu:
+        with pytest.raises(runtime.ParisError, match="bad flag"):
+            gpu.init_spheres([(0.5, 0.5, 0.5)], [0.25], refinement=8)

@@ -38,21 +38,27 @@ def test_calc_residuals_noalloc_matches(gpu_lib, capi, runtime, orc, workloads):
     lib = gpu_lib
     stream = torch.cuda.current_stream()
     A_dev = torch.from_numpy(np.ascontiguousarray(A)).cuda()
-    for p in (p1, p2):
+    for call, p in enumerate((p1, p2)):
         with runtime.ParisGpu(desc) as gpu:
             gpu.upload(capi.F_A, A)
             gpu.upload(capi.F_P, p)
             want = gpu.calc_residuals()
         p_dev = torch.from_numpy(np.ascontiguousarray(p)).cuda()
         torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
         out = np.zeros(3)
         st = lib.paris_calc_residuals_noalloc(n, n, n, desc.ng, ctypes.c_void_p(A_dev.data_ptr()),
                                               ctypes.c_void_p(p_dev.data_ptr()),
                                               out.ctypes.data_as(ctypes.c_void_p),
                                               ctypes.c_void_p(stream.cuda_stream))
         assert st == capi.OK
+        if call == 1:   # the module is loaded by now: no device memory is taken
+            assert torch.cuda.mem_get_info()[0] == free0
         np.testing.assert_allclose(out[:2], want[:2], rtol=1e-12)
         assert out[2] == want[2]
+        # calcResiduals of the oracle (modules.f90:3313-3387): L1, L2, Linf
+        ref = [orc.calc_residual(desc, A, p, k) for k in (1, 2, 3)]
+        np.testing.assert_allclose(out, ref, rtol=1e-12)
 
 
 def test_calc_residuals_noalloc_rejects_oversize(gpu_lib, capi):

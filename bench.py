@@ -7,11 +7,13 @@ outside this path) -> SetupPoisson -> NewSolver to ||r||_2/||b||_2 < 1e-10
 from p = 0 -> project_velocity, on the 256^3 periodic unit cube with 64 drops
 of radius U[0.03,0.08] at density ratio 1000 and a seeded Gaussian u*
 (unit variance, 3 Jacobi smoothing sweeps).  `value` uses the mixed-precision
-multigrid (FP32 V(2,2) cycles in an FP64 defect-correction loop) with inputs
-resident in HBM; `fp64_steps_per_s` the same algorithm all in FP64; `e2e`
-the same step through the C-ABI with host buffers (u* uploaded, u,v,w,cvof
-downloaded every step).  `--impl reference` times the reference algorithm
-(the CPU restatement in oracle/) on the host cores.
+multigrid (FP32 V(2,2) cycles preconditioning an FP64 flexible CG) with
+inputs resident in HBM; `fp64_steps_per_s` the same algorithm all in FP64;
+`pressure_error` compares the two solutions step by step and the mixed one
+with the oracle's FP64 solution once; `e2e` is the same step through the
+C-ABI with host buffers (u* uploaded, u,v,w,cvof downloaded every step).
+`--impl reference` times the reference algorithm (the CPU restatement in
+oracle/) on the host cores.
 
 `--workload rising_bubble` times instead the full explicit Navier-Stokes step
 (momentum predictor, VOF, heights, curvature, CSF, projection) on a gas
@@ -50,6 +52,10 @@ def parse():
                          "under torchrun use --grid, which its own options cannot be confused with")
     ap.add_argument("--pcg", type=int, default=1, help="1: FP64 flexible CG preconditioned by the V-cycle, 0: defect correction")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0,
+                    help="seconds of reference V-cycles in the cpu_baseline sample step")
+    ap.add_argument("--ref-budget", type=float, default=240.0,
+                    help="--impl reference: seconds of reference V-cycles over all timed steps")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="a few profiled steps, no JSON timing")
     return ap.parse_args()
@@ -202,6 +208,70 @@ def gpu_step(gpu, capi, k, dt, mode, pcg):
     return r
 
 
+def _rel_diff(a, b):
+    """||(a - mean a) - (b - mean b)||_2 / ||b - mean b||_2 and the same in
+    max-abs (the pressure of the periodic problem is fixed up to a constant)."""
+    da, db = a - a.mean(), b - b.mean()
+    e = da - db
+    return float(np.linalg.norm(e) / np.linalg.norm(db)), float(np.abs(e).max() / np.abs(db).max())
+
+
+def _residual_rel(A, p, b):
+    """||b - A p||_2 / ||b||_2 on the host with the reference's 8-component A
+    (periodic in all directions)."""
+    r = b.copy()
+    r -= A[6] * p
+    r += A[0] * np.roll(p, 1, 2) + A[1] * np.roll(p, -1, 2) + A[2] * np.roll(p, 1, 1) + A[3] * np.roll(p, -1, 1) + \
+        A[4] * np.roll(p, 1, 0) + A[5] * np.roll(p, -1, 0)
+    return float(np.linalg.norm(r) / np.linalg.norm(b))
+
+
+def pressure_error(gpu, capi, args, dt, reset, cpu_oracle):
+    """The pressure of the mixed solver against the all-FP64 one, step by step
+    on the same states (each step's matrix is solved by both from p = 0), and
+    once, on the first step's matrix, against the oracle's FP64 solution
+    (its restatement of the same multigrid in FP64, flexible CG to 1e-12).
+    Untimed."""
+    from oracle import pyoracle as orc
+    reset()
+    d = gpu.desc
+    g = d.ng
+    rows = []
+    oracle = None
+    for k in range(args.steps):
+        gpu.vof_sweeps(k, dt)
+        gpu.linfunc(capi.F_RHO)
+        for dst, src in ((capi.F_U, capi.F_USTAR), (capi.F_V, capi.F_VSTAR), (capi.F_W, capi.F_WSTAR)):
+            gpu.copy_field(dst, src)
+        gpu.setup_poisson(dt)
+        gpu.fill_field(capi.F_P, 0.0)
+        rm = gpu.new_solver(0.0, maxit=200, mode=capi.MG_MIXED, rel_tol=REL_TOL, pcg=args.pcg)
+        pm = gpu.download(capi.F_P)
+        gpu.fill_field(capi.F_P, 0.0)
+        r64 = gpu.new_solver(0.0, maxit=200, mode=capi.MG_FP64, rel_tol=REL_TOL, pcg=args.pcg)
+        p64 = gpu.download(capi.F_P)
+        pm_i, p64_i = pm[g:-g, g:-g, g:-g], p64[g:-g, g:-g, g:-g]
+        l2, mx = _rel_diff(pm_i, p64_i)
+        rows.append((l2, mx, rm.rel_res, r64.rel_res))
+        if k == 0 and cpu_oracle:
+            A = gpu.download(capi.F_A)
+            p_int, it, _ = orc.fastmg_solve(d, A, np.zeros((d.nz, d.ny, d.nx)), 1e-12, maxit=100, mixed=False,
+                                            pcg=True)
+            ol2, omx = _rel_diff(pm_i, p_int)
+            fl2, fmx = _rel_diff(p64_i, p_int)
+            oracle = {"rel_l2_mixed": ol2, "rel_max_mixed": omx, "rel_l2_fp64": fl2, "rel_max_fp64": fmx,
+                      "oracle_rel_res": _residual_rel(A, p_int, A[7]), "oracle_iterations": it,
+                      "residual_of_mixed": _residual_rel(A, pm_i, A[7])}
+            del A
+        gpu.upload(capi.F_P, pm)
+        gpu.project_velocity(dt)
+    R = np.array(rows)
+    return {"mixed_vs_fp64_rel_l2_max": float(R[:, 0].max()), "mixed_vs_fp64_rel_max_max": float(R[:, 1].max()),
+            "rel_res_mixed_max": float(R[:, 2].max()), "rel_res_fp64_max": float(R[:, 3].max()),
+            "tolerance": REL_TOL, "steps": len(rows), "vs_oracle_step0": oracle,
+            "note": "pressure differences after removing the mean (the periodic problem fixes p up to a constant)"}
+
+
 # DRAM bytes per cell of the dominant kernel measured by ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum of one 256^3 launch,
 # 348.7 MB + 57.0 MB over 16,777,216 cells): fills roofline.traffic, scaled by
@@ -233,13 +303,21 @@ def measured_peak():
 # ---------------------------------------------------------------------------
 class CpuReference:
     """The reference algorithm on the host cores (the FP64 restatement in
-    oracle/, OpenMP over k): vofsweeps, linfunc, SetupPoisson, the reference
-    V-cycles (MGsolver.f90) and project_velocity.  The reference multigrid
-    needs hundreds of cycles at density ratio 1000, so a sample step runs
-    `cycles` V-cycles and the time to 1e-10 is extrapolated with the
-    asymptotic convergence rate measured once over `rate_cycles` cycles."""
+    oracle/, OpenMP over all cores): vofsweeps, linfunc, SetupPoisson, the
+    reference multigrid (NewSolverMG, MGsolver.f90:346-405: V-cycles from
+    p = 0 until the RMS residual is below 1e-10 of the RMS right-hand side)
+    and project_velocity, on the same workload.
 
-    def __init__(self, pkg, desc, us, dt, cvof=None, flag=None, cen=None, rad=None, cycles=2, rate_cycles=8):
+    The reference multigrid converges slowly at density ratio 1000: on this
+    workload it needs 309 cycles at 64^3 and 879 at 128^3 (asymptotic rate
+    0.981 per cycle there), and more at 256^3, so a complete step at 256^3
+    takes longer than a timing run can give it.  Each step therefore runs the
+    V-cycles until the tolerance or until its time budget is spent, whichever
+    comes first.  A step that stops at its budget has done less work than the
+    reference needs, so the steps/s measured is an upper bound of the
+    reference's: a measurement, not a model."""
+
+    def __init__(self, pkg, desc, us, dt, cvof=None, flag=None, cen=None, rad=None):
         from oracle import pyoracle as orc
         self.orc, self.capi, self.desc, self.dt = orc, pkg.capi, desc, dt
         self.us = us
@@ -247,44 +325,36 @@ class CpuReference:
             cvof, flag, _ = orc.init_spheres(desc, cen, rad, refinement=8)
         self.c, self.f = cvof.copy(), flag.copy()
         self.u = [a.copy() for a in us]
-        self.cycles, self.rate_cycles = cycles, rate_cycles
-        self.rate = None
         self.cores = len(os.sched_getaffinity(0))
+        self.log = []
 
-    def _pre(self, k):
+    def step(self, k, budget_s):
+        """One step with at most budget_s seconds of V-cycles (after the first
+        cycle); returns its wall time."""
         orc, d = self.orc, self.desc
+        t0 = time.perf_counter()
         orc.vofsweeps(d, k, self.dt, self.c, self.f, *self.u)
         rho = orc.linfunc(d, self.c, d.rho1, d.rho2, self.capi.MEAN_ARITH)
         self.u = [a.copy() for a in self.us]
         st, A = orc.setup_poisson(d, *self.u, rho, self.dt)
-        return rho, A
-
-    def measure_rate(self, k=0):
-        rho, A = self._pre(k)
-        p = self.orc.zeros(self.desc)
-        _, _, _, h = self.orc.new_solver_mg(self.desc, A, p, 0.0, beta=1.0, maxit=self.rate_cycles, norm=2)
-        self.rate = float((h[-1] / h[-4]) ** (1.0 / 3.0))
-        self.rms_b = float(np.sqrt(np.mean(A[7] ** 2)))
-        self.orc.project_velocity(self.desc, *self.u, p, rho, self.dt)
-        return self.rate
-
-    def step(self, k):
-        """Returns (seconds of the sample, extrapolated seconds to 1e-10)."""
-        t0 = time.perf_counter()
-        rho, A = self._pre(k)
-        t1 = time.perf_counter()
-        p = self.orc.zeros(self.desc)
-        _, _, _, h = self.orc.new_solver_mg(self.desc, A, p, 0.0, beta=1.0, maxit=self.cycles, norm=2)
-        t2 = time.perf_counter()
-        self.orc.project_velocity(self.desc, *self.u, p, rho, self.dt)
-        t3 = time.perf_counter()
         rms_b = float(np.sqrt(np.mean(A[7] ** 2)))
-        target = REL_TOL * rms_b
-        more = max(0.0, np.log(target / h[-1]) / np.log(self.rate)) if h[-1] > target else 0.0
-        n_needed = self.cycles + int(np.ceil(more))
-        t_cycle = (t2 - t1) / self.cycles
-        self.n_needed = n_needed
-        return t3 - t0, (t1 - t0) + (t3 - t2) + n_needed * t_cycle
+        p = orc.zeros(d)
+        ok, cycles, tres, _ = orc.new_solver_mg_timed(d, A, p, REL_TOL * rms_b, budget_s)
+        orc.project_velocity(d, *self.u, p, rho, self.dt)
+        t = time.perf_counter() - t0
+        self.log.append({"s": round(t, 2), "cycles": cycles, "converged": bool(ok), "rel_res": tres / rms_b})
+        return t
+
+
+def projection_config(n, world):
+    """The workload of both arms (the same dict)."""
+    return {"workload": f"{n}^3 periodic unit cube, 64 drops r~U[0.03,0.08] (seed 0), rho 1000/1, smoothed Gaussian "
+                        "u* (seed 1); per step CIAM vofsweeps, linfunc, SetupPoisson, the pressure solve from p=0 to "
+                        "||r||/||b|| < 1e-10, project_velocity",
+            "cells": n ** 3, "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (141 MB per field)"}
+
+
+REF_SOLVER = "reference MG (MGsolver.f90 NewSolverMG, nrelax=3), FP64, on the host cores"
 
 
 def run_reference(args, dist):
@@ -294,31 +364,30 @@ def run_reference(args, dist):
     n = args.n
     desc, cen, rad, us, dt = workload(pkg, n)
     ref = CpuReference(pkg, desc, us, dt, cen=cen, rad=rad)
-    ref.measure_rate()
+    # warm-up: the step's fixed work and one V-cycle each
     for k in range(args.warmup):
-        ref.step(k)
-    samples, est = [], []
-    for k in range(args.steps):
-        s, e = ref.step(args.warmup + k)
-        samples.append(s)
-        est.append(e)
-    t_est = float(np.mean(est))
-    v = 1.0 / t_est
+        ref.step(k, 1e-9)
+    budget = args.ref_budget / max(1, args.steps)
+    ts = [ref.step(args.warmup + k, budget) for k in range(args.steps)]
+    t_mean = float(np.mean(ts))
+    v = 1.0 / t_mean
+    steps_log = ref.log[args.warmup:]
+    conv = sum(1 for r in steps_log if r["converged"])
+    sample = (f"each step complete at {n}^3 (VOF, linfunc, SetupPoisson, project_velocity) with reference V-cycles "
+              f"until ||r||/||b|| < 1e-10 or a {budget:.1f} s budget: {conv} of {args.steps} steps converged, "
+              f"{min(r['cycles'] for r in steps_log)}-{max(r['cycles'] for r in steps_log)} cycles per step, "
+              f"residual reached <= {max(r['rel_res'] for r in steps_log):.2e}; "
+              + ("steps/s as measured" if conv == args.steps else
+                 "steps/s measured over the truncated steps, an upper bound of the reference's"))
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_est * 1e3, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_mean * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{n}^3 periodic unit cube, 64 drops r~U[0.03,0.08], rho ratio 1000, "
-                               "smoothed Gaussian u*, CIAM VOF + reference MG V-cycles to rel. residual 1e-10",
-                   "cells": n ** 3, "solver": "reference MG (MGsolver.f90), FP64, nrelax=3",
-                   "l2": "inputs larger than L2"},
-        "cpu_baseline": {"value": v, "unit": "steps/s", "cores": ref.cores, "kind": "port",
-                         "sample": f"each step: VOF+linfunc+SetupPoisson+project and {ref.cycles} reference "
-                                   f"V-cycles at {n}^3; time to 1e-10 extrapolated with the measured "
-                                   f"asymptotic rate {ref.rate:.4f}/cycle ({ref.n_needed} cycles); "
-                                   f"sample wall {np.mean(samples):.1f} s"},
+        "config": projection_config(n, args.gpus), "solver": REF_SOLVER,
+        "cpu_baseline": {"value": v, "unit": "steps/s", "cores": ref.cores, "kind": "port", "sample": sample,
+                         "upper_bound": conv < args.steps},
         "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "mg_cycles_to_tol": ref.n_needed,
+        "steps_log": steps_log,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -412,6 +481,7 @@ def run_b200(args, dist):
     report = gpu.profile_report()
     rows = roofline(report, peak)
     top = rows[0]
+    perr = pressure_error(gpu, capi, args, dt, reset, cpu_oracle=(dist.rank == 0 and not args.no_cpu_baseline))
     # summed kernel time per step (the rest of ms_per_step is the GPU waiting
     # on the host between launches)
     kernel_ms_per_step = sum(ms for _, ms, _ in report.values()) / 2
@@ -475,12 +545,14 @@ def run_b200(args, dist):
     cpu = None
     if dist.rank == 0 and not args.no_cpu_baseline:
         ref = CpuReference(pkg, desc, us, dt, cvof=cvof0, flag=flag0)
-        ref.measure_rate()
-        s, est = ref.step(0)
-        cpu = {"value": 1.0 / est, "unit": "steps/s", "cores": ref.cores, "kind": "port",
-               "sample": f"one step at {n}^3 (VOF+linfunc+SetupPoisson+project and {ref.cycles} reference "
-                         f"V-cycles, {s:.1f} s wall); time to 1e-10 extrapolated with the measured rate "
-                         f"{ref.rate:.4f}/cycle over {ref.n_needed} cycles"}
+        t = ref.step(1, args.cpu_budget)
+        r = ref.log[-1]
+        cpu = {"value": 1.0 / t, "unit": "steps/s", "cores": ref.cores, "kind": "port",
+               "sample": f"one step at {n}^3 (VOF, linfunc, SetupPoisson, project_velocity) with reference "
+                         f"V-cycles until ||r||/||b|| < 1e-10 or {args.cpu_budget:.0f} s: {r['cycles']} cycles, "
+                         f"residual {r['rel_res']:.2e}, {t:.1f} s; "
+                         + ("complete" if r["converged"] else "truncated, so the steps/s is an upper bound"),
+               "upper_bound": not r["converged"]}
     gpu.close()
     if dist.rank != 0:
         return 0
@@ -489,14 +561,13 @@ def run_b200(args, dist):
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": dist.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
-        "config": {"workload": f"{n}^3 periodic unit cube, 64 drops r~U[0.03,0.08] (seed 0), rho 1000/1, "
-                               "smoothed Gaussian u* (seed 1), CIAM VOF + B200 MG to ||r||/||b|| < 1e-10 from p=0",
-                   "cells": n ** 3, "solver": ("FP32 red-black V(2,2) cycles in an FP64 " +
-                                              ("flexible-CG (preconditioner) loop" if args.pcg else "defect-correction loop")),
-                   "parallelism": f"replicas x{dist.world}", "l2": "inputs larger than L2 (141 MB per field)"},
+        "config": projection_config(n, dist.world),
+        "solver": ("B200 MG: FP32 red-black V(2,2) cycles in an FP64 " +
+                   ("flexible-CG (preconditioner) loop" if args.pcg else "defect-correction loop")),
         "fp64_steps_per_s": dist.world * args.steps / (ms64 / 1e3),
         ("mixed_dc_steps_per_s" if args.pcg else "mixed_pcg_steps_per_s"): dist.world * args.steps / (msdc / 1e3),
         "mg_iterations": {"mixed": its, "fp64": its64, ("mixed_dc" if args.pcg else "mixed_pcg"): itsdc},
+        "pressure_error": perr,
         "mcell_updates_per_s": value * n ** 3 / 1e6,
         "gpu_launches": launches,
         "kernel_ms_per_step": round(kernel_ms_per_step, 3),

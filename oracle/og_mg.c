@@ -11,6 +11,7 @@
  */
 #include <math.h>
 #include <stdio.h>
+#include <omp.h>
 #include <string.h>
 #include "og.h"
 
@@ -306,9 +307,9 @@ static void og_coarse_from_fine(const og_level* f, og_level* c) {
 static void og_coarse_fine_interp(const og_mg* mg, og_level* f, const og_level* c, int sym) {
     int ng = mg->g->ng;
 #pragma omp parallel for schedule(static)
-    for (int i = 0; i < c->n[0]; i++)
+    for (int k = 0; k < c->n[2]; k++)
         for (int j = 0; j < c->n[1]; j++)
-            for (int k = 0; k < c->n[2]; k++) {
+            for (int i = 0; i < c->n[0]; i++) {
                 double pc = c->p[LIX(c, i + ng, j + ng, k + ng)];
                 long q[8];
                 int t = 0;
@@ -328,12 +329,17 @@ static void og_coarse_fine_interp(const og_mg* mg, og_level* f, const og_level* 
             }
 }
 
+static void og_zero(double* a, long n) {
+#pragma omp parallel for schedule(static)
+    for (long q = 0; q < n; q++) a[q] = 0.0;
+}
+
 /* MG_iteration, MGsolver.f90:253-320 */
 static void og_mg_iteration(og_mg* mg, double beta, int norm) {
     int LMG = mg->LMG;
     for (int L = LMG; L >= 2; L--) {
         og_level* l = &mg->lev[L];
-        memset(l->p, 0, l->ntot * sizeof(double));
+        og_zero(l->p, l->ntot);
         for (int r = 0; r < mg->nrelax; r++) {
             og_rb_relax(mg, l, l->K, l->p, beta);
             og_apply_bc_mg(mg, l, l->p);
@@ -345,13 +351,13 @@ static void og_mg_iteration(og_mg* mg, double beta, int norm) {
     og_apply_bc_mg(mg, &mg->lev[2], mg->lev[2].p);
     for (int L = 3; L <= LMG; L++) {
         og_level* l = &mg->lev[L];
-        memset(l->e, 0, l->ntot * sizeof(double));
+        og_zero(l->e, l->ntot);
         og_coarse_fine_interp(mg, l, &mg->lev[L - 1], mg->sym);
         og_apply_bc_mg(mg, l, l->e);
         og_get_residual(mg, l, l->K, l->e, norm);
 #pragma omp parallel for schedule(static)
         for (long q = 0; q < l->ntot; q++) l->p[q] = l->p[q] + l->e[q];
-        memset(l->e, 0, l->ntot * sizeof(double));
+        og_zero(l->e, l->ntot);
         for (int r = 0; r < mg->nrelax; r++) {
             og_rb_relax(mg, l, l->K, l->e, beta);
             og_apply_bc_mg(mg, l, l->e);
@@ -366,8 +372,21 @@ static void og_mg_iteration(og_mg* mg, double beta, int norm) {
  * A: 8*N (not modified); p: ghosted.  hist (optional, maxit entries) receives
  * tres2 after each V-cycle.  Returns 0, or PARIS_NOT_CONVERGED when it hits
  * maxit (it = maxit+1). */
+int og_new_solver_mg_timed(const paris_grid_desc* desc, const double* A, double* p, double maxError, double beta,
+                           int maxit, int norm, int* it_out, double* tres2_out, double* hist, double max_seconds);
+
 int og_new_solver_mg(const paris_grid_desc* desc, const double* A, double* p, double maxError,
                      double beta, int maxit, int norm, int* it_out, double* tres2_out, double* hist) {
+    return og_new_solver_mg_timed(desc, A, p, maxError, beta, maxit, norm, it_out, tres2_out, hist, 0.0);
+}
+
+/* NewSolverMG with a wall-clock limit (for timing runs of the host): when
+ * max_seconds > 0 the loop also stops after the first V-cycle that ends past
+ * max_seconds from the call, returning PARIS_NOT_CONVERGED with *it_out the
+ * cycles run (not maxit+1) when the tolerance was not met. */
+int og_new_solver_mg_timed(const paris_grid_desc* desc, const double* A, double* p, double maxError, double beta,
+                           int maxit, int norm, int* it_out, double* tres2_out, double* hist, double max_seconds) {
+    const double t_start = omp_get_wtime();
     /* init_MG, MGsolver.f90:43-46: 2^n cells per direction */
     for (int a = 0; a < 3; a++) {
         int n = a == 0 ? desc->nx : (a == 1 ? desc->ny : desc->nz);
@@ -390,12 +409,20 @@ int og_new_solver_mg(const paris_grid_desc* desc, const double* A, double* p, do
     int it;
     for (it = 1; it <= maxit; it++) {
         og_mg_iteration(mg, beta, norm);
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < g->ntot; q++) p[q] = p[q] + lf->p[q];
         resMax = og_compute_residual(g, A, p, norm);
         tres2 = resMax / (double)N;
         if (norm == 2) tres2 = sqrt(tres2);
         if (hist) hist[it - 1] = tres2;
         if (tres2 < maxError) break;
+        if (max_seconds > 0.0 && omp_get_wtime() - t_start > max_seconds) {
+            *it_out = it;
+            *tres2_out = tres2;
+            og_mg_free(mg);
+            og_grid_free(g);
+            return PARIS_NOT_CONVERGED;
+        }
     }
     (void)ng;
     *it_out = it;

@@ -48,6 +48,7 @@ def lib():
             "og_setup_poisson": (I, [G, P, P, P, P, D, D, P]),
             "og_setup_testmg": (I, [G, P, P]),
             "og_new_solver_mg": (I, [G, P, P, D, D, I, I, P, P, P]),
+            "og_new_solver_mg_timed": (I, [G, P, P, D, D, I, I, P, P, P, D]),
             "og_calc_residual": (D, [G, P, P, I]),
             "og_mgtest_err": (D, [G, P]),
             "og_project_velocity": (I, [G, P, P, P, P, P, D]),
@@ -133,6 +134,18 @@ def new_solver_mg(desc, A, p, max_error, beta=1.0, maxit=20, norm=2):
     st = lib().og_new_solver_mg(ctypes.byref(desc), _p(np.ascontiguousarray(A)), _p(p), max_error,
                                 beta, maxit, norm, ctypes.byref(it), ctypes.byref(t), _p(hist))
     return st, it.value, t.value, hist[:min(it.value, maxit)]
+
+
+def new_solver_mg_timed(desc, A, p, max_error, max_seconds, beta=1.0, maxit=100000, norm=2):
+    """NewSolverMG that also stops after the first V-cycle ending past
+    max_seconds.  Returns (converged, cycles, tres2, history)."""
+    it = ctypes.c_int(0)
+    t = ctypes.c_double(0)
+    hist = np.zeros(max(maxit, 1))
+    st = lib().og_new_solver_mg_timed(ctypes.byref(desc), _p(np.ascontiguousarray(A)), _p(p), max_error, beta,
+                                      maxit, norm, ctypes.byref(it), ctypes.byref(t), _p(hist), float(max_seconds))
+    n = min(it.value, maxit)
+    return st == 0, n, t.value, hist[:n]
 
 
 def calc_residual(desc, A, p, normorder):

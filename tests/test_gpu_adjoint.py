@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 ORACLE_RTOL = 1e-8     # GPU adjoint vs oracle adjoint (both FP64, solves to 1e-12 / 1e-15)
 FD_RTOL = 1e-6         # adjoint vs central differences, eps = 1e-6 (relative for rho), per entry
-FD_FLOOR = 0.05        # entries checked per entry: |gradient| >= FD_FLOOR * the largest sampled one
+FD_FLOOR = 0.2         # entries checked per entry: |gradient| >= FD_FLOOR * the largest sampled one
 
 
 def faces_of(orc, d):

@@ -20,7 +20,10 @@ rounding only.
 The device and the oracle run free, each from its own previous step; the
 test records per step max |dcvof| and the RMS of dcvof, the first step at
 which max |dcvof| passes 1e-12, and the liquid volume sum(c) h^3 against
-step 0 on both sides."""
+step 0 on both sides.  Measured on a B200: Weymouth-Yue stays within
+2.5e-14 of the oracle for all 768 steps and holds the volume to 4.8e-14;
+CIAM stays within 1e-12 until step 715 (6.3e-13 at the end) and its volume
+grows by 4.08e-2, identically on both sides."""
 import numpy as np
 import pytest
 
@@ -77,11 +80,23 @@ def test_deformation_32_against_oracle(gpu_lib, capi, runtime, orc, workloads, a
     step, dmax, drms, vgpu, vref, itg, itr = R.T
     over = np.nonzero(dmax > 1e-12)[0]
     first = int(step[over[0]]) if len(over) else None
-    print(f"\n{name}: first step with max|dcvof| > 1e-12: {first}")
+    print(f"\n{name}: first step with max|dcvof| > 1e-12: {first}; largest max|dcvof| {dmax.max():.2e} "
+          f"(step {int(step[np.argmax(dmax)])}); largest |volume drift| {np.abs(vgpu).max():.2e}")
     for s in (1, 10, 100, 200, 384, 500, 600, 700, 768):
         q = s - 1
         print(f"  step {s:4d}: max|dcvof| {dmax[q]:.2e}  rms {drms[q]:.2e}  volume drift device {vgpu[q]:+.3e} "
               f"oracle {vref[q]:+.3e}  V-cycles {int(itg[q])}/{int(itr[q])}")
     assert np.array_equal(itg, itr)
-    assert np.abs(vgpu - vref).max() <= 1e-9
-    assert dmax[:100].max() <= 1e-12
+    if advect == 1:
+        # Weymouth-Yue: within 1e-12 of the oracle over all 768 steps (2.5e-14
+        # measured), the liquid volume held to 1e-13 on both sides (-4.8e-14)
+        assert first is None
+        assert np.abs(vgpu).max() <= 1e-13 and np.abs(vref).max() <= 1e-13
+    else:
+        # CIAM: within 1e-12 to step 714 (715 measured), 6.3e-13 at step 768;
+        # the Lagrangian-explicit sweeps are not conservative under this
+        # deformation: the volume grows by 4.08e-2 on both sides alike
+        assert first is None or first >= 700
+        assert dmax.max() <= 1e-11
+        assert np.abs(vgpu - vref).max() <= 1e-11
+        assert 0.03 < vgpu[-1] < 0.05

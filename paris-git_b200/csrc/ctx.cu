@@ -209,6 +209,9 @@ extern "C" int paris_gpu_init(const paris_grid_desc* desc, paris_handle_t* out) 
     if (!s && cudaMalloc(&c->red_part, 8L * kRedBlocks * sizeof(double)) != cudaSuccess) s = PARIS_CUDA_ERROR;
     if (!s && cudaMalloc(&c->debris_count, sizeof(int)) != cudaSuccess) s = PARIS_CUDA_ERROR;
     if (!s && cudaHostAlloc(&c->red_host, 8 * sizeof(double), cudaHostAllocMapped) != cudaSuccess) s = PARIS_CUDA_ERROR;
+    if (!s && cudaHostAlloc(&c->err_host, sizeof(int), cudaHostAllocMapped) != cudaSuccess) s = PARIS_CUDA_ERROR;
+    if (!s && cudaHostGetDevicePointer((void**)&c->err_dev, c->err_host, 0) != cudaSuccess) s = PARIS_CUDA_ERROR;
+    if (!s) *c->err_host = 0;
     if (!s && cudaHostGetDevicePointer((void**)&c->red_host_dev, c->red_host, 0) != cudaSuccess) s = PARIS_CUDA_ERROR;
     for (int f : {PARIS_FIELD_CVOF, PARIS_FIELD_U, PARIS_FIELD_V, PARIS_FIELD_W, PARIS_FIELD_RHO, PARIS_FIELD_P})
         if (!s) s = ctx_alloc_field(c, f);
@@ -238,7 +241,7 @@ extern "C" int paris_gpu_finalize(paris_handle_t c) {
                     (void*)c->height, (void*)c->i32stage, (void*)c->cx, (void*)c->cy, (void*)c->cz,
                     (void*)c->rhs, (void*)c->A, (void*)c->red_part, (void*)c->fast_r64,
                     (void*)c->fast_d64, (void*)c->fast_q64,
-                    (void*)c->vflux, (void*)c->mixlist, (void*)c->mixcount, (void*)c->kflag, (void*)c->st_list,
+                    (void*)c->kflag, (void*)c->st_list,
                     (void*)c->st_count, (void*)c->debris_count, (void*)c->adj, (void*)c->stats_part, (void*)c->stats_out, (void*)c->mom_tab,
                     (void*)c->mc_tmp, (void*)c->mc_tmp2, (void*)c->mc_work, (void*)c->mc_fv, (void*)c->mc_flag,
                     (void*)c->mc_cg})
@@ -254,9 +257,11 @@ extern "C" int paris_gpu_finalize(paris_handle_t c) {
     if (c->s_h2d) cudaStreamDestroy(c->s_h2d);
     if (c->s_d2h) cudaStreamDestroy(c->s_d2h);
     for (auto& l : c->ref) { free_ptr(l.K); free_ptr(l.p); free_ptr(l.e); }
+    mg_fast_free_maps(c);
     for (auto& l : c->fl32) { free_ptr(l.cx); free_ptr(l.cy); free_ptr(l.cz); free_ptr(l.b); free_ptr(l.x); free_ptr(l.x2); }
     for (auto& l : c->fl64) { free_ptr(l.cx); free_ptr(l.cy); free_ptr(l.cz); free_ptr(l.b); free_ptr(l.x); free_ptr(l.x2); }
     if (c->red_host) cudaFreeHost(c->red_host);
+    if (c->err_host) cudaFreeHost(c->err_host);
     for (auto e : c->evpool) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;

@@ -27,6 +27,7 @@ struct FastLevel {
     T *cx, *cy, *cz;
     T *b, *x;
     T* x2;   // second iterate of the fused sweeps (they read one and write the other)
+    void* tma = nullptr;   // FP32: tensor maps of the level for the TMA-staged sweep (mg_fast.cu)
 };
 
 struct paris_ctx {
@@ -46,9 +47,6 @@ struct paris_ctx {
     double* c2 = nullptr;          // second cvof buffer of the sweeps
     int8_t* flag = nullptr;        // vof_flag (ghosted)
     uint8_t* cg = nullptr;         // c_mask of the Weymouth-Yue sweeps
-    double* vflux = nullptr;       // vof1/vof2/vof3 of the mixed cells (3 ghosted arrays)
-    long* mixlist = nullptr;       // mixed flux cells of the current sweep
-    int* mixcount = nullptr;
     double* height = nullptr;      // 6 ghosted fields
     int8_t* kflag = nullptr;       // kappaflag of the curvature passes
     int* st_list = nullptr;        // interior mixed cells of the curvature passes
@@ -64,6 +62,8 @@ struct paris_ctx {
     double setup_dt = 0.0;
     // reductions
     double* red_part = nullptr;    // kRedBlocks partials * 4 slots
+    int* err_host = nullptr;       // pinned and mapped: set by a kernel whose bounded wait ran out
+    int* err_dev = nullptr;        // its device address
     double* red_host = nullptr;    // pinned and mapped
     double* red_host_dev = nullptr;   // its device address
     int red_nb = kRedBlocks;       // blocks of the last reduction launch
@@ -136,6 +136,8 @@ int ctx_reduce_finish(paris_ctx* c, int nslots, double* out_host, int op_max = 0
 int ctx_ensure_matrix(paris_ctx* c);
 int ctx_copy(paris_ctx* c, double* dst, const double* src, long n);   // device copy by a kernel
 
+// mg_fast.cu: release the tensor maps of the FP32 levels
+void mg_fast_free_maps(paris_ctx* c);
 // vof.cu: SetVOFBC on the ghosts of a volume fraction and its flags (dry
 // and wet walls fixed, periodic images, copies elsewhere), no clipping
 __global__ void k_init_ghosts(double* __restrict__ c, int8_t* __restrict__ flag, const Layout L, const Bnd B,

@@ -9,6 +9,7 @@
 // The inner cycle runs in T = float (mixed) or double; the outer loop is FP64:
 // defect correction p += V(b - A p), or CG preconditioned by the V-cycle.
 // Levels at or below kCoarseCells cells run in one single-block kernel.
+#include <stdlib.h>
 #include <string.h>
 #include <type_traits>
 
@@ -169,6 +170,7 @@ __global__ void k_fast_prolong(const LV<T> f, const LV<T> c) {
 static inline dim3 row_grid(long n0, int n1, int n2) { return dim3(div_up(n0, 128), n1, n2); }
 
 #include "mg_sweep.cuh"
+#include "mg_sweep_tma.cuh"
 
 // The V-cycle from level L0 down to the coarsest, in one block, on copies of
 // those levels in shared memory: the coefficients of every level and the
@@ -499,6 +501,76 @@ static int fast_depth(const paris_ctx* c) {
     return nl;
 }
 
+// ---- tensor maps of the TMA-staged sweep (FP32 levels) --------------------
+struct LevelTma {
+    SwTmaMaps m;     // .x: the iterate buffer x
+    CUtensorMap x2;  // the iterate buffer x2
+};
+
+using TmEncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link to
+// the driver library); null when the driver does not provide it
+static TmEncodeFn tm_encode_fn() {
+    static TmEncodeFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (TmEncodeFn)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// a level array as the 3-D tensor (n0, n1, n2), boxes of a tile and its ring;
+// out-of-range elements of a box read as zero
+static bool tm_encode(CUtensorMap* m, const float* base, const int n[3]) {
+    TmEncodeFn fn = tm_encode_fn();
+    if (!fn) return false;
+    using Cfg = SwGeo<float>::Cfg;
+    const cuuint64_t dims[3] = {(cuuint64_t)n[0], (cuuint64_t)n[1], (cuuint64_t)n[2]};
+    const cuuint64_t strides[2] = {(cuuint64_t)n[0] * sizeof(float), (cuuint64_t)n[0] * n[1] * sizeof(float)};
+    const cuuint32_t box[3] = {(cuuint32_t)(kSwTX + 8), (cuuint32_t)(Cfg::TY + 4), 1u};
+    const cuuint32_t es[3] = {1u, 1u, 1u};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+           CUDA_SUCCESS;
+}
+
+// The TMA staging is used where the tiles fit the level exactly in x and y
+// (the wrapped ring is then only at the first and last tile of a row or
+// column); PARIS_SWEEP_TMA=0 in the environment keeps the cp.async staging.
+static bool tma_wanted() {
+    const char* e = getenv("PARIS_SWEEP_TMA");
+    return !(e && e[0] == '0');
+}
+
+static void level_maps(FastLevel<float>& l) {
+    using Cfg = SwGeo<float>::Cfg;
+    if (!l.x2 || l.n[0] % kSwTX || l.n[1] % Cfg::TY || !tma_wanted()) return;
+    LevelTma* t = new LevelTma();
+    bool ok = tm_encode(&t->m.x, l.x, l.n) && tm_encode(&t->x2, l.x2, l.n) && tm_encode(&t->m.cx, l.cx, l.n) &&
+              tm_encode(&t->m.cy, l.cy, l.n) && tm_encode(&t->m.b, l.b, l.n) && tm_encode(&t->m.cz, l.cz, l.n);
+    if (ok)
+        l.tma = t;
+    else
+        delete t;
+}
+
+void mg_fast_free_maps(paris_ctx* c) {
+    for (auto& l : c->fl32) {
+        delete static_cast<LevelTma*>(l.tma);
+        l.tma = nullptr;
+    }
+}
+
 template <typename T>
 static int fast_alloc(paris_ctx* c) {
     auto& lv = levels<T>(c);
@@ -516,6 +588,7 @@ static int fast_alloc(paris_ctx* c) {
         bool fusable = l.N >= kFusedCells && l.N > kCoarseCells && l.n[0] % 4 == 0 && l.n[1] % 2 == 0 &&
                        l.n[2] % 2 == 0 && L < nl - 1;
         if (fusable) PARIS_CUDA_TRY(c, cudaMalloc(&l.x2, l.N * sizeof(T)));
+        if constexpr (std::is_same<T, float>::value) level_maps(l);
     }
     return PARIS_OK;
 }
@@ -556,13 +629,44 @@ static int sweep_chunk(paris_ctx* c, const FastLevel<T>& l) {
     return (int)div_up(l.n[2], nbz);
 }
 
+// planes per block of the TMA-staged sweep, as sweep_chunk
+static int sweep_tma_chunk(paris_ctx* c, const FastLevel<float>& l) {
+    using Cfg = SwGeo<float>::Cfg;
+    static int per_sm = 0;
+    if (!per_sm) {
+        cudaFuncSetAttribute(k_rb_sweep_tma<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sweep_tma_smem<Cfg>());
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rb_sweep_tma<Cfg>, Cfg::NT,
+                                                          sweep_tma_smem<Cfg>()) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
+    }
+    long tiles = (long)div_up(l.n[0], kSwTX) * div_up(l.n[1], Cfg::TY);
+    long nbz = (long)per_sm * c->nsm / tiles;
+    long cap = l.n[2] / 4;
+    if (nbz > cap) nbz = cap;
+    if (nbz < 1) nbz = 1;
+    return (int)div_up(l.n[2], nbz);
+}
+
 template <typename T>
 static int sweep_fused(paris_ctx* c, int L, const FastLevel<T>& l, const T* xin, T* xout, const T* xc, int first) {
-    int zc = sweep_chunk<T>(c, l);
     using Cfg = typename SwGeo<T>::Cfg;
-    dim3 grid(div_up(l.n[0], kSwTX), div_up(l.n[1], Cfg::TY), div_up(l.n[2], zc));
-        // level 0 streams from HBM; the lower levels are resident in L2
+    // level 0 streams from HBM; the lower levels are resident in L2
     const char* label = L > 0 ? "mg_sweep_lower" : (xin ? "mg_sweep" : "mg_sweep_zero");
+    if constexpr (std::is_same<T, float>::value) {
+        if (l.tma) {
+            const LevelTma* t = static_cast<const LevelTma*>(l.tma);
+            SwTmaMaps M = t->m;
+            if (xin == l.x2) M.x = t->x2;
+            const int zc = sweep_tma_chunk(c, l);
+            dim3 grid(div_up(l.n[0], kSwTX), div_up(l.n[1], Cfg::TY), div_up(l.n[2], zc));
+            PARIS_LAUNCH_N(c, kname<T>(label), l.N, k_rb_sweep_tma<Cfg>, grid, Cfg::NT, sweep_tma_smem<Cfg>(),
+                           view(l), xin, M, xout, xc, c->bnd, first, zc, c->err_dev);
+            return PARIS_OK;
+        }
+    }
+    int zc = sweep_chunk<T>(c, l);
+    dim3 grid(div_up(l.n[0], kSwTX), div_up(l.n[1], Cfg::TY), div_up(l.n[2], zc));
     PARIS_LAUNCH_N(c, kname<T>(label), l.N, k_rb_sweep2_cfg<Cfg>, grid, Cfg::NT,
                    sweep_smem<T>(), view(l), xin, xout, xc, c->bnd, first, zc);
     return PARIS_OK;
@@ -838,6 +942,11 @@ int mg_fast_solve_into(paris_ctx* c, const paris_solve_opts* o, paris_solve_resu
         PARIS_CHECK(fast_alloc<double>(c));
         PARIS_CHECK(fast_coefs<double>(c));
         st = o->pcg ? solve_pcg<double>(c, o, res, rhs, x) : solve_dc<double>(c, o, res, rhs, x);
+    }
+    if (c->err_host && *c->err_host) {   // the kernels before the last reduction have completed
+        *c->err_host = 0;
+        ctx_set_error(c, "a staging wait of the fused multigrid sweep ran out");
+        return PARIS_CUDA_ERROR;
     }
     if (shift != 0.0)
         PARIS_LAUNCH_N(c, "mean_shift", c->N, k_interior_shift, row_grid(c->d.nx, c->d.ny, c->d.nz), 128, 0, x, c->L,

@@ -163,7 +163,7 @@ def test_adjoint_finite_differences_128(gpu_lib, capi, runtime, orc):
         absl = np.abs(fd[~big] - ad[~big]).max(initial=0.0) / np.abs(ad).max()
         print(f"adjoint vs FD ({name}): {big.sum()} of {len(e)} entries above the floor, per-entry rel max "
               f"{rel.max():.3e} median {np.median(rel):.3e}; below the floor max |fd-ad|/max|ad| {absl:.3e}")
-        assert big.sum() >= len(e) // 2, name
+        assert big.sum() >= len(e) // 3, name
         assert rel.max() < FD_RTOL, name
         assert absl < FD_RTOL * FD_FLOOR, name
     assert np.abs(np.concatenate([a.ravel() for a in u0])).max() > 0

@@ -121,45 +121,48 @@ def test_static_droplet_64_follows_oracle(gpu_lib, capi, runtime, orc, mode):
     assert dpr <= tol[2]
 
 
-@pytest.mark.parametrize("mode,tol", [("fp64", 1e-12), ("mixed", 1e-10)])
-def test_static_droplet_128_follows_oracle(gpu_lib, capi, runtime, orc, mode, tol):
-    """The droplet at its stated size, 128^3, for 10 steps from the same
-    state on both sides.  The oracle solves with its FP64 restatement of the
-    B200 multigrid (flexible CG preconditioned by V(2,2) cycles); the device
-    with the same algorithm in FP64 or with FP32 cycles inside the FP64 loop
-    (mixed).  The velocity after the projection is the small difference of
-    u* and dt B grad p (spurious currents), so it carries the solver
-    tolerance amplified: at ||r||/||b|| < 1e-10 the FP64 solves of the two
-    sides left the velocities 1e-2 of max |u| apart and one cell of cvof
-    1.2e-9 apart (RMS 2.5e-12).  The FP64 comparison therefore solves both
-    sides to 1e-12; the mixed one runs at the workload's 1e-10."""
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_static_droplet_128_follows_oracle(gpu_lib, capi, runtime, orc, mode):
+    """The droplet at its stated size, 128^3, for 10 steps, each from the same
+    state on both sides: the oracle's state after the previous step is
+    uploaded, one step runs on each side, and cvof, velocity and pressure are
+    compared.  The oracle solves with its FP64 restatement of the B200
+    multigrid (flexible CG preconditioned by V(2,2) cycles) to
+    ||r||/||b|| < 1e-10; the device with the same algorithm in FP64, or with
+    FP32 cycles inside the FP64 loop (mixed).  Run free instead, the two
+    sides part after a few steps where two candidate PLIC normals of a mixed
+    cell tie to the last bit: CUDA's and glibc's pow/acos differ by an ulp,
+    and one cell of cvof moves by 1.2e-9 (RMS 2.5e-12 over the box)."""
     n, steps = 128, 10
     d, dt, _ = droplet(capi, n)
     cvof, flag, _ = orc.init_spheres(d, [(0.5, 0.5, 0.5)], [R], refinement=8)
     st = {"cvof": cvof, "flag": flag, "u": orc.zeros(d), "v": orc.zeros(d), "w": orc.zeros(d), "p": orc.zeros(d)}
-    solve = {"max_error": 0.0, "rel_tol": tol, "maxit": 200, "pcg": 1,
+    solve = {"max_error": 0.0, "rel_tol": 1e-10, "maxit": 200, "pcg": 1,
              "mode": capi.MG_FP64 if mode == "fp64" else capi.MG_MIXED}
-    with runtime.ParisGpu(d) as gpu:
-        gpu.upload(capi.F_CVOF, st["cvof"])
-        gpu.upload(capi.F_VOF_FLAG, st["flag"])
-        for f in (capi.F_U, capi.F_V, capi.F_W, capi.F_P):
-            gpu.fill_field(f, 0.0)
-        its = run(gpu, capi, runtime, steps, dt, solve)
-        out = {f: gpu.download(getattr(capi, "F_" + f.upper())) for f in ("cvof", "u", "v", "w", "p")}
-    its_ref = [orc.ns_step(d, st, k, dt, solver="fast", rel_tol=tol, maxit=200) for k in range(1, steps + 1)]
     g = d.ng
     inner = (slice(g, -g),) * 3
-    dc = np.abs(out["cvof"] - st["cvof"]).max()
-    dc2 = float(np.sqrt(np.mean((out["cvof"] - st["cvof"])[inner] ** 2)))
-    vmax = max(np.abs(st[c][inner]).max() for c in "uvw")
-    du = max(np.abs(out[c] - st[c]).max() for c in "uvw") / vmax
-    pi, po = st["p"][inner], out["p"][inner]
-    dpr = np.abs((po - po.mean()) - (pi - pi.mean())).max() / (2.0 * SIGMA / R)
-    print(f"\nstatic droplet {n}^3, {steps} steps, {mode} solver to {tol:g} against the oracle: max |dcvof| "
-          f"{dc:.3e} (rms {dc2:.3e}), max |du| / max|u| {du:.3e} (max|u| {vmax:.3e}), max |dp| / (2 sigma/R) "
-          f"{dpr:.3e}; iterations {its} oracle {its_ref}")
-    lim = {"fp64": (1e-11, 1e-13, 1e-3, 1e-9), "mixed": (1e-8, 1e-10, 1e-1, 1e-6)}[mode]
-    assert dc <= lim[0]
-    assert dc2 <= lim[1]
-    assert du <= lim[2]
-    assert dpr <= lim[3]
+    rows = []
+    with runtime.ParisGpu(d) as gpu:
+        for k in range(1, steps + 1):
+            gpu.upload(capi.F_CVOF, st["cvof"])
+            gpu.upload(capi.F_VOF_FLAG, st["flag"])
+            for c in "uvwp":
+                gpu.upload(getattr(capi, "F_" + c.upper()), st[c])
+            r = gpu.ns_step(k, dt, solve=solve)
+            out = {f: gpu.download(getattr(capi, "F_" + f.upper())) for f in ("cvof", "u", "v", "w", "p")}
+            it_ref = orc.ns_step(d, st, k, dt, solver="fast", rel_tol=1e-10, maxit=200)
+            dc = np.abs(out["cvof"] - st["cvof"]).max()
+            vmax = max(np.abs(st[c][inner]).max() for c in "uvw")
+            du = max(np.abs(out[c] - st[c]).max() for c in "uvw") / vmax
+            pi, po = st["p"][inner], out["p"][inner]
+            dpr = np.abs((po - po.mean()) - (pi - pi.mean())).max() / (2.0 * SIGMA / R)
+            rows.append((dc, du, dpr, r.it, it_ref, vmax))
+    R_ = np.array(rows)
+    print(f"\nstatic droplet {n}^3, {steps} steps from the same state, {mode} solver against the oracle: "
+          f"max |dcvof| {R_[:, 0].max():.3e}, max |du| / max|u| {R_[:, 1].max():.3e} (max|u| up to "
+          f"{R_[:, 5].max():.3e}), max |dp| / (2 sigma/R) {R_[:, 2].max():.3e}; iterations "
+          f"{R_[:, 3].astype(int).tolist()} oracle {R_[:, 4].astype(int).tolist()}")
+    lim = {"fp64": (1e-13, 1e-4, 1e-9), "mixed": (1e-13, 1e-3, 1e-8)}[mode]
+    assert R_[:, 0].max() <= lim[0]
+    assert R_[:, 1].max() <= lim[1]
+    assert R_[:, 2].max() <= lim[2]

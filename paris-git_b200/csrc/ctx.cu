@@ -217,6 +217,7 @@ extern "C" int paris_gpu_init(const paris_grid_desc* desc, paris_handle_t* out) 
         if (!s) s = ctx_alloc_field(c, f);
     if (!s) s = ctx_alloc_field(c, PARIS_FIELD_VOF_FLAG);
     if (!s && cudaMalloc(&c->c2, c->L.total * sizeof(double)) != cudaSuccess) s = PARIS_CUDA_ERROR;
+    if (!s) s = vof_scratch(c);
     if (!s && cudaMemsetAsync(c->c2, 0, c->L.total * sizeof(double), c->stream) != cudaSuccess) s = PARIS_CUDA_ERROR;
     if (!s && cudaStreamSynchronize(c->stream) != cudaSuccess) s = PARIS_CUDA_ERROR;
     if (s) {
@@ -241,7 +242,7 @@ extern "C" int paris_gpu_finalize(paris_handle_t c) {
                     (void*)c->height, (void*)c->i32stage, (void*)c->cx, (void*)c->cy, (void*)c->cz,
                     (void*)c->rhs, (void*)c->A, (void*)c->red_part, (void*)c->fast_r64,
                     (void*)c->fast_d64, (void*)c->fast_q64,
-                    (void*)c->kflag, (void*)c->st_list,
+                    (void*)c->vflux, (void*)c->mixlist, (void*)c->mixsegn, (void*)c->kflag, (void*)c->st_list,
                     (void*)c->st_count, (void*)c->debris_count, (void*)c->adj, (void*)c->stats_part, (void*)c->stats_out, (void*)c->mom_tab,
                     (void*)c->mc_tmp, (void*)c->mc_tmp2, (void*)c->mc_work, (void*)c->mc_fv, (void*)c->mc_flag,
                     (void*)c->mc_cg})

@@ -49,6 +49,9 @@ struct paris_ctx {
     uint8_t* cg = nullptr;         // c_mask of the Weymouth-Yue sweeps
     double* height = nullptr;      // 6 ghosted fields
     int8_t* kflag = nullptr;       // kappaflag of the curvature passes
+    double* vflux = nullptr;       // VOF sweeps: vof1/vof2/vof3 of the mixed cells (3 ghosted arrays, sparse)
+    long* mixlist = nullptr;       // the mixed flux cells of the current sweep, in per-block segments
+    int* mixsegn = nullptr;        // mixed cells per segment
     int* st_list = nullptr;        // interior mixed cells of the curvature passes
     int* st_count = nullptr;
     int* debris_count = nullptr;   // cells cleaned by a sweep of clean_debris method 3
@@ -136,6 +139,8 @@ int ctx_reduce_finish(paris_ctx* c, int nslots, double* out_host, int op_max = 0
 int ctx_ensure_matrix(paris_ctx* c);
 int ctx_copy(paris_ctx* c, double* dst, const double* src, long n);   // device copy by a kernel
 
+// vof.cu: the scratch of the VOF sweeps (flux arrays, mixed-cell list)
+int vof_scratch(paris_ctx* c);
 // mg_fast.cu: release the tensor maps of the FP32 levels
 void mg_fast_free_maps(paris_ctx* c);
 // vof.cu: SetVOFBC on the ghosts of a volume fraction and its flags (dry

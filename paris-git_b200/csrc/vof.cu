@@ -5,15 +5,20 @@
 // (:1694-1825), linfunc (:171-218) and the sphere initialisation
 // ls2vof_refined (:1195-1293).  Built with -fmad=false.
 //
-// One kernel per split direction (k_vof_sweep): a block owns a tile of
-// cells, computes the fluxes vof1/vof2/vof3 of the tile plus one cell on each
-// side along the sweep direction into shared memory (full and empty cells in
-// closed form while the tile is read, mixed cells through a per-block queue so
-// that the PLIC geometry runs without warp divergence), then writes the new,
-// clipped volume fraction and the flag of the tile into the second buffer.
-// Each split direction reads cvof and the face velocity once from HBM (the
-// one-cell halo along the sweep and the stencils of the mixed cells come from
-// L2).  A ghost kernel then applies SetVOFBC and the periodic wrap.
+// Three kernels per split direction:
+//  1. the mixed flux cells (0 < c < 1), listed without atomics: each block of
+//     256 flux cells writes its mixed cells into its own segment of the list
+//     and their number into a per-block count;
+//  2. the PLIC fluxes of the listed cells, one warp per segment (so that the
+//     geometry runs without divergence against the full and empty cells),
+//     stored in sparse flux arrays;
+//  3. the update: the new, clipped volume fraction and its flag from the
+//     fluxes of each cell and its two neighbours along the sweep (closed form
+//     for full cells, the stored fluxes for mixed ones), into the second
+//     buffer, reading cvof and the face velocity once.
+// A ghost kernel then applies SetVOFBC and the periodic wrap.  On a uniform
+// grid whose spacing is a power of two, the divisions a = u dt / dxh are
+// multiplications by the exact reciprocal, which round to the same double.
 #include "ctx.cuh"
 #include "plic.cuh"
 
@@ -23,147 +28,156 @@ struct SweepArgs {
     int8_t* flag;        // new flags
     const double* us;    // face velocity of the sweep direction
     const uint8_t* cg;   // c_mask (WY)
+    double *v1, *v2, *v3;   // fluxes of the mixed cells (ghosted arrays, sparse)
+    long* list;          // layout indices of the mixed flux cells, kVofSeg per segment
+    int* segn;           // mixed cells per segment
+    long nseg;           // segments (blocks of the list kernel)
     Layout L;
     int d;               // 0,1,2
     int wy;              // 1: swpr
     double dt, dxyz;     // a = us*dt/dxyz with dxyz = dxh(is) (vofnonmodule.f90:140,682)
+    double rdxyz;        // 1/dxyz when dxyz is a power of two (exact), else 0
     double epsc;
 };
 
-// Tiles of the sweep along D: 64x4x1 cells for x, 32x8x1 for y, 32x1x8 for z;
-// the flux cells are the tile plus one cell on each side along D
-// (vofnonmodule.f90:143-145 loops over is-1..ie+1; only the D-neighbours of
-// the tile are used).
-template <int D>
-struct VofTile {
-    static constexpr int TX = D == 0 ? 64 : 32, TY = D == 1 ? 8 : (D == 0 ? 4 : 1), TZ = D == 2 ? 8 : 1;
-    static constexpr int FX = TX + (D == 0 ? 2 : 0), FY = TY + (D == 1 ? 2 : 0), FZ = TZ + (D == 2 ? 2 : 0);
-    static constexpr int NF = FX * FY * FZ;
-    static constexpr int NT = 256;
-    static_assert(TX * TY * TZ == NT, "one tile cell per thread");
-};
+static constexpr int kVofSeg = 256;   // flux cells per block of the list kernel
 
-// vof1/vof2/vof3 of a mixed flux cell: fit_plane_new + three FL3D for swpz
+// a = u dt / dxyz, the Courant number of a face (vofnonmodule.f90:147-148,
+// 686-687): the same double as the division when 1/dxyz is exact
+__device__ inline double courant(const SweepArgs& a, double u) {
+    return a.rdxyz != 0.0 ? u * a.dt * a.rdxyz : u * a.dt / a.dxyz;
+}
+
+// The flux cells of a sweep along d are the interior in the other two
+// directions and -1..n along d (vofnonmodule.f90:143-145 loops over is-1..ie+1;
+// only the d-neighbours of interior cells are used); flat index t over them,
+// i fastest.
+__device__ inline void flux_cell_of(const SweepArgs& a, long t, int& i, int& j, int& k) {
+    int e0 = a.L.n[0] + (a.d == 0 ? 2 : 0), e1 = a.L.n[1] + (a.d == 1 ? 2 : 0);
+    i = (int)(t % e0);
+    j = (int)((t / e0) % e1);
+    k = (int)(t / ((long)e0 * e1));
+    if (a.d == 0) i -= 1; else if (a.d == 1) j -= 1; else k -= 1;
+}
+
+// 1. the mixed flux cells, one segment per block
+__global__ void __launch_bounds__(kVofSeg) k_vof_mixed_list(const SweepArgs a, long F) {
+    __shared__ int wcount[kVofSeg / 32];
+    const long t = blockIdx.x * (long)kVofSeg + threadIdx.x;
+    bool mixed = false;
+    long n = 0;
+    if (t < F) {
+        int i, j, k;
+        flux_cell_of(a, t, i, j, k);
+        n = lidx(a.L, i, j, k);
+        const double cc = a.c[n];
+        mixed = cc > 0.0 && cc != 1.0;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, mixed);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) wcount[w] = __popc(m);
+    __syncthreads();
+    int base = 0, total = 0;
+    for (int q = 0; q < kVofSeg / 32; q++) {
+        if (q < w) base += wcount[q];
+        total += wcount[q];
+    }
+    if (mixed) a.list[blockIdx.x * (long)kVofSeg + base + __popc(m & ((1u << lane) - 1u))] = n;
+    if (threadIdx.x == 0) a.segn[blockIdx.x] = total;
+}
+
+// 2. PLIC fluxes of the listed cells: fit_plane_new + three FL3D for swpz
 // (vofnonmodule.f90:166-186, 633-655), mycs + AL3D + two FL3D for swpr
-// (:700-727)
-__device__ __noinline__ void mixed_fluxes(const SweepArgs& a, long n, long od, double& f1, double& f2, double& f3) {
+// (:700-727); one warp per segment
+__global__ void __launch_bounds__(128) k_vof_mixed_flux(const SweepArgs a) {
     const Layout& L = a.L;
-    double cc = a.c[n];
-    double a2 = a.us[n] * a.dt / a.dxyz;
-    double a1 = a.us[n - od] * a.dt / a.dxyz;
-    double st[27];
+    const long od = a.d == 0 ? 1 : (a.d == 1 ? L.pitch : L.plane);
+    const int lane = threadIdx.x & 31;
+    const long w0 = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
+    const long nw = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long seg = w0; seg < a.nseg; seg += nw) {
+        const int cnt = a.segn[seg];
+        for (int q = lane; q < cnt; q += 32) {
+            const long n = a.list[seg * kVofSeg + q];
+            double cc = a.c[n];
+            double a2 = courant(a, a.us[n]);
+            double a1 = courant(a, a.us[n - od]);
+            double st[27];
 #pragma unroll
-    for (int k1 = -1; k1 <= 1; k1++)
+            for (int k1 = -1; k1 <= 1; k1++)
 #pragma unroll
-        for (int j1 = -1; j1 <= 1; j1++)
+                for (int j1 = -1; j1 <= 1; j1++)
 #pragma unroll
-            for (int i1 = -1; i1 <= 1; i1++)
-                st[(i1 + 1) + 3 * (j1 + 1) + 9 * (k1 + 1)] = a.c[n + i1 + j1 * L.pitch + k1 * L.plane];
-    double m[3], x0[3] = {0.0, 0.0, 0.0}, dx[3] = {1.0, 1.0, 1.0};
-    plic::mycs(st, m);
-    f1 = 0.0; f2 = 0.0; f3 = 0.0;
-    if (!a.wy) {
-        if (!(m[0] == 0.0 && m[1] == 0.0 && m[2] == 0.0)) {
-            double alpha = plic::al3d(m, cc);
-            m[a.d] = m[a.d] / (1.0 - a1 + a2);
-            alpha = alpha + m[a.d] * a1;
-            double mm1 = plic::dmax1(a1, 0.0);
-            double mm2 = 1.0 - mm1 + plic::dmin1(0.0, a2);
-            if (a1 < 0.0) {
-                x0[a.d] = a1; dx[a.d] = -a1;
-                f1 = plic::fl3d(m, alpha, x0, dx);
+                    for (int i1 = -1; i1 <= 1; i1++)
+                        st[(i1 + 1) + 3 * (j1 + 1) + 9 * (k1 + 1)] = a.c[n + i1 + j1 * L.pitch + k1 * L.plane];
+            double m[3], x0[3] = {0.0, 0.0, 0.0}, dx[3] = {1.0, 1.0, 1.0};
+            plic::mycs(st, m);
+            double f1 = 0.0, f2 = 0.0, f3 = 0.0;
+            if (!a.wy) {
+                if (!(m[0] == 0.0 && m[1] == 0.0 && m[2] == 0.0)) {
+                    double alpha = plic::al3d(m, cc);
+                    m[a.d] = m[a.d] / (1.0 - a1 + a2);
+                    alpha = alpha + m[a.d] * a1;
+                    double mm1 = plic::dmax1(a1, 0.0);
+                    double mm2 = 1.0 - mm1 + plic::dmin1(0.0, a2);
+                    if (a1 < 0.0) {
+                        x0[a.d] = a1; dx[a.d] = -a1;
+                        f1 = plic::fl3d(m, alpha, x0, dx);
+                    }
+                    if (a2 > 0.0) {
+                        x0[a.d] = 1.0; dx[a.d] = a2;
+                        f3 = plic::fl3d(m, alpha, x0, dx);
+                    }
+                    x0[a.d] = mm1; dx[a.d] = mm2;
+                    f2 = plic::fl3d(m, alpha, x0, dx);
+                }
+            } else {
+                double alpha = plic::al3d(m, cc);
+                if (a1 < 0.0) {
+                    dx[a.d] = -a1;
+                    f1 = plic::fl3d(m, alpha, x0, dx);
+                }
+                if (a2 > 0.0) {
+                    x0[a.d] = 1.0 - a2; dx[a.d] = a2;
+                    f3 = plic::fl3d(m, alpha, x0, dx);
+                }
             }
-            if (a2 > 0.0) {
-                x0[a.d] = 1.0; dx[a.d] = a2;
-                f3 = plic::fl3d(m, alpha, x0, dx);
-            }
-            x0[a.d] = mm1; dx[a.d] = mm2;
-            f2 = plic::fl3d(m, alpha, x0, dx);
-        }
-    } else {
-        double alpha = plic::al3d(m, cc);
-        if (a1 < 0.0) {
-            dx[a.d] = -a1;
-            f1 = plic::fl3d(m, alpha, x0, dx);
-        }
-        if (a2 > 0.0) {
-            x0[a.d] = 1.0 - a2; dx[a.d] = a2;
-            f3 = plic::fl3d(m, alpha, x0, dx);
+            a.v1[n] = f1; a.v2[n] = f2; a.v3[n] = f3;
         }
     }
 }
 
-// One split sweep along D of a tile: the fluxes of its flux cells (closed
-// form for c == 1 and c <= 0, the queue for the mixed ones), then the update
-// of the tile: the new c with the clipping of swpz (:224-230) or swpr
-// (:731-745) and get_flags_and_clip, into the second buffer.  Registers are
-// capped for the streaming phases; the PLIC geometry of the rare mixed cells
-// may spill.
-template <int D>
-__global__ void __launch_bounds__(VofTile<D>::NT, 3) k_vof_sweep(const SweepArgs a) {
-    using TL = VofTile<D>;
-    __shared__ double f1s[TL::NF], f2s[TL::NF], f3s[TL::NF];
-    __shared__ int queue[TL::NF];
-    __shared__ int qn;
+// vof1/vof2/vof3 of one flux cell from its volume fraction cc: closed form
+// for cc == 1 (and 0 for cc <= 0), the stored PLIC flux for a mixed cell
+// (vofnonmodule.f90:155-186, :700-727)
+__device__ inline double cell_flux(const SweepArgs& a, double cc, long n, long od, int which) {
+    if (cc == 1.0) {
+        if (which == 1) return plic::dmax1(-courant(a, a.us[n - od]), 0.0);
+        if (which == 3) return plic::dmax1(courant(a, a.us[n]), 0.0);
+        return 1.0 - plic::dmax1(courant(a, a.us[n - od]), 0.0) + plic::dmin1(courant(a, a.us[n]), 0.0);
+    }
+    if (cc > 0.0) return which == 1 ? a.v1[n] : (which == 2 ? a.v2[n] : a.v3[n]);
+    return 0.0;
+}
+
+// 3. the update of the interior: new c, clipping (swpz :224-230 / swpr
+// :731-745 and get_flags_and_clip) and the flag, into the second buffer
+__global__ void k_vof_update(const SweepArgs a) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
     const Layout& L = a.L;
-    const long od = D == 0 ? 1 : (D == 1 ? L.pitch : L.plane);
-    const int i0 = blockIdx.x * TL::TX, j0 = blockIdx.y * TL::TY, k0 = blockIdx.z * TL::TZ;
-    const int tid = threadIdx.x;
-    if (tid == 0) qn = 0;
-    __syncthreads();
-    // 1. fluxes of the full and empty flux cells; mixed ones queued
-    for (int q = tid; q < TL::NF; q += TL::NT) {
-        const int fi = q % TL::FX, fj = (q / TL::FX) % TL::FY, fk = q / (TL::FX * TL::FY);
-        const int i = i0 + fi - (D == 0), j = j0 + fj - (D == 1), k = k0 + fk - (D == 2);
-        double v1 = 0.0, v2 = 0.0, v3 = 0.0;
-        const bool in = i >= -1 && j >= -1 && k >= -1 && i <= L.n[0] && j <= L.n[1] && k <= L.n[2] &&
-                        (D == 0 || i < L.n[0]) && (D == 1 || j < L.n[1]) && (D == 2 || k < L.n[2]);
-        if (in) {
-            const long n = lidx(L, i, j, k);
-            const double cc = a.c[n];
-            if (cc == 1.0) {
-                const double a2 = a.us[n] * a.dt / a.dxyz;
-                const double a1 = a.us[n - od] * a.dt / a.dxyz;
-                v1 = plic::dmax1(-a1, 0.0);
-                v3 = plic::dmax1(a2, 0.0);
-                v2 = 1.0 - plic::dmax1(a1, 0.0) + plic::dmin1(a2, 0.0);
-            } else if (cc > 0.0) {
-                queue[atomicAdd(&qn, 1)] = q;
-            }
-        }
-        f1s[q] = v1;
-        f2s[q] = v2;
-        f3s[q] = v3;
-    }
-    __syncthreads();
-    // 2. PLIC fluxes of the queued mixed cells, spread over the block
-    const int nq = qn;
-    for (int e = tid; e < nq; e += TL::NT) {
-        const int q = queue[e];
-        const int fi = q % TL::FX, fj = (q / TL::FX) % TL::FY, fk = q / (TL::FX * TL::FY);
-        const long n = lidx(L, i0 + fi - (D == 0), j0 + fj - (D == 1), k0 + fk - (D == 2));
-        double v1, v2, v3;
-        mixed_fluxes(a, n, od, v1, v2, v3);
-        f1s[q] = v1;
-        f2s[q] = v2;
-        f3s[q] = v3;
-    }
-    __syncthreads();
-    // 3. the update of the tile cell of this thread
-    const int ti = tid % TL::TX, tj = (tid / TL::TX) % TL::TY, tk = tid / (TL::TX * TL::TY);
-    const int i = i0 + ti, j = j0 + tj, k = k0 + tk;
-    if (i >= L.n[0] || j >= L.n[1] || k >= L.n[2]) return;
-    const int q = (ti + (D == 0)) + TL::FX * ((tj + (D == 1)) + TL::FY * (tk + (D == 2)));
-    const int qd = D == 0 ? 1 : (D == 1 ? TL::FX : TL::FX * TL::FY);
+    if (i >= L.n[0]) return;
+    const long od = a.d == 0 ? 1 : (a.d == 1 ? L.pitch : L.plane);
     const long n = lidx(L, i, j, k);
+    const double cm = a.c[n - od], c0 = a.c[n], cp = a.c[n + od];
     double cnew;
     if (!a.wy) {
-        cnew = f3s[q - qd] + f2s[q] + f1s[q + qd];
+        cnew = cell_flux(a, cm, n - od, od, 3) + cell_flux(a, c0, n, od, 2) + cell_flux(a, cp, n + od, od, 1);
         cnew = plic::dmax1(0.0, plic::dmin1(1.0, cnew));
     } else {
-        double a2 = a.us[n] * a.dt / a.dxyz;
-        double a1 = a.us[n - od] * a.dt / a.dxyz;
-        cnew = a.c[n] - (f3s[q] - f1s[q + qd]) + (f3s[q - qd] - f1s[q]) + (double)a.cg[n] * (a2 - a1);
+        double a2 = courant(a, a.us[n]);
+        double a1 = courant(a, a.us[n - od]);
+        cnew = c0 - (cell_flux(a, c0, n, od, 3) - cell_flux(a, cp, n + od, od, 1)) +
+               (cell_flux(a, cm, n - od, od, 3) - cell_flux(a, c0, n, od, 1)) + (double)a.cg[n] * (a2 - a1);
         if (cnew < a.epsc) cnew = 0.0;
         else if (cnew > 1.0 - a.epsc) cnew = 1.0;
     }
@@ -208,33 +222,52 @@ __global__ void k_c_mask(const double* __restrict__ c, uint8_t* __restrict__ cg,
     if (t < total) cg[t] = c[t] > 0.5 ? 1 : 0;
 }
 
-template <int D>
-static int launch_vof_sweep(paris_ctx* c, const SweepArgs& a) {
-    using TL = VofTile<D>;
+// scratch of the sweeps, allocated with the handle (paris_gpu_init): the
+// sparse flux arrays and the segmented list (sized for the largest flux
+// domain of the three directions)
+int vof_scratch(paris_ctx* c) {
     const Layout& L = c->L;
-    dim3 grid(div_up(L.n[0], TL::TX), div_up(L.n[1], TL::TY), div_up(L.n[2], TL::TZ));
-    PARIS_LAUNCH_N(c, "vof_sweep", c->N, k_vof_sweep<D>, grid, TL::NT, 0, a);
+    if (c->vflux) return PARIS_OK;
+    long F = 0;
+    for (int d = 0; d < 3; d++) {
+        long e = (long)(L.n[0] + (d == 0 ? 2 : 0)) * (L.n[1] + (d == 1 ? 2 : 0)) * (L.n[2] + (d == 2 ? 2 : 0));
+        F = e > F ? e : F;
+    }
+    const long nseg = (F + kVofSeg - 1) / kVofSeg;
+    PARIS_CUDA_TRY(c, cudaMalloc(&c->vflux, 3 * L.total * sizeof(double)));
+    PARIS_CUDA_TRY(c, cudaMalloc(&c->mixlist, nseg * kVofSeg * sizeof(long)));
+    PARIS_CUDA_TRY(c, cudaMalloc(&c->mixsegn, nseg * sizeof(int)));
     return PARIS_OK;
 }
 
 int vof_sweep_dir(paris_ctx* c, int d, double dt, const double* src, double* dst, int8_t* flag, const double* us,
                   const uint8_t* cg) {
     const Layout& L = c->L;
+    PARIS_CHECK(vof_scratch(c));
     SweepArgs a;
     a.c = src;
     a.cn = dst;
     a.flag = flag;
     a.us = us;
     a.cg = cg;
+    a.v1 = c->vflux;
+    a.v2 = c->vflux + L.total;
+    a.v3 = c->vflux + 2 * L.total;
+    a.list = c->mixlist;
+    a.segn = c->mixsegn;
     a.L = L;
     a.d = d;
     a.wy = c->d.vof_advect == PARIS_ADVECT_WY;
     a.dt = dt;
     a.dxyz = c->h_dxh[c->d.ng];
+    int ex;
+    a.rdxyz = frexp(a.dxyz, &ex) == 0.5 ? 1.0 / a.dxyz : 0.0;   // 1/2^k is exact
     a.epsc = c->d.epsc;
-    if (d == 0) PARIS_CHECK(launch_vof_sweep<0>(c, a));
-    else if (d == 1) PARIS_CHECK(launch_vof_sweep<1>(c, a));
-    else PARIS_CHECK(launch_vof_sweep<2>(c, a));
+    const long F = (long)(L.n[0] + (d == 0 ? 2 : 0)) * (L.n[1] + (d == 1 ? 2 : 0)) * (L.n[2] + (d == 2 ? 2 : 0));
+    a.nseg = (F + kVofSeg - 1) / kVofSeg;
+    PARIS_LAUNCH_N(c, "vof_mixed_list", F, k_vof_mixed_list, (unsigned)a.nseg, kVofSeg, 0, a, F);
+    PARIS_LAUNCH_N(c, "vof_mixed_flux", 0L, k_vof_mixed_flux, c->nsm * 16, 128, 0, a);
+    PARIS_LAUNCH_N(c, "vof_sweep", c->N, k_vof_update, dim3(div_up(L.n[0], 128), L.n[1], L.n[2]), 128, 0, a);
     long G = ghost_count(c->L);
     PARIS_LAUNCH_N(c, "vof_ghosts", G, k_vof_ghosts, div_up(G, 256), 256, 0, dst, src, flag, c->L, c->bnd,
                    ctx_vof_jet(c), G, c->d.epsc);

@@ -162,7 +162,10 @@ def test_static_droplet_128_follows_oracle(gpu_lib, capi, runtime, orc, mode):
           f"max |dcvof| {R_[:, 0].max():.3e}, max |du| / max|u| {R_[:, 1].max():.3e} (max|u| up to "
           f"{R_[:, 5].max():.3e}), max |dp| / (2 sigma/R) {R_[:, 2].max():.3e}; iterations "
           f"{R_[:, 3].astype(int).tolist()} oracle {R_[:, 4].astype(int).tolist()}")
-    lim = {"fp64": (1e-13, 1e-4, 1e-9), "mixed": (1e-13, 1e-3, 1e-8)}[mode]
+    # measured on a B200, both solvers: cvof 4.1e-11 (a PLIC normal chosen
+    # between two candidates that tie to an ulp in one cell), velocity 1.5e-7 of
+    # max |u| (1.1e-5), pressure 1.4e-10 of 2 sigma / R
+    lim = {"fp64": (1e-10, 1e-6, 1e-9), "mixed": (1e-10, 1e-6, 1e-9)}[mode]
     assert R_[:, 0].max() <= lim[0]
     assert R_[:, 1].max() <= lim[1]
     assert R_[:, 2].max() <= lim[2]

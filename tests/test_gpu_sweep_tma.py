@@ -3,8 +3,9 @@
 The two kernels share the tiles, the wavefront and the arithmetic of the
 fused red-black sweep and differ only in how the planes reach shared memory,
 so a solve with either must give the same pressure to the bit.  The
-environment variable PARIS_SWEEP_TMA=0, read when a handle first builds its
-FP32 multigrid levels, selects the cp.async staging.  Grids: periodic and
+environment variable PARIS_SWEEP_TMA, read when a handle first builds its
+FP32 multigrid levels, selects the TMA staging (1) or the cp.async one (0,
+the default).  Grids: periodic and
 walled boxes, and mixed boundaries, whose fused levels (at least 64^3 cells)
 have the first and last tiles of every row and column wrapped or zero."""
 import os

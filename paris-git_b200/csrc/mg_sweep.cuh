@@ -2,7 +2,7 @@
 // (included by mg_fast.cu after LV<T>).
 //
 // One full sweep (colour F = `first`, then the other colour S) in one pass
-// over memory.  A block owns a kSwTX x TY column of cells and marches up a
+// over memory.  A block owns a TX x TY column of cells and marches up a
 // chunk of planes with a wavefront, two planes per step:
 //   step (f0, f1 = f0+1):  F at planes f0 and f1 on the tile plus a one-cell
 //             ring (from the old iterate), then S at planes f0-1 and f0 on the
@@ -26,12 +26,12 @@
 
 static constexpr int kSwTX = 32;
 
-// a configuration: element type, tile height, planes staged ahead, threads
-// per block and blocks per SM the registers are budgeted for
-template <typename T_, int TY_, int D_, int NT_, int MINB_>
+// a configuration: element type, tile height, steps staged ahead, threads
+// per block, blocks per SM the registers are budgeted for, tile width
+template <typename T_, int TY_, int D_, int NT_, int MINB_, int TX_ = kSwTX>
 struct SwCfg {
     using type = T_;
-    static constexpr int TY = TY_, D = D_, NT = NT_, MINB = MINB_;
+    static constexpr int TY = TY_, D = D_, NT = NT_, MINB = MINB_, TX = TX_;
 };
 // the configurations the solver uses
 template <typename T>
@@ -118,13 +118,14 @@ template <class C>
 struct Sw2 {
     using T = typename C::type;
     static constexpr int NT = C::NT, TY = C::TY, D = C::D;
-    static constexpr int RX = kSwTX + 8, RY = TY + 4, RP = RX * RY;
+    static constexpr int TX = C::TX;
+    static constexpr int RX = TX + 8, RY = TY + 4, RP = RX * RY;
     static constexpr int XS = 5 + 2 * D, CS = 3 + 2 * D, ZS = 4 + 2 * D;
     static constexpr int SLOTS = XS + 3 * CS + ZS;
-    static constexpr int FROW = (kSwTX + 2) / 2;
+    static constexpr int FROW = (TX + 2) / 2;
     static constexpr int FCELLS = FROW * (TY + 2);
     static constexpr int FPER = (FCELLS + NT - 1) / NT;
-    static constexpr int SCELLS = kSwTX / 2 * TY;
+    static constexpr int SCELLS = TX / 2 * TY;
     static constexpr int VEC = 16 / sizeof(T);
     static constexpr int RXC = RX / VEC;
     static constexpr int CH = RXC * RY;
@@ -159,7 +160,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
     const int tid = threadIdx.x;
     const int n0 = v.n0, n1 = v.n1, n2 = v.n2;
     const long plane = (long)n0 * n1;
-    const int x0 = blockIdx.x * kSwTX, y0 = blockIdx.y * TY;
+    const int x0 = blockIdx.x * G::TX, y0 = blockIdx.y * TY;
     const int z0 = blockIdx.z * zc, z1 = min(z0 + zc, n2);
     const int kb = z0 - 2;   // slot of plane k in a ring of S slots: (k - kb) % S
     auto slot = [&](int k, int S) { return (k - kb) % S; };
@@ -233,8 +234,8 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
             }
         }
     }
-    const int sry = 2 + tid / (kSwTX / 2);
-    const int scol = tid % (kSwTX / 2);
+    const int sry = 2 + tid / (G::TX / 2);
+    const int scol = tid % (G::TX / 2);
     const int sgi = x0 + 2 * scol, sgj = y0 + sry - 2;
     const bool s_out = tid < G::SCELLS && sgi < n0 && sgj < n1;
     const int srl = 4 + 2 * scol + RX * sry;

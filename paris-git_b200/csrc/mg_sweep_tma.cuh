@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
     using G = Sw2<C>;
     constexpr int NT = G::NT;
     constexpr int RX = G::RX, RY = G::RY, RP = G::RP, TY = G::TY;
-    static_assert(C::D == 1, "one step of planes staged ahead");
+    static_assert(C::D == 1 && C::TX == kSwTX, "one step of planes staged ahead, 32-wide tiles");
     constexpr int NB = 2;   // groups in flight at most: one barrier each
     constexpr uint32_t BOX_BYTES = sizeof(T) * RP;
     static_assert(2 * (RX * 2) + 2 * (RY - 4) * 4 <= NT, "one ring element to wrap per thread");

@@ -65,12 +65,15 @@ __device__ inline double inter_q(const QuickCoef* __restrict__ c, double y0, dou
 
 // QUICK value of a component at its own cell centre ii along its axis
 // (work(:,:,:,d) of the component's own direction): phi at n, stride st
+// Both candidates of the upwind point are loaded before the upwind test, so
+// the four loads of a face value are independent (one memory round trip
+// instead of two); the arithmetic is unchanged.
 template <bool R>
 __device__ inline double quick_same(const double* __restrict__ phi, long n, long st, const QuickCoef* __restrict__ Q,
                                     int t) {
-    const double pm1 = phi[n - st], p0 = phi[n];
+    const double pm2 = phi[n - 2 * st], pm1 = phi[n - st], p0 = phi[n], pp1 = phi[n + st];
     const bool up = pm1 + p0 > 0.0;
-    const double y2 = phi[up ? n - 2 * st : n + st];
+    const double y2 = up ? pm2 : pp1;
     return inter_q<R>(Q + 4 * t + (up ? 0 : 1), up ? pm1 : p0, up ? p0 : pm1, y2);
 }
 // the same with the two coefficient sets of a uniform axis
@@ -79,10 +82,10 @@ __device__ inline QuickCoef pick(bool up, const QuickCoef& a, const QuickCoef& b
 }
 __device__ inline double quick_same_u(const double* __restrict__ phi, long n, long st, const QuickCoef& cu,
                                       const QuickCoef& cd) {
-    const double pm1 = phi[n - st], p0 = phi[n];
+    const double pm2 = phi[n - 2 * st], pm1 = phi[n - st], p0 = phi[n], pp1 = phi[n + st];
     const bool up = pm1 + p0 > 0.0;
     const QuickCoef c = pick(up, cu, cd);
-    return inter_q<true>(&c, up ? pm1 : p0, up ? p0 : pm1, phi[up ? n - 2 * st : n + st]);
+    return inter_q<true>(&c, up ? pm1 : p0, up ? p0 : pm1, up ? pm2 : pp1);
 }
 
 // QUICK value of a component on the face jj+1/2 of another axis, upwinded
@@ -90,17 +93,18 @@ __device__ inline double quick_same_u(const double* __restrict__ phi, long n, lo
 template <bool R>
 __device__ inline double quick_cross(const double* __restrict__ phi, const double* __restrict__ vel, long n, long st,
                                      long sc, const QuickCoef* __restrict__ Q, int t) {
-    const bool up = vel[n] + vel[n + sc] > 0.0;
-    const double a = phi[n], b = phi[n + st];
-    const double y2 = phi[up ? n - st : n + 2 * st];
-    return inter_q<R>(Q + 4 * t + (up ? 2 : 3), up ? a : b, up ? b : a, y2);
+    const double v0 = vel[n], v1 = vel[n + sc];
+    const double am = phi[n - st], a = phi[n], b = phi[n + st], bp = phi[n + 2 * st];
+    const bool up = v0 + v1 > 0.0;
+    return inter_q<R>(Q + 4 * t + (up ? 2 : 3), up ? a : b, up ? b : a, up ? am : bp);
 }
 __device__ inline double quick_cross_u(const double* __restrict__ phi, const double* __restrict__ vel, long n, long st,
                                        long sc, const QuickCoef& cu, const QuickCoef& cd) {
-    const double a = phi[n], b = phi[n + st];
-    const bool up = vel[n] + vel[n + sc] > 0.0;
+    const double v0 = vel[n], v1 = vel[n + sc];
+    const double am = phi[n - st], a = phi[n], b = phi[n + st], bp = phi[n + 2 * st];
+    const bool up = v0 + v1 > 0.0;
     const QuickCoef c = pick(up, cu, cd);
-    return inter_q<true>(&c, up ? a : b, up ? b : a, phi[up ? n - st : n + 2 * st]);
+    return inter_q<true>(&c, up ? a : b, up ? b : a, up ? am : bp);
 }
 
 // x / den, or x * (1/den) where that reciprocal is exact (same double)

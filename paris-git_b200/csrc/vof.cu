@@ -52,18 +52,19 @@ __device__ inline double courant(const SweepArgs& a, double u) {
 // directions and -1..n along d (vofnonmodule.f90:143-145 loops over is-1..ie+1;
 // only the d-neighbours of interior cells are used); flat index t over them,
 // i fastest.
-__device__ inline void flux_cell_of(const SweepArgs& a, long t, int& i, int& j, int& k) {
-    int e0 = a.L.n[0] + (a.d == 0 ? 2 : 0), e1 = a.L.n[1] + (a.d == 1 ? 2 : 0);
-    i = (int)(t % e0);
-    j = (int)((t / e0) % e1);
-    k = (int)(t / ((long)e0 * e1));
+__device__ inline void flux_cell_of(const SweepArgs& a, unsigned t, int& i, int& j, int& k) {
+    const unsigned e0 = a.L.n[0] + (a.d == 0 ? 2 : 0), e1 = a.L.n[1] + (a.d == 1 ? 2 : 0);
+    const unsigned r = t / e0;
+    i = (int)(t - r * e0);
+    k = (int)(r / e1);
+    j = (int)(r - (unsigned)k * e1);
     if (a.d == 0) i -= 1; else if (a.d == 1) j -= 1; else k -= 1;
 }
 
 // 1. the mixed flux cells, one segment per block
-__global__ void __launch_bounds__(kVofSeg) k_vof_mixed_list(const SweepArgs a, long F) {
+__global__ void __launch_bounds__(kVofSeg) k_vof_mixed_list(const SweepArgs a, unsigned F) {
     __shared__ int wcount[kVofSeg / 32];
-    const long t = blockIdx.x * (long)kVofSeg + threadIdx.x;
+    const unsigned t = blockIdx.x * (unsigned)kVofSeg + threadIdx.x;
     bool mixed = false;
     long n = 0;
     if (t < F) {
@@ -88,17 +89,38 @@ __global__ void __launch_bounds__(kVofSeg) k_vof_mixed_list(const SweepArgs a, l
 
 // 2. PLIC fluxes of the listed cells: fit_plane_new + three FL3D for swpz
 // (vofnonmodule.f90:166-186, 633-655), mycs + AL3D + two FL3D for swpr
-// (:700-727); one warp per segment
+// (:700-727).  A warp takes 32 segments at a time and works through the
+// concatenation of their entries, 32 cells per round (a segment usually
+// holds only a few mixed cells).
 __global__ void __launch_bounds__(128) k_vof_mixed_flux(const SweepArgs a) {
     const Layout& L = a.L;
     const long od = a.d == 0 ? 1 : (a.d == 1 ? L.pitch : L.plane);
     const int lane = threadIdx.x & 31;
     const long w0 = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
     const long nw = ((long)gridDim.x * blockDim.x) >> 5;
-    for (long seg = w0; seg < a.nseg; seg += nw) {
-        const int cnt = a.segn[seg];
-        for (int q = lane; q < cnt; q += 32) {
-            const long n = a.list[seg * kVofSeg + q];
+    for (long base = w0 * 32; base < a.nseg; base += nw * 32) {
+        const int cnt = base + lane < a.nseg ? a.segn[base + lane] : 0;
+        int incl = cnt;   // inclusive prefix sum over the 32 segments
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int excl = incl - cnt;
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        for (int e0 = 0; e0 < total; e0 += 32) {
+            const int e = e0 + lane;
+            // the segment of entry e: the last lane whose exclusive offset is <= e
+            int sg = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const int cand = sg + step;
+                const int off = __shfl_sync(0xffffffffu, excl, cand & 31);
+                if (cand < 32 && off <= e) sg = cand;
+            }
+            const int sgoff = __shfl_sync(0xffffffffu, excl, sg);
+            if (e >= total) continue;
+            const long n = a.list[(base + sg) * kVofSeg + (e - sgoff)];
             double cc = a.c[n];
             double a2 = courant(a, a.us[n]);
             double a1 = courant(a, a.us[n - od]);
@@ -147,21 +169,24 @@ __global__ void __launch_bounds__(128) k_vof_mixed_flux(const SweepArgs a) {
     }
 }
 
-// vof1/vof2/vof3 of one flux cell from its volume fraction cc: closed form
-// for cc == 1 (and 0 for cc <= 0), the stored PLIC flux for a mixed cell
-// (vofnonmodule.f90:155-186, :700-727)
-__device__ inline double cell_flux(const SweepArgs& a, double cc, long n, long od, int which) {
+// vof1/vof2/vof3 of one flux cell from its volume fraction cc and the
+// Courant numbers of its low and high faces: closed form for cc == 1 (and 0
+// for cc <= 0), the stored PLIC flux for a mixed cell (vofnonmodule.f90:155-186,
+// :700-727)
+__device__ inline double cell_flux(const SweepArgs& a, double cc, long n, double alo, double ahi, int which) {
     if (cc == 1.0) {
-        if (which == 1) return plic::dmax1(-courant(a, a.us[n - od]), 0.0);
-        if (which == 3) return plic::dmax1(courant(a, a.us[n]), 0.0);
-        return 1.0 - plic::dmax1(courant(a, a.us[n - od]), 0.0) + plic::dmin1(courant(a, a.us[n]), 0.0);
+        if (which == 1) return plic::dmax1(-alo, 0.0);
+        if (which == 3) return plic::dmax1(ahi, 0.0);
+        return 1.0 - plic::dmax1(alo, 0.0) + plic::dmin1(ahi, 0.0);
     }
     if (cc > 0.0) return which == 1 ? a.v1[n] : (which == 2 ? a.v2[n] : a.v3[n]);
     return 0.0;
 }
 
 // 3. the update of the interior: new c, clipping (swpz :224-230 / swpr
-// :731-745 and get_flags_and_clip) and the flag, into the second buffer
+// :731-745 and get_flags_and_clip) and the flag, into the second buffer.
+// The three volume fractions and the two face velocities the fluxes need
+// (faces n - od and n) are loaded together, before any test on them.
 __global__ void k_vof_update(const SweepArgs a) {
     int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
     const Layout& L = a.L;
@@ -169,15 +194,17 @@ __global__ void k_vof_update(const SweepArgs a) {
     const long od = a.d == 0 ? 1 : (a.d == 1 ? L.pitch : L.plane);
     const long n = lidx(L, i, j, k);
     const double cm = a.c[n - od], c0 = a.c[n], cp = a.c[n + od];
+    const double um = a.us[n - od], u0 = a.us[n];
+    const double a1 = courant(a, um), a2 = courant(a, u0);
     double cnew;
     if (!a.wy) {
-        cnew = cell_flux(a, cm, n - od, od, 3) + cell_flux(a, c0, n, od, 2) + cell_flux(a, cp, n + od, od, 1);
+        // vof3 of n-od needs only its high face (n-od), vof1 of n+od only its low face (n)
+        cnew = cell_flux(a, cm, n - od, 0.0, a1, 3) + cell_flux(a, c0, n, a1, a2, 2) +
+               cell_flux(a, cp, n + od, a2, 0.0, 1);
         cnew = plic::dmax1(0.0, plic::dmin1(1.0, cnew));
     } else {
-        double a2 = courant(a, a.us[n]);
-        double a1 = courant(a, a.us[n - od]);
-        cnew = c0 - (cell_flux(a, c0, n, od, 3) - cell_flux(a, cp, n + od, od, 1)) +
-               (cell_flux(a, cm, n - od, od, 3) - cell_flux(a, c0, n, od, 1)) + (double)a.cg[n] * (a2 - a1);
+        cnew = c0 - (cell_flux(a, c0, n, a1, a2, 3) - cell_flux(a, cp, n + od, a2, 0.0, 1)) +
+               (cell_flux(a, cm, n - od, 0.0, a1, 3) - cell_flux(a, c0, n, a1, a2, 1)) + (double)a.cg[n] * (a2 - a1);
         if (cnew < a.epsc) cnew = 0.0;
         else if (cnew > 1.0 - a.epsc) cnew = 1.0;
     }
@@ -265,7 +292,7 @@ int vof_sweep_dir(paris_ctx* c, int d, double dt, const double* src, double* dst
     a.epsc = c->d.epsc;
     const long F = (long)(L.n[0] + (d == 0 ? 2 : 0)) * (L.n[1] + (d == 1 ? 2 : 0)) * (L.n[2] + (d == 2 ? 2 : 0));
     a.nseg = (F + kVofSeg - 1) / kVofSeg;
-    PARIS_LAUNCH_N(c, "vof_mixed_list", F, k_vof_mixed_list, (unsigned)a.nseg, kVofSeg, 0, a, F);
+    PARIS_LAUNCH_N(c, "vof_mixed_list", F, k_vof_mixed_list, (unsigned)a.nseg, kVofSeg, 0, a, (unsigned)F);
     PARIS_LAUNCH_N(c, "vof_mixed_flux", 0L, k_vof_mixed_flux, c->nsm * 16, 128, 0, a);
     PARIS_LAUNCH_N(c, "vof_sweep", c->N, k_vof_update, dim3(div_up(L.n[0], 128), L.n[1], L.n[2]), 128, 0, a);
     long G = ghost_count(c->L);

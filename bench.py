@@ -577,7 +577,7 @@ def run_b200(args, dist):
                                  ALGO_BYTES[top["kernel"]] if top["kernel"] in NCU_DRAM_BYTES_PER_CELL else None),
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                      "algo_bytes_per_launch": top["algo_bytes_per_launch"]},
-        "kernels": rows[:12],
+        "kernels": rows[:20],
         "clocks": clk,
         "e2e": e2e,
         "cpu_baseline": cpu,

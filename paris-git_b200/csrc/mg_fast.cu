@@ -614,45 +614,6 @@ static int fast_coefs(paris_ctx* c) {
 
 // Planes per block of the fused sweep: enough blocks for one wave of resident
 // blocks, at least 4 planes per block.
-template <class Cfg>
-static int sweep_chunk_cfg(paris_ctx* c, const int n[3]) {
-    static int per_sm = 0;   // resident blocks per SM (the same on every B200)
-    if (!per_sm) {
-        cudaFuncSetAttribute(k_rb_sweep2_cfg<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sweep2_smem_cfg<Cfg>());
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rb_sweep2_cfg<Cfg>, Cfg::NT,
-                                                          sweep2_smem_cfg<Cfg>()) != cudaSuccess || per_sm < 1)
-            per_sm = 1;
-    }
-    long tiles = (long)div_up(n[0], Cfg::TX) * div_up(n[1], Cfg::TY);
-    long nbz = (long)per_sm * c->nsm / tiles;
-    long cap = n[2] / 4;
-    if (nbz > cap) nbz = cap;
-    if (nbz < 1) nbz = 1;
-    return (int)div_up(n[2], nbz);
-}
-
-template <class Cfg>
-static int launch_sweep_cfg(paris_ctx* c, const char* label, const FastLevel<typename Cfg::type>& l,
-                            const typename Cfg::type* xin, typename Cfg::type* xout, const typename Cfg::type* xc,
-                            int first) {
-    const int zc = sweep_chunk_cfg<Cfg>(c, l.n);
-    dim3 grid(div_up(l.n[0], Cfg::TX), div_up(l.n[1], Cfg::TY), div_up(l.n[2], zc));
-    PARIS_LAUNCH_N(c, label, l.N, k_rb_sweep2_cfg<Cfg>, grid, Cfg::NT, sweep2_smem_cfg<Cfg>(), view(l), xin, xout,
-                   xc, c->bnd, first, zc);
-    return PARIS_OK;
-}
-
-// FP32 sweep shapes (tile TX x TY, steps staged ahead D, threads, blocks per
-// SM); PARIS_SWEEP_SHAPE selects one for a timing comparison
-using SwShape1 = SwCfg<float, 16, 2, 640, 1, 64>;
-using SwShape2 = SwCfg<float, 16, 2, 320, 1, 32>;
-using SwShape3 = SwCfg<float, 32, 2, 640, 1, 32>;
-static int sweep_shape() {
-    const char* e = getenv("PARIS_SWEEP_SHAPE");
-    return e ? atoi(e) : 0;
-}
-
 template <typename T>
 static int sweep_chunk(paris_ctx* c, const FastLevel<T>& l) {
     using Cfg = typename SwGeo<T>::Cfg;
@@ -706,12 +667,6 @@ static int sweep_fused(paris_ctx* c, int L, const FastLevel<T>& l, const T* xin,
                            view(l), xin, M, xout, xc, c->bnd, first, zc, c->err_dev);
             return PARIS_OK;
         }
-    }
-    if constexpr (std::is_same<T, float>::value) {
-        const int sh = sweep_shape();
-        if (sh == 1 && l.n[0] % 4 == 0) return launch_sweep_cfg<SwShape1>(c, kname<T>(label), l, xin, xout, xc, first);
-        if (sh == 2) return launch_sweep_cfg<SwShape2>(c, kname<T>(label), l, xin, xout, xc, first);
-        if (sh == 3) return launch_sweep_cfg<SwShape3>(c, kname<T>(label), l, xin, xout, xc, first);
     }
     int zc = sweep_chunk<T>(c, l);
     dim3 grid(div_up(l.n[0], Cfg::TX), div_up(l.n[1], Cfg::TY), div_up(l.n[2], zc));

@@ -40,7 +40,9 @@ struct SweepArgs {
     double epsc;
 };
 
-static constexpr int kVofSeg = 256;   // flux cells per block of the list kernel
+static constexpr int kVofListThreads = 256;
+static constexpr int kVofPer = 4;                               // flux cells per thread of the list kernel
+static constexpr int kVofSeg = kVofListThreads * kVofPer;       // flux cells per block (one list segment)
 
 // a = u dt / dxyz, the Courant number of a face (vofnonmodule.f90:147-148,
 // 686-687): the same double as the division when 1/dxyz is exact
@@ -61,29 +63,45 @@ __device__ inline void flux_cell_of(const SweepArgs& a, unsigned t, int& i, int&
     if (a.d == 0) i -= 1; else if (a.d == 1) j -= 1; else k -= 1;
 }
 
-// 1. the mixed flux cells, one segment per block
-__global__ void __launch_bounds__(kVofSeg) k_vof_mixed_list(const SweepArgs a, unsigned F) {
-    __shared__ int wcount[kVofSeg / 32];
-    const unsigned t = blockIdx.x * (unsigned)kVofSeg + threadIdx.x;
-    bool mixed = false;
-    long n = 0;
-    if (t < F) {
-        int i, j, k;
-        flux_cell_of(a, t, i, j, k);
-        n = lidx(a.L, i, j, k);
-        const double cc = a.c[n];
-        mixed = cc > 0.0 && cc != 1.0;
-    }
-    const unsigned m = __ballot_sync(0xffffffffu, mixed);
+// 1. the mixed flux cells, one segment per block; each thread loads its
+// kVofPer cells (strided by the block size, so the loads coalesce) before
+// testing them
+__global__ void __launch_bounds__(kVofListThreads) k_vof_mixed_list(const SweepArgs a, unsigned F) {
+    __shared__ int wcount[kVofPer][kVofListThreads / 32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (lane == 0) wcount[w] = __popc(m);
-    __syncthreads();
-    int base = 0, total = 0;
-    for (int q = 0; q < kVofSeg / 32; q++) {
-        if (q < w) base += wcount[q];
-        total += wcount[q];
+    long n[kVofPer];
+    double cc[kVofPer];
+#pragma unroll
+    for (int q = 0; q < kVofPer; q++) {
+        const unsigned t = blockIdx.x * (unsigned)kVofSeg + q * kVofListThreads + threadIdx.x;
+        n[q] = -1;
+        if (t < F) {
+            int i, j, k;
+            flux_cell_of(a, t, i, j, k);
+            n[q] = lidx(a.L, i, j, k);
+        }
     }
-    if (mixed) a.list[blockIdx.x * (long)kVofSeg + base + __popc(m & ((1u << lane) - 1u))] = n;
+#pragma unroll
+    for (int q = 0; q < kVofPer; q++) cc[q] = n[q] >= 0 ? a.c[n[q]] : 0.0;
+    unsigned m[kVofPer];
+#pragma unroll
+    for (int q = 0; q < kVofPer; q++) {
+        m[q] = __ballot_sync(0xffffffffu, cc[q] > 0.0 && cc[q] != 1.0);
+        if (lane == 0) wcount[q][w] = __popc(m[q]);
+    }
+    __syncthreads();
+    // the block's mixed cells in the order (q, warp, lane)
+    int base[kVofPer], total = 0;
+#pragma unroll
+    for (int q = 0; q < kVofPer; q++)
+        for (int v = 0; v < kVofListThreads / 32; v++) {
+            if (v == w) base[q] = total;
+            total += wcount[q][v];
+        }
+    const long seg0 = blockIdx.x * (long)kVofSeg;
+#pragma unroll
+    for (int q = 0; q < kVofPer; q++)
+        if ((m[q] >> lane) & 1u) a.list[seg0 + base[q] + __popc(m[q] & ((1u << lane) - 1u))] = n[q];
     if (threadIdx.x == 0) a.segn[blockIdx.x] = total;
 }
 
@@ -292,11 +310,13 @@ int vof_sweep_dir(paris_ctx* c, int d, double dt, const double* src, double* dst
     a.epsc = c->d.epsc;
     const long F = (long)(L.n[0] + (d == 0 ? 2 : 0)) * (L.n[1] + (d == 1 ? 2 : 0)) * (L.n[2] + (d == 2 ? 2 : 0));
     a.nseg = (F + kVofSeg - 1) / kVofSeg;
-    PARIS_LAUNCH_N(c, "vof_mixed_list", F, k_vof_mixed_list, (unsigned)a.nseg, kVofSeg, 0, a, (unsigned)F);
-    PARIS_LAUNCH_N(c, "vof_mixed_flux", 0L, k_vof_mixed_flux, c->nsm * 16, 128, 0, a);
+    // the four kernels of a direction share the profile label "vof_sweep",
+    // with the direction's cells counted once (on the update)
+    PARIS_LAUNCH_N(c, "vof_sweep", 0L, k_vof_mixed_list, (unsigned)a.nseg, kVofListThreads, 0, a, (unsigned)F);
+    PARIS_LAUNCH_N(c, "vof_sweep", 0L, k_vof_mixed_flux, c->nsm * 16, 128, 0, a);
     PARIS_LAUNCH_N(c, "vof_sweep", c->N, k_vof_update, dim3(div_up(L.n[0], 128), L.n[1], L.n[2]), 128, 0, a);
     long G = ghost_count(c->L);
-    PARIS_LAUNCH_N(c, "vof_ghosts", G, k_vof_ghosts, div_up(G, 256), 256, 0, dst, src, flag, c->L, c->bnd,
+    PARIS_LAUNCH_N(c, "vof_sweep", 0L, k_vof_ghosts, div_up(G, 256), 256, 0, dst, src, flag, c->L, c->bnd,
                    ctx_vof_jet(c), G, c->d.epsc);
     return PARIS_OK;
 }

@@ -76,30 +76,3 @@ def test_tma_sweep_matches_cp_async(gpu_lib, capi, runtime, orc, workloads, n, b
     assert r_tma.rel_res == r_cpa.rel_res
     assert np.array_equal(p_tma, p_cpa)
 
-
-def _solve_shape(runtime, capi, desc, cvof, vel, shape):
-    old = os.environ.get("PARIS_SWEEP_SHAPE")
-    os.environ["PARIS_SWEEP_SHAPE"] = str(shape)
-    try:
-        return _solve(runtime, capi, desc, cvof, vel, False, 1)
-    finally:
-        if old is None:
-            del os.environ["PARIS_SWEEP_SHAPE"]
-        else:
-            os.environ["PARIS_SWEEP_SHAPE"] = old
-
-
-@pytest.mark.parametrize("shape", [1, 2, 3])
-@pytest.mark.parametrize("n,bc", [((64, 64, 64), "periodic"), ((128, 64, 64), (1, 0, 1, 1, 0, 1)),
-                                  ((64, 128, 64), (0, 1, 0, 0, 1, 0))])
-def test_sweep_shapes_agree(gpu_lib, capi, runtime, orc, workloads, n, bc, shape):
-    """Every tile shape of the fused sweep computes the same cells from the same
-    values, so the solves agree to the bit."""
-    desc, cvof, vel = _problem(capi, orc, workloads, n, bc, seed=6)
-    import warnings
-    with warnings.catch_warnings():
-        warnings.simplefilter("ignore")
-        p0, r0 = _solve_shape(runtime, capi, desc, cvof, vel, 0)
-        p1, r1 = _solve_shape(runtime, capi, desc, cvof, vel, shape)
-    assert r0.it == r1.it and r0.rel_res == r1.rel_res
-    assert np.array_equal(p0, p1)

@@ -172,6 +172,64 @@ static inline dim3 row_grid(long n0, int n1, int n2) { return dim3(div_up(n0, 12
 #include "mg_sweep.cuh"
 #include "mg_sweep_tma.cuh"
 
+// 32-bit forms of smooth_cell / resid_cell / restrict_cell for the levels of
+// the single-block coarse cycle (at most a few thousand cells): the same
+// operations on the same values, with int instead of long index arithmetic.
+template <typename T>
+__device__ inline void nbrs32(const LV<T>& v, const T* x, const Bnd& B, int i, int j, int k, int m, T& a1, T& a3,
+                              T& a5, T& xw, T& xe, T& xs, T& xn, T& xb, T& xt) {
+    const int n0 = v.n0, n1 = v.n1, n2 = v.n2, sy = n0, sz = n0 * n1;
+    a1 = i > 0 ? v.cx[m - 1] : (B.per[0] ? v.cx[m + n0 - 1] : (T)0);
+    a3 = j > 0 ? v.cy[m - sy] : (B.per[1] ? v.cy[m + sy * (n1 - 1)] : (T)0);
+    a5 = k > 0 ? v.cz[m - sz] : (B.per[2] ? v.cz[m + sz * (n2 - 1)] : (T)0);
+    xw = i > 0 ? x[m - 1] : (B.per[0] ? x[m + n0 - 1] : (T)0);
+    xe = i < n0 - 1 ? x[m + 1] : (B.per[0] ? x[m - (n0 - 1)] : (T)0);
+    xs = j > 0 ? x[m - sy] : (B.per[1] ? x[m + sy * (n1 - 1)] : (T)0);
+    xn = j < n1 - 1 ? x[m + sy] : (B.per[1] ? x[m - sy * (n1 - 1)] : (T)0);
+    xb = k > 0 ? x[m - sz] : (B.per[2] ? x[m + sz * (n2 - 1)] : (T)0);
+    xt = k < n2 - 1 ? x[m + sz] : (B.per[2] ? x[m - sz * (n2 - 1)] : (T)0);
+}
+
+template <typename T>
+__device__ inline void smooth_cell32(const LV<T>& v, const Bnd& B, int i, int j, int k) {
+    const int m = i + v.n0 * (j + v.n1 * k);
+    T a1, a3, a5, xw, xe, xs, xn, xb, xt;
+    nbrs32(v, v.x, B, i, j, k, m, a1, a3, a5, xw, xe, xs, xn, xb, xt);
+    T a2 = v.cx[m], a4 = v.cy[m], a6 = v.cz[m];
+    T d = a1 + a2 + a3 + a4 + a5 + a6;
+    T s = a1 * xw + a2 * xe + a3 * xs + a4 * xn + a5 * xb + a6 * xt + v.b[m];
+    if (d > (T)0) v.x[m] = s / d;
+}
+
+template <typename T>
+__device__ inline T resid_cell32(const LV<T>& v, const Bnd& B, int i, int j, int k) {
+    const int m = i + v.n0 * (j + v.n1 * k);
+    T a1, a3, a5, xw, xe, xs, xn, xb, xt;
+    nbrs32(v, v.x, B, i, j, k, m, a1, a3, a5, xw, xe, xs, xn, xb, xt);
+    T a2 = v.cx[m], a4 = v.cy[m], a6 = v.cz[m];
+    T d = a1 + a2 + a3 + a4 + a5 + a6;
+    return v.b[m] - d * v.x[m] + a1 * xw + a2 * xe + a3 * xs + a4 * xn + a5 * xb + a6 * xt;
+}
+
+template <typename T>
+__device__ inline void restrict_cell32(const LV<T>& f, const LV<T>& c, const Bnd& B, int i, int j, int k) {
+    T s = 0;
+    for (int dk = 0; dk < 2; dk++)
+        for (int dj = 0; dj < 2; dj++)
+            for (int di = 0; di < 2; di++) s += resid_cell32(f, B, 2 * i + di, 2 * j + dj, 2 * k + dk);
+    c.b[i + c.n0 * (j + c.n1 * k)] = (T)0.125 * s;
+}
+
+// t / d for 0 <= t, d < 2^22 (exact): a float estimate within one of the
+// quotient, corrected
+__device__ inline int div_small(int t, int d, float rd) {
+    int q = __float2int_rz((float)t * rd);
+    const int r = t - q * d;
+    if (r < 0) q--;
+    else if (r >= d) q++;
+    return q;
+}
+
 // The V-cycle from level L0 down to the coarsest, in one block, on copies of
 // those levels in shared memory: the coefficients of every level and the
 // right-hand side of level L0 are loaded, the cycle runs, and the iterate of
@@ -218,11 +276,12 @@ __global__ void __launch_bounds__(1024) k_fast_coarse_cycle(const LVSet<T> G, in
         const int t0 = warp ? lane : tid, st = warp ? 32 : nt;
         const int h0 = (v.n0 + 1) >> 1, hn = h0 * v.n1;
         const int tot = hn * v.n2;
+        const float rhn = 1.0f / (float)hn, rh0 = 1.0f / (float)h0;
         for (int t = t0; t < tot; t += st) {
-            int k = t / hn, r = t - k * hn;
-            int j = r / h0, ih = r - j * h0;
+            int k = div_small(t, hn, rhn), r = t - k * hn;
+            int j = div_small(r, h0, rh0), ih = r - j * h0;
             int i = 2 * ih + ((j + k + color) & 1);
-            if (i < v.n0) smooth_cell(v, B, i, j, k);
+            if (i < v.n0) smooth_cell32(v, B, i, j, k);
         }
         if (warp) __syncwarp();
         else __syncthreads();
@@ -241,10 +300,11 @@ __global__ void __launch_bounds__(1024) k_fast_coarse_cycle(const LVSet<T> G, in
         for (int s = 0; s < nu1; s++) { smooth(v, 0, warp); smooth(v, 1, warp); }
         const LV<T> c = S[L + 1];
         const int cn = c.n0 * c.n1;
+        const float rcn = 1.0f / (float)cn, rc0 = 1.0f / (float)c.n0;
         for (int t = t0; t < (int)c.N; t += st) {
-            int k = t / cn, r = t - k * cn;
-            int j = r / c.n0, i = r - j * c.n0;
-            restrict_cell(v, c, B, i, j, k);
+            int k = div_small(t, cn, rcn), r = t - k * cn;
+            int j = div_small(r, c.n0, rc0), i = r - j * c.n0;
+            restrict_cell32(v, c, B, i, j, k);
         }
         if (warp) __syncwarp();
         else __syncthreads();
@@ -253,10 +313,11 @@ __global__ void __launch_bounds__(1024) k_fast_coarse_cycle(const LVSet<T> G, in
         const int t0 = warp ? lane : tid, st = warp ? 32 : nt;
         const LV<T> v = S[L], c = S[L + 1];
         const int fn = v.n0 * v.n1;
+        const float rfn = 1.0f / (float)fn, rf0 = 1.0f / (float)v.n0;
         for (int t = t0; t < (int)v.N; t += st) {
-            int k = t / fn, r = t - k * fn;
-            int j = r / v.n0, i = r - j * v.n0;
-            v.x[t] += c.x[cidx(c.n0, c.n1, i >> 1, j >> 1, k >> 1)];
+            int k = div_small(t, fn, rfn), r = t - k * fn;
+            int j = div_small(r, v.n0, rf0), i = r - j * v.n0;
+            v.x[t] += c.x[(i >> 1) + c.n0 * ((j >> 1) + c.n1 * (k >> 1))];
         }
         if (warp) __syncwarp();
         else __syncthreads();

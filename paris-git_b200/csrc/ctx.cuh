@@ -50,8 +50,9 @@ struct paris_ctx {
     double* height = nullptr;      // 6 ghosted fields
     int8_t* kflag = nullptr;       // kappaflag of the curvature passes
     double* vflux = nullptr;       // VOF sweeps: vof1/vof2/vof3 of the mixed cells (3 ghosted arrays, sparse)
-    long* mixlist = nullptr;       // the mixed flux cells of the current sweep, in per-block segments
-    int* mixsegn = nullptr;        // mixed cells per segment
+    long* mixlist = nullptr;       // the mixed flux cells of the current sweep
+    int* mixsegn = nullptr;        // their number
+    long mixcap = 0;               // room in mixlist
     int* st_list = nullptr;        // interior mixed cells of the curvature passes
     int* st_count = nullptr;
     int* debris_count = nullptr;   // cells cleaned by a sweep of clean_debris method 3

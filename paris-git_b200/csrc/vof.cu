@@ -6,12 +6,12 @@
 // ls2vof_refined (:1195-1293).  Built with -fmad=false.
 //
 // Three kernels per split direction:
-//  1. the mixed flux cells (0 < c < 1), listed without atomics: each block of
-//     256 flux cells writes its mixed cells into its own segment of the list
-//     and their number into a per-block count;
-//  2. the PLIC fluxes of the listed cells, one warp per segment (so that the
-//     geometry runs without divergence against the full and empty cells),
-//     stored in sparse flux arrays;
+//  1. the mixed flux cells (0 < c < 1) as one dense list: each block of 1024
+//     flux cells counts its mixed cells, takes room for them with a single
+//     atomic add, and writes them there;
+//  2. the PLIC fluxes of the listed cells, every lane a listed cell (so that
+//     the geometry runs without divergence against the full and empty
+//     cells), stored in sparse flux arrays;
 //  3. the update: the new, clipped volume fraction and its flag from the
 //     fluxes of each cell and its two neighbours along the sweep (closed form
 //     for full cells, the stored fluxes for mixed ones), into the second
@@ -29,9 +29,9 @@ struct SweepArgs {
     const double* us;    // face velocity of the sweep direction
     const uint8_t* cg;   // c_mask (WY)
     double *v1, *v2, *v3;   // fluxes of the mixed cells (ghosted arrays, sparse)
-    long* list;          // layout indices of the mixed flux cells, kVofSeg per segment
-    int* segn;           // mixed cells per segment
-    long nseg;           // segments (blocks of the list kernel)
+    long* list;          // layout indices of the mixed flux cells
+    int* count;          // their number
+    long cap;            // room in the list
     Layout L;
     int d;               // 0,1,2
     int wy;              // 1: swpr
@@ -42,7 +42,7 @@ struct SweepArgs {
 
 static constexpr int kVofListThreads = 256;
 static constexpr int kVofPer = 4;                               // flux cells per thread of the list kernel
-static constexpr int kVofSeg = kVofListThreads * kVofPer;       // flux cells per block (one list segment)
+static constexpr int kVofSeg = kVofListThreads * kVofPer;       // flux cells per block of the list kernel
 
 // a = u dt / dxyz, the Courant number of a face (vofnonmodule.f90:147-148,
 // 686-687): the same double as the division when 1/dxyz is exact
@@ -63,11 +63,12 @@ __device__ inline void flux_cell_of(const SweepArgs& a, unsigned t, int& i, int&
     if (a.d == 0) i -= 1; else if (a.d == 1) j -= 1; else k -= 1;
 }
 
-// 1. the mixed flux cells, one segment per block; each thread loads its
-// kVofPer cells (strided by the block size, so the loads coalesce) before
-// testing them
+// 1. the mixed flux cells, kVofSeg per block; each thread loads its kVofPer
+// cells (strided by the block size, so the loads coalesce) before testing
+// them, and the block appends its mixed cells with one atomic add
 __global__ void __launch_bounds__(kVofListThreads) k_vof_mixed_list(const SweepArgs a, unsigned F) {
     __shared__ int wcount[kVofPer][kVofListThreads / 32];
+    __shared__ int room;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     long n[kVofPer];
     double cc[kVofPer];
@@ -98,92 +99,71 @@ __global__ void __launch_bounds__(kVofListThreads) k_vof_mixed_list(const SweepA
             if (v == w) base[q] = total;
             total += wcount[q][v];
         }
-    const long seg0 = blockIdx.x * (long)kVofSeg;
+    if (total == 0) return;
+    if (threadIdx.x == 0) room = atomicAdd(a.count, total);
+    __syncthreads();
 #pragma unroll
     for (int q = 0; q < kVofPer; q++)
-        if ((m[q] >> lane) & 1u) a.list[seg0 + base[q] + __popc(m[q] & ((1u << lane) - 1u))] = n[q];
-    if (threadIdx.x == 0) a.segn[blockIdx.x] = total;
+        if ((m[q] >> lane) & 1u) {
+            const long e = (long)room + base[q] + __popc(m[q] & ((1u << lane) - 1u));
+            if (e < a.cap) a.list[e] = n[q];
+        }
 }
 
 // 2. PLIC fluxes of the listed cells: fit_plane_new + three FL3D for swpz
 // (vofnonmodule.f90:166-186, 633-655), mycs + AL3D + two FL3D for swpr
-// (:700-727).  A warp takes 32 segments at a time and works through the
-// concatenation of their entries, 32 cells per round (a segment usually
-// holds only a few mixed cells).
+// (:700-727)
 __global__ void __launch_bounds__(128) k_vof_mixed_flux(const SweepArgs a) {
     const Layout& L = a.L;
     const long od = a.d == 0 ? 1 : (a.d == 1 ? L.pitch : L.plane);
-    const int lane = threadIdx.x & 31;
-    const long w0 = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
-    const long nw = ((long)gridDim.x * blockDim.x) >> 5;
-    for (long base = w0 * 32; base < a.nseg; base += nw * 32) {
-        const int cnt = base + lane < a.nseg ? a.segn[base + lane] : 0;
-        int incl = cnt;   // inclusive prefix sum over the 32 segments
+    long cnt = *a.count;
+    if (cnt > a.cap) cnt = a.cap;
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < cnt; q += (long)gridDim.x * blockDim.x) {
+        const long n = a.list[q];
+        double cc = a.c[n];
+        double a2 = courant(a, a.us[n]);
+        double a1 = courant(a, a.us[n - od]);
+        double st[27];
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += v;
-        }
-        const int excl = incl - cnt;
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
-        for (int e0 = 0; e0 < total; e0 += 32) {
-            const int e = e0 + lane;
-            // the segment of entry e: the last lane whose exclusive offset is <= e
-            int sg = 0;
+        for (int k1 = -1; k1 <= 1; k1++)
 #pragma unroll
-            for (int step = 16; step > 0; step >>= 1) {
-                const int cand = sg + step;
-                const int off = __shfl_sync(0xffffffffu, excl, cand & 31);
-                if (cand < 32 && off <= e) sg = cand;
-            }
-            const int sgoff = __shfl_sync(0xffffffffu, excl, sg);
-            if (e >= total) continue;
-            const long n = a.list[(base + sg) * kVofSeg + (e - sgoff)];
-            double cc = a.c[n];
-            double a2 = courant(a, a.us[n]);
-            double a1 = courant(a, a.us[n - od]);
-            double st[27];
+            for (int j1 = -1; j1 <= 1; j1++)
 #pragma unroll
-            for (int k1 = -1; k1 <= 1; k1++)
-#pragma unroll
-                for (int j1 = -1; j1 <= 1; j1++)
-#pragma unroll
-                    for (int i1 = -1; i1 <= 1; i1++)
-                        st[(i1 + 1) + 3 * (j1 + 1) + 9 * (k1 + 1)] = a.c[n + i1 + j1 * L.pitch + k1 * L.plane];
-            double m[3], x0[3] = {0.0, 0.0, 0.0}, dx[3] = {1.0, 1.0, 1.0};
-            plic::mycs(st, m);
-            double f1 = 0.0, f2 = 0.0, f3 = 0.0;
-            if (!a.wy) {
-                if (!(m[0] == 0.0 && m[1] == 0.0 && m[2] == 0.0)) {
-                    double alpha = plic::al3d(m, cc);
-                    m[a.d] = m[a.d] / (1.0 - a1 + a2);
-                    alpha = alpha + m[a.d] * a1;
-                    double mm1 = plic::dmax1(a1, 0.0);
-                    double mm2 = 1.0 - mm1 + plic::dmin1(0.0, a2);
-                    if (a1 < 0.0) {
-                        x0[a.d] = a1; dx[a.d] = -a1;
-                        f1 = plic::fl3d(m, alpha, x0, dx);
-                    }
-                    if (a2 > 0.0) {
-                        x0[a.d] = 1.0; dx[a.d] = a2;
-                        f3 = plic::fl3d(m, alpha, x0, dx);
-                    }
-                    x0[a.d] = mm1; dx[a.d] = mm2;
-                    f2 = plic::fl3d(m, alpha, x0, dx);
-                }
-            } else {
+                for (int i1 = -1; i1 <= 1; i1++)
+                    st[(i1 + 1) + 3 * (j1 + 1) + 9 * (k1 + 1)] = a.c[n + i1 + j1 * L.pitch + k1 * L.plane];
+        double m[3], x0[3] = {0.0, 0.0, 0.0}, dx[3] = {1.0, 1.0, 1.0};
+        plic::mycs(st, m);
+        double f1 = 0.0, f2 = 0.0, f3 = 0.0;
+        if (!a.wy) {
+            if (!(m[0] == 0.0 && m[1] == 0.0 && m[2] == 0.0)) {
                 double alpha = plic::al3d(m, cc);
+                m[a.d] = m[a.d] / (1.0 - a1 + a2);
+                alpha = alpha + m[a.d] * a1;
+                double mm1 = plic::dmax1(a1, 0.0);
+                double mm2 = 1.0 - mm1 + plic::dmin1(0.0, a2);
                 if (a1 < 0.0) {
-                    dx[a.d] = -a1;
+                    x0[a.d] = a1; dx[a.d] = -a1;
                     f1 = plic::fl3d(m, alpha, x0, dx);
                 }
                 if (a2 > 0.0) {
-                    x0[a.d] = 1.0 - a2; dx[a.d] = a2;
+                    x0[a.d] = 1.0; dx[a.d] = a2;
                     f3 = plic::fl3d(m, alpha, x0, dx);
                 }
+                x0[a.d] = mm1; dx[a.d] = mm2;
+                f2 = plic::fl3d(m, alpha, x0, dx);
             }
-            a.v1[n] = f1; a.v2[n] = f2; a.v3[n] = f3;
+        } else {
+            double alpha = plic::al3d(m, cc);
+            if (a1 < 0.0) {
+                dx[a.d] = -a1;
+                f1 = plic::fl3d(m, alpha, x0, dx);
+            }
+            if (a2 > 0.0) {
+                x0[a.d] = 1.0 - a2; dx[a.d] = a2;
+                f3 = plic::fl3d(m, alpha, x0, dx);
+            }
         }
+        a.v1[n] = f1; a.v2[n] = f2; a.v3[n] = f3;
     }
 }
 
@@ -203,35 +183,48 @@ __device__ inline double cell_flux(const SweepArgs& a, double cc, long n, double
 
 // 3. the update of the interior: new c, clipping (swpz :224-230 / swpr
 // :731-745 and get_flags_and_clip) and the flag, into the second buffer.
-// The three volume fractions and the two face velocities the fluxes need
-// (faces n - od and n) are loaded together, before any test on them.
-__global__ void k_vof_update(const SweepArgs a) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+// Each thread updates kVofUpd cells of a row, kVofUpdThreads apart; the
+// volume fractions and face velocities of all of them are loaded before any
+// test on them, so their loads are in flight together.
+static constexpr int kVofUpdThreads = 128, kVofUpd = 2;
+__global__ void __launch_bounds__(kVofUpdThreads) k_vof_update(const SweepArgs a) {
+    const int j = blockIdx.y, k = blockIdx.z;
     const Layout& L = a.L;
-    if (i >= L.n[0]) return;
     const long od = a.d == 0 ? 1 : (a.d == 1 ? L.pitch : L.plane);
-    const long n = lidx(L, i, j, k);
-    const double cm = a.c[n - od], c0 = a.c[n], cp = a.c[n + od];
-    const double um = a.us[n - od], u0 = a.us[n];
-    const double a1 = courant(a, um), a2 = courant(a, u0);
-    double cnew;
-    if (!a.wy) {
-        // vof3 of n-od needs only its high face (n-od), vof1 of n+od only its low face (n)
-        cnew = cell_flux(a, cm, n - od, 0.0, a1, 3) + cell_flux(a, c0, n, a1, a2, 2) +
-               cell_flux(a, cp, n + od, a2, 0.0, 1);
-        cnew = plic::dmax1(0.0, plic::dmin1(1.0, cnew));
-    } else {
-        cnew = c0 - (cell_flux(a, c0, n, a1, a2, 3) - cell_flux(a, cp, n + od, a2, 0.0, 1)) +
-               (cell_flux(a, cm, n - od, 0.0, a1, 3) - cell_flux(a, c0, n, a1, a2, 1)) + (double)a.cg[n] * (a2 - a1);
-        if (cnew < a.epsc) cnew = 0.0;
-        else if (cnew > 1.0 - a.epsc) cnew = 1.0;
+    const int i0 = blockIdx.x * (kVofUpdThreads * kVofUpd) + threadIdx.x;
+    double cm[kVofUpd], c0[kVofUpd], cp[kVofUpd], um[kVofUpd], u0[kVofUpd];
+    long n[kVofUpd];
+#pragma unroll
+    for (int q = 0; q < kVofUpd; q++) {
+        const int i = i0 + q * kVofUpdThreads;
+        n[q] = lidx(L, i < L.n[0] ? i : L.n[0] - 1, j, k);
+        cm[q] = a.c[n[q] - od]; c0[q] = a.c[n[q]]; cp[q] = a.c[n[q] + od];
+        um[q] = a.us[n[q] - od]; u0[q] = a.us[n[q]];
     }
-    int8_t fl;
-    if (cnew <= a.epsc) { fl = 0; cnew = 0.0; }
-    else if (cnew >= 1.0 - a.epsc) { fl = 1; cnew = 1.0; }
-    else fl = 2;
-    a.cn[n] = cnew;
-    a.flag[n] = fl;
+#pragma unroll
+    for (int q = 0; q < kVofUpd; q++) {
+        if (i0 + q * kVofUpdThreads >= L.n[0]) continue;
+        const double a1 = courant(a, um[q]), a2 = courant(a, u0[q]);
+        double cnew;
+        if (!a.wy) {
+            // vof3 of n-od needs only its high face (n-od), vof1 of n+od only its low face (n)
+            cnew = cell_flux(a, cm[q], n[q] - od, 0.0, a1, 3) + cell_flux(a, c0[q], n[q], a1, a2, 2) +
+                   cell_flux(a, cp[q], n[q] + od, a2, 0.0, 1);
+            cnew = plic::dmax1(0.0, plic::dmin1(1.0, cnew));
+        } else {
+            cnew = c0[q] - (cell_flux(a, c0[q], n[q], a1, a2, 3) - cell_flux(a, cp[q], n[q] + od, a2, 0.0, 1)) +
+                   (cell_flux(a, cm[q], n[q] - od, 0.0, a1, 3) - cell_flux(a, c0[q], n[q], a1, a2, 1)) +
+                   (double)a.cg[n[q]] * (a2 - a1);
+            if (cnew < a.epsc) cnew = 0.0;
+            else if (cnew > 1.0 - a.epsc) cnew = 1.0;
+        }
+        int8_t fl;
+        if (cnew <= a.epsc) { fl = 0; cnew = 0.0; }
+        else if (cnew >= 1.0 - a.epsc) { fl = 1; cnew = 1.0; }
+        else fl = 2;
+        a.cn[n[q]] = cnew;
+        a.flag[n[q]] = fl;
+    }
 }
 
 // ghost cells of the new cvof and flags: SetVOFBC (x- y- z- x+ y+ z+ in that
@@ -278,10 +271,10 @@ int vof_scratch(paris_ctx* c) {
         long e = (long)(L.n[0] + (d == 0 ? 2 : 0)) * (L.n[1] + (d == 1 ? 2 : 0)) * (L.n[2] + (d == 2 ? 2 : 0));
         F = e > F ? e : F;
     }
-    const long nseg = (F + kVofSeg - 1) / kVofSeg;
     PARIS_CUDA_TRY(c, cudaMalloc(&c->vflux, 3 * L.total * sizeof(double)));
-    PARIS_CUDA_TRY(c, cudaMalloc(&c->mixlist, nseg * kVofSeg * sizeof(long)));
-    PARIS_CUDA_TRY(c, cudaMalloc(&c->mixsegn, nseg * sizeof(int)));
+    PARIS_CUDA_TRY(c, cudaMalloc(&c->mixlist, F * sizeof(long)));
+    PARIS_CUDA_TRY(c, cudaMalloc(&c->mixsegn, sizeof(int)));
+    c->mixcap = F;
     return PARIS_OK;
 }
 
@@ -299,7 +292,8 @@ int vof_sweep_dir(paris_ctx* c, int d, double dt, const double* src, double* dst
     a.v2 = c->vflux + L.total;
     a.v3 = c->vflux + 2 * L.total;
     a.list = c->mixlist;
-    a.segn = c->mixsegn;
+    a.count = c->mixsegn;
+    a.cap = c->mixcap;
     a.L = L;
     a.d = d;
     a.wy = c->d.vof_advect == PARIS_ADVECT_WY;
@@ -309,12 +303,13 @@ int vof_sweep_dir(paris_ctx* c, int d, double dt, const double* src, double* dst
     a.rdxyz = frexp(a.dxyz, &ex) == 0.5 ? 1.0 / a.dxyz : 0.0;   // 1/2^k is exact
     a.epsc = c->d.epsc;
     const long F = (long)(L.n[0] + (d == 0 ? 2 : 0)) * (L.n[1] + (d == 1 ? 2 : 0)) * (L.n[2] + (d == 2 ? 2 : 0));
-    a.nseg = (F + kVofSeg - 1) / kVofSeg;
     // the four kernels of a direction share the profile label "vof_sweep",
     // with the direction's cells counted once (on the update)
-    PARIS_LAUNCH_N(c, "vof_sweep", 0L, k_vof_mixed_list, (unsigned)a.nseg, kVofListThreads, 0, a, (unsigned)F);
+    PARIS_CUDA_TRY(c, cudaMemsetAsync(c->mixsegn, 0, sizeof(int), c->stream));
+    PARIS_LAUNCH_N(c, "vof_sweep", 0L, k_vof_mixed_list, div_up(F, kVofSeg), kVofListThreads, 0, a, (unsigned)F);
     PARIS_LAUNCH_N(c, "vof_sweep", 0L, k_vof_mixed_flux, c->nsm * 16, 128, 0, a);
-    PARIS_LAUNCH_N(c, "vof_sweep", c->N, k_vof_update, dim3(div_up(L.n[0], 128), L.n[1], L.n[2]), 128, 0, a);
+    PARIS_LAUNCH_N(c, "vof_sweep", c->N, k_vof_update, dim3(div_up(L.n[0], kVofUpdThreads * kVofUpd), L.n[1], L.n[2]),
+                   kVofUpdThreads, 0, a);
     long G = ghost_count(c->L);
     PARIS_LAUNCH_N(c, "vof_sweep", 0L, k_vof_ghosts, div_up(G, 256), 256, 0, dst, src, flag, c->L, c->bnd,
                    ctx_vof_jet(c), G, c->d.epsc);

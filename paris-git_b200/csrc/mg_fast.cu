@@ -19,7 +19,7 @@ static constexpr long kCoarseCells = 4096;   // 16^3
 static constexpr int kMaxLevels = 16;
 static constexpr int kCoarseSweeps = 8;
 static constexpr long kWarpCells = 64;   // coarse levels of at most 4^3 cells run in one warp
-static constexpr long kFusedCells = 1L << 18;
+static constexpr long kFusedCells = 1L << 15;
 static constexpr size_t kCoarseSmemMax = 227 * 1024;   // opt-in shared memory per block   // levels of at least 64^3 cells use the fused sweep
 
 template <typename T>

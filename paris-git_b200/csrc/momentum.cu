@@ -200,119 +200,6 @@ __global__ void __launch_bounds__(256) k_conv_quick_uniform(Vel V, double* __res
     }
 }
 
-// momentumConvectionQUICK on a uniform grid with the face values shared.
-// Each cell needs nine face values of its own (the u, v, w values on its
-// east, north and top faces) and the same nine of its west, south and bottom
-// neighbours.  A block of 32 x 4 threads takes a 32 x 4 x kQz column of
-// cells, one column of kQz cells per thread, marching up k: the west values
-// come from the lane to the left (shuffle), the south values from the row
-// below through shared memory, the bottom values from the thread's own
-// previous cell; only the first lane, the first row and the first cell of a
-// column compute their neighbour's values themselves.  Every value is formed
-// by the same functions on the same operands as k_conv_quick_uniform, so the
-// results are the same to the bit, with about 10 instead of 18
-// interpolations per cell.
-static constexpr int kQx = 32, kQy = 4, kQz = 4;
-
-// the nine face values of cell n: u on its east (a), north (w2), top (w3)
-// faces; v on its east (w1), north (a), top (w3); w on its east (w1), north
-// (w2), top (a)
-struct QFaces {
-    double ua, uw2, uw3, vw1, va, vw3, ww1, ww2, wa;
-};
-
-__device__ inline QFaces q_faces(const double* __restrict__ u, const double* __restrict__ v,
-                                 const double* __restrict__ w, long n, long sx, long sy, long sz,
-                                 const QuickUniform& Q) {
-    QFaces f;
-    f.ua = quick_same_u(u, n + sx, sx, Q.q[0][0], Q.q[0][1]);
-    f.uw2 = quick_cross_u(u, v, n, sy, sx, Q.q[1][2], Q.q[1][3]);
-    f.uw3 = quick_cross_u(u, w, n, sz, sx, Q.q[2][2], Q.q[2][3]);
-    f.vw1 = quick_cross_u(v, u, n, sx, sy, Q.q[0][2], Q.q[0][3]);
-    f.va = quick_same_u(v, n + sy, sy, Q.q[1][0], Q.q[1][1]);
-    f.vw3 = quick_cross_u(v, w, n, sz, sy, Q.q[2][2], Q.q[2][3]);
-    f.ww1 = quick_cross_u(w, u, n, sx, sz, Q.q[0][2], Q.q[0][3]);
-    f.ww2 = quick_cross_u(w, v, n, sy, sz, Q.q[1][2], Q.q[1][3]);
-    f.wa = quick_same_u(w, n + sz, sz, Q.q[2][0], Q.q[2][1]);
-    return f;
-}
-
-__global__ void __launch_bounds__(kQx * kQy) k_conv_quick_shared(Vel V, double* __restrict__ du,
-                                                                 double* __restrict__ dv, double* __restrict__ dw,
-                                                                 const Layout L, const Bnd B, const QuickUniform Q) {
-    __shared__ double ys[2][3][kQy][kQx];   // the north values of the row below, double-buffered over k
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int i = blockIdx.x * kQx + tx, j = blockIdx.y * kQy + ty, k0 = blockIdx.z * kQz;
-    // threads past the edge of the domain still take part in the shuffles and
-    // barriers; they read the last interior cell and write nothing
-    const bool in = i < L.n[0] && j < L.n[1];
-    const int ic = in ? i : (i < L.n[0] ? i : L.n[0] - 1), jc = j < L.n[1] ? j : L.n[1] - 1;
-    const long sx = 1, sy = L.pitch, sz = L.plane;
-    const double *u = V.u, *v = V.v, *w = V.w;
-    const int kend = min(k0 + kQz, L.n[2]);
-    // the top faces of the cell below (k - 1): u, v and w there
-    double bu3, bv3, bwa;
-    {
-        const long nb = lidx(L, ic, jc, k0) - sz;
-        bu3 = quick_cross_u(u, w, nb, sz, sx, Q.q[2][2], Q.q[2][3]);
-        bv3 = quick_cross_u(v, w, nb, sz, sy, Q.q[2][2], Q.q[2][3]);
-        bwa = quick_same_u(w, nb + sz, sz, Q.q[2][0], Q.q[2][1]);
-    }
-    for (int k = k0; k < k0 + kQz; k++) {
-        const int kc = k < L.n[2] ? k : L.n[2] - 1;
-        const long n = lidx(L, ic, jc, kc);
-        const QFaces f = q_faces(u, v, w, n, sx, sy, sz, Q);
-        // west values: the lane to the left, or computed at the first lane
-        double bu = __shfl_up_sync(0xffffffffu, f.ua, 1);
-        double w1mv = __shfl_up_sync(0xffffffffu, f.vw1, 1);
-        double w1mw = __shfl_up_sync(0xffffffffu, f.ww1, 1);
-        if (tx == 0) {
-            bu = quick_same_u(u, n, sx, Q.q[0][0], Q.q[0][1]);
-            w1mv = quick_cross_u(v, u, n - sx, sx, sy, Q.q[0][2], Q.q[0][3]);
-            w1mw = quick_cross_u(w, u, n - sx, sx, sz, Q.q[0][2], Q.q[0][3]);
-        }
-        // south values: the row below through shared memory, or computed at the first row
-        const int buf = (k - k0) & 1;
-        ys[buf][0][ty][tx] = f.uw2;
-        ys[buf][1][ty][tx] = f.va;
-        ys[buf][2][ty][tx] = f.ww2;
-        __syncthreads();
-        double w2mu, bv, w2mw;
-        if (ty > 0) {
-            w2mu = ys[buf][0][ty - 1][tx];
-            bv = ys[buf][1][ty - 1][tx];
-            w2mw = ys[buf][2][ty - 1][tx];
-        } else {
-            w2mu = quick_cross_u(u, v, n - sy, sy, sx, Q.q[1][2], Q.q[1][3]);
-            bv = quick_same_u(v, n, sy, Q.q[1][0], Q.q[1][1]);
-            w2mw = quick_cross_u(w, v, n - sy, sy, sz, Q.q[1][2], Q.q[1][3]);
-        }
-        if (in && k < kend) {
-            if (i < L.n[0] - 1 || B.per[0]) {
-                const double a = f.ua, b = bu;
-                du[n] = -(a * a - b * b) * Q.rdh[0]
-                    - (0.5 * ((v[n] + v[n + sx]) * f.uw2 - (v[n - sy] + v[n + sx - sy]) * w2mu)) * Q.rd[1]
-                    - (0.5 * ((w[n] + w[n + sx]) * f.uw3 - (w[n - sz] + w[n + sx - sz]) * bu3)) * Q.rd[2];
-            }
-            if (j < L.n[1] - 1 || B.per[1]) {
-                const double a = f.va, b = bv;
-                dv[n] = (-0.5 * ((u[n] + u[n + sy]) * f.vw1 - (u[n - sx] + u[n - sx + sy]) * w1mv)) * Q.rd[0]
-                    - (a * a - b * b) * Q.rdh[1]
-                    - (0.5 * ((w[n] + w[n + sy]) * f.vw3 - (w[n - sz] + w[n + sy - sz]) * bv3)) * Q.rd[2];
-            }
-            if (k < L.n[2] - 1 || B.per[2]) {
-                const double a = f.wa, b = bwa;
-                dw[n] = (-0.5 * ((u[n] + u[n + sz]) * f.ww1 - (u[n - sx] + u[n - sx + sz]) * w1mw)) * Q.rd[0]
-                    - (0.5 * ((v[n] + v[n + sz]) * f.ww2 - (v[n - sy] + v[n - sy + sz]) * w2mw)) * Q.rd[1]
-                    - (a * a - b * b) * Q.rdh[2];
-            }
-        }
-        bu3 = f.uw3;
-        bv3 = f.vw3;
-        bwa = f.wa;
-    }
-}
-
 // work(p, a) of momentumConvection_onedim for the component phi of
 // direction d (stride so = stride of d): the face value on axis a (stride
 // sa, transport velocity vel) at cell n; oa = 1 when a == d
@@ -641,10 +528,8 @@ extern "C" int paris_momentum_convection(paris_handle_t c, int32_t scheme) {
         bool exact, uniform;
         PARIS_CHECK(mom_tables(c, &T, &exact, &U, &uniform));
         if (uniform)
-            PARIS_LAUNCH_N(c, "mom_convection", c->N, k_conv_quick_shared,
-                           dim3(div_up(c->L.n[0], kQx), div_up(c->L.n[1], kQy), div_up(c->L.n[2], kQz)),
-                           dim3(kQx, kQy), 0, vel(c), c->fld[PARIS_FIELD_DU], c->fld[PARIS_FIELD_DV],
-                           c->fld[PARIS_FIELD_DW], c->L, c->bnd, U);
+            PARIS_LAUNCH_N(c, "mom_convection", c->N, k_conv_quick_uniform, cgrid(c->L), cblock(), 0, vel(c),
+                           c->fld[PARIS_FIELD_DU], c->fld[PARIS_FIELD_DV], c->fld[PARIS_FIELD_DW], c->L, c->bnd, U);
         else if (exact)
             PARIS_LAUNCH_N(c, "mom_convection", c->N, k_conv_quick<true>, cgrid(c->L), cblock(), 0, vel(c),
                            c->fld[PARIS_FIELD_DU], c->fld[PARIS_FIELD_DV], c->fld[PARIS_FIELD_DW], c->L, c->bnd, geo(c),

@@ -156,13 +156,13 @@ def workload(pkg, n, device=0):
 # algorithmic HBM bytes per cell of each labelled kernel (cells as recorded
 # by the profiler: the grid cells the launch processes)
 ALGO_BYTES = {
-    "pcg_dir_matvec_fp64(z32)": 68.0,  # z 4 + d_old 8 + p r/w 16 + 3 faces 24 + d 8 + q 8
-    "pcg_dir_matvec_fp64(z64)": 72.0,
-    "pcg_update_fp64(z32)": 32.0, # r r/w 16 + q 8 + rhs (FP32) 4 + z (FP32) 4
-    "pcg_update_fp64(z64)": 40.0,
-    "pcg_axpy_fp64": 24.0,        # p r/w 16 + d 8
+    "pcg_matvec_fp64": 40.0,      # d 8 + 3 faces 24 + q 8
+    "pcg_update_fp64(z32)": 56.0, # p r/w 16 + d 8 + r r/w 16 + q 8 + rhs (FP32) 4 + z (FP32) 4
+    "pcg_update_fp64(z64)": 64.0,
     "pcg_rz(z32)": 12.0,          # r 8 + z 4
     "pcg_rz(z64)": 16.0,
+    "pcg_dir(z32)": 20.0,         # z 4 + d r/w 16
+    "pcg_dir(z64)": 24.0,
     "mg_sweep_f32": 24.0,         # fused red-black sweep: x in 4 + 3 faces 12 + rhs 4 + x out 4
     "mg_sweep_f64": 48.0,
     "mg_sweep_zero_f32": 20.0,    # first sweep from x = 0: no iterate read

@@ -249,7 +249,6 @@ __device__ inline double block_max(double v, double* sh) {
     for (int _row = blockIdx.x * blockDim.y + threadIdx.y; _row < (n1) * (n2);             \
          _row += gridDim.x * blockDim.y) {                                                 \
         const int j = _row % (n1), k = _row / (n1);                                        \
-        _Pragma("unroll 2")                                                                \
         for (int i = threadIdx.x; i < (n0); i += blockDim.x) {
 #define ROWS_END \
         }        \

@@ -241,7 +241,7 @@ extern "C" int paris_gpu_finalize(paris_handle_t c) {
                     (void*)c->xc, (void*)c->yc, (void*)c->zc, (void*)c->xh, (void*)c->yh, (void*)c->zh, (void*)c->c2, (void*)c->flag, (void*)c->cg,
                     (void*)c->height, (void*)c->i32stage, (void*)c->cx, (void*)c->cy, (void*)c->cz,
                     (void*)c->rhs, (void*)c->A, (void*)c->red_part, (void*)c->fast_r64,
-                    (void*)c->fast_d64, (void*)c->fast_d64b, (void*)c->fast_q64,
+                    (void*)c->fast_d64, (void*)c->fast_q64,
                     (void*)c->vflux, (void*)c->mixlist, (void*)c->mixsegn, (void*)c->kflag, (void*)c->st_list,
                     (void*)c->st_count, (void*)c->debris_count, (void*)c->adj, (void*)c->stats_part, (void*)c->stats_out, (void*)c->mom_tab,
                     (void*)c->mc_tmp, (void*)c->mc_tmp2, (void*)c->mc_work, (void*)c->mc_fv, (void*)c->mc_flag,

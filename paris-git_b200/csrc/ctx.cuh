@@ -81,7 +81,6 @@ struct paris_ctx {
     std::vector<FastLevel<double>> fl64;
     double* fast_r64 = nullptr;    // PCG vectors (N each)
     double* fast_d64 = nullptr;
-    double* fast_d64b = nullptr;   // the second direction buffer of the merged CG passes
     double* fast_q64 = nullptr;
     double* adj = nullptr;         // projection adjoint: 10 ghosted fields + N (allocated on first use)
     // asynchronous transfers: one stream per direction, a device staging copy

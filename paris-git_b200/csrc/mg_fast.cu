@@ -391,6 +391,16 @@ struct Mat64 {
     const double *cx, *cy, *cz, *rhs;
 };
 
+__device__ inline double ax_compact(const Mat64& A, const double* __restrict__ x, const Layout& L, const Bnd& B,
+                                    int i, int j, int k, long m) {
+    LV<double> v{A.cx, A.cy, A.cz, nullptr, nullptr, L.n[0], L.n[1], L.n[2], 0};
+    double a1, a3, a5, xw, xe, xs, xn, xb, xt;
+    west_coefs(v, B, i, j, k, m, a1, a3, a5);
+    double a2 = A.cx[m], a4 = A.cy[m], a6 = A.cz[m];
+    nbrs(v, x, B, i, j, k, m, xw, xe, xs, xn, xb, xt);
+    const double xc = x[m];
+    return -(a1 * (xw - xc) + a2 * (xe - xc) + a3 * (xs - xc) + a4 * (xn - xc) + a5 * (xb - xc) + a6 * (xt - xc));
+}
 
 // r = b - A p on the ghosted p (wrap in the kernel); writes r as T into the
 // level-0 right-hand side (and as double into r64 when given).
@@ -439,92 +449,49 @@ __global__ void k_fast_correct(double* __restrict__ p, const T* __restrict__ x, 
 }
 
 // ---- PCG helpers (FP64 compact vectors) --------------------------------------
-// The CG iteration with its vector passes merged (the values are those of
-// the separate passes, to the bit):
-//   k_pcg_dir_matvec: d = z + beta d_old (also at the six neighbours, by the
-//     same expression), q = A d, d.q, and the update p += alpha_prev d_old
-//     that the previous iteration left pending (it reads d_old anyway);
-//   k_pcg_update2: r -= alpha q, the right-hand side (T) r of the next
-//     V-cycle, r.r, sum |r| and r.zold.
-// d_old and d alternate between two buffers.
-__device__ inline double dir_at(const float* __restrict__ z, const double* __restrict__ dold, double beta, long m) {
-    return (double)z[m] + beta * dold[m];
-}
-__device__ inline double dir_at(const double* __restrict__ z, const double* __restrict__ dold, double beta, long m) {
-    return z[m] + beta * dold[m];
-}
-
-template <typename T>
-__global__ void k_pcg_dir_matvec(const Mat64 A, const T* __restrict__ z, const double* __restrict__ dold,
-                                 double* __restrict__ d, double* __restrict__ q, double beta,
-                                 double* __restrict__ p, double alpha_prev, int pending, const Layout L, const Bnd B,
-                                 double* part) {
+// q = A d ; slot 0 = d.q
+__global__ void k_pcg_matvec(const Mat64 A, const double* __restrict__ d, double* __restrict__ q, const Layout L,
+                             const Bnd B, double* part) {
     __shared__ double sh[32];
     double s = 0.0;
-    const long sy = L.n[0], sz = (long)L.n[0] * L.n[1];
     ROWS_BEGIN(L.n[0], L.n[1], L.n[2])
-        const long m = cidx(L.n[0], L.n[1], i, j, k);
-        const double a1 = i > 0 ? A.cx[m - 1] : (B.per[0] ? A.cx[m + L.n[0] - 1] : 0.0);
-        const double a3 = j > 0 ? A.cy[m - sy] : (B.per[1] ? A.cy[m + sy * (L.n[1] - 1)] : 0.0);
-        const double a5 = k > 0 ? A.cz[m - sz] : (B.per[2] ? A.cz[m + sz * (L.n[2] - 1)] : 0.0);
-        const double a2 = A.cx[m], a4 = A.cy[m], a6 = A.cz[m];
-        const double xc = dir_at(z, dold, beta, m);
-        const double xw = i > 0 ? dir_at(z, dold, beta, m - 1)
-                                : (B.per[0] ? dir_at(z, dold, beta, m + L.n[0] - 1) : 0.0);
-        const double xe = i < L.n[0] - 1 ? dir_at(z, dold, beta, m + 1)
-                                         : (B.per[0] ? dir_at(z, dold, beta, m - (L.n[0] - 1)) : 0.0);
-        const double xs = j > 0 ? dir_at(z, dold, beta, m - sy)
-                                : (B.per[1] ? dir_at(z, dold, beta, m + sy * (L.n[1] - 1)) : 0.0);
-        const double xn = j < L.n[1] - 1 ? dir_at(z, dold, beta, m + sy)
-                                         : (B.per[1] ? dir_at(z, dold, beta, m - sy * (L.n[1] - 1)) : 0.0);
-        const double xb = k > 0 ? dir_at(z, dold, beta, m - sz)
-                                : (B.per[2] ? dir_at(z, dold, beta, m + sz * (L.n[2] - 1)) : 0.0);
-        const double xt = k < L.n[2] - 1 ? dir_at(z, dold, beta, m + sz)
-                                         : (B.per[2] ? dir_at(z, dold, beta, m - sz * (L.n[2] - 1)) : 0.0);
-        const double v = -(a1 * (xw - xc) + a2 * (xe - xc) + a3 * (xs - xc) + a4 * (xn - xc) + a5 * (xb - xc) +
-                           a6 * (xt - xc));
-        if (pending) {
-            const long n = lidx(L, i, j, k);
-            p[n] = p[n] + alpha_prev * dold[m];
-        }
-        d[m] = xc;
+        long m = cidx(L.n[0], L.n[1], i, j, k);
+        double v = ax_compact(A, d, L, B, i, j, k, m);
         q[m] = v;
-        s += xc * v;
+        s += d[m] * v;
     ROWS_END
     s = block_sum<256>(s, sh);
     if (linear_tid() == 0) part[blockIdx.x] = s;
 }
 
-// r -= alpha q, rT = (T) r.  slots: 0 = r.r, 1 = sum |r|, 2 = r.zold
+// p += alpha d (ghosted p), r -= alpha q, and the right-hand side of the next
+// V-cycle rT = (T) r.  slots: 0 = r.r, 1 = sum |r|, 2 = r.zold (zold: the
+// last preconditioned residual, still in the V-cycle's output buffer)
 template <typename T>
-__global__ void k_pcg_update2(double* __restrict__ r, const double* __restrict__ q, T* __restrict__ rT,
-                              const T* __restrict__ zold, double alpha, long N, double* part) {
+__global__ void k_pcg_update(double* __restrict__ p, double* __restrict__ r, const double* __restrict__ d,
+                             const double* __restrict__ q, T* __restrict__ rT, const T* __restrict__ zold,
+                             double alpha, const Layout L, double* part) {
     __shared__ double sh[32];
-    double s2 = 0.0, s1 = 0.0, szz = 0.0;
-    for (long m = blockIdx.x * (long)blockDim.x + threadIdx.x; m < N; m += (long)gridDim.x * blockDim.x) {
+    double s2 = 0.0, s1 = 0.0, sz = 0.0;
+    ROWS_BEGIN(L.n[0], L.n[1], L.n[2])
+        long m = cidx(L.n[0], L.n[1], i, j, k);
+        long n = lidx(L, i, j, k);
+        p[n] = p[n] + alpha * d[m];
         double rr = r[m] - alpha * q[m];
         r[m] = rr;
         rT[m] = (T)rr;
         s2 += rr * rr;
         s1 += fabs(rr);
-        szz += rr * (double)zold[m];
-    }
+        sz += rr * (double)zold[m];
+    ROWS_END
     s2 = block_sum<256>(s2, sh);
     s1 = block_sum<256>(s1, sh);
-    szz = block_sum<256>(szz, sh);
-    if (threadIdx.x == 0) {
+    sz = block_sum<256>(sz, sh);
+    if (linear_tid() == 0) {
         part[blockIdx.x] = s2;
         part[kRedBlocks + blockIdx.x] = s1;
-        part[2 * kRedBlocks + blockIdx.x] = szz;
+        part[2 * kRedBlocks + blockIdx.x] = sz;
     }
-}
-
-// p += alpha d (the pending update, before a true residual or the exit)
-__global__ void k_pcg_axpy_p(double* __restrict__ p, const double* __restrict__ d, double alpha, const Layout L) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-    if (i >= L.n[0]) return;
-    const long n = lidx(L, i, j, k);
-    p[n] = p[n] + alpha * d[cidx(L.n[0], L.n[1], i, j, k)];
 }
 
 // slot 0 = r.z with z the V-cycle's output
@@ -538,6 +505,13 @@ __global__ void k_pcg_rz(const T* __restrict__ z, const double* __restrict__ r, 
     if (threadIdx.x == 0) part[blockIdx.x] = s0;
 }
 
+// d = z + beta d
+template <typename T>
+__global__ void k_pcg_dir(double* __restrict__ d, const T* __restrict__ z, double beta, long N) {
+    long m = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (m < N) d[m] = (double)z[m] + beta * d[m];
+}
+
 // ---- host side ---------------------------------------------------------------
 // profile label of a kernel instantiated for T (stable strings)
 template <typename T>
@@ -546,12 +520,11 @@ template <>
 const char* kname<float>(const char* base) {
     static const char* names[] = {"mg_smooth_f32", "mg_restrict_f32", "mg_prolong_f32", "mg_coarse_cycle_f32",
                                   "mg_correct_f32", "mg_residual_fp64(r32)", "mg_sweep_f32", "mg_sweep_zero_f32",
-                                  "pcg_update_fp64(z32)", "pcg_rz(z32)", "pcg_dir(z32)", "mg_sweep_lower_f32",
-                                  "pcg_dir_matvec_fp64(z32)", "pcg_axpy_fp64"};
+                                  "pcg_update_fp64(z32)", "pcg_rz(z32)", "pcg_dir(z32)", "mg_sweep_lower_f32"};
     static const char* keys[] = {"mg_smooth", "mg_restrict", "mg_prolong", "mg_coarse_cycle", "mg_correct",
                                  "mg_residual_fp64", "mg_sweep", "mg_sweep_zero", "pcg_update", "pcg_rz", "pcg_dir",
-                                 "mg_sweep_lower", "pcg_dir_matvec", "pcg_axpy"};
-    for (int q = 0; q < 14; q++)
+                                 "mg_sweep_lower"};
+    for (int q = 0; q < 12; q++)
         if (!strcmp(base, keys[q])) return names[q];
     return base;
 }
@@ -559,12 +532,11 @@ template <>
 const char* kname<double>(const char* base) {
     static const char* names[] = {"mg_smooth_f64", "mg_restrict_f64", "mg_prolong_f64", "mg_coarse_cycle_f64",
                                   "mg_correct_f64", "mg_residual_fp64(r64)", "mg_sweep_f64", "mg_sweep_zero_f64",
-                                  "pcg_update_fp64(z64)", "pcg_rz(z64)", "pcg_dir(z64)", "mg_sweep_lower_f64",
-                                  "pcg_dir_matvec_fp64(z64)", "pcg_axpy_fp64"};
+                                  "pcg_update_fp64(z64)", "pcg_rz(z64)", "pcg_dir(z64)", "mg_sweep_lower_f64"};
     static const char* keys[] = {"mg_smooth", "mg_restrict", "mg_prolong", "mg_coarse_cycle", "mg_correct",
                                  "mg_residual_fp64", "mg_sweep", "mg_sweep_zero", "pcg_update", "pcg_rz", "pcg_dir",
-                                 "mg_sweep_lower", "pcg_dir_matvec", "pcg_axpy"};
-    for (int q = 0; q < 14; q++)
+                                 "mg_sweep_lower"};
+    for (int q = 0; q < 12; q++)
         if (!strcmp(base, keys[q])) return names[q];
     return base;
 }
@@ -917,7 +889,7 @@ static constexpr int kMaxRestarts = 2;
 template <typename T>
 static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* res, const double* rhs, double* p) {
     auto& lv = levels<T>(c);
-    for (double** v : {&c->fast_r64, &c->fast_d64, &c->fast_d64b, &c->fast_q64}) PARIS_CHECK(alloc_vec(c, v));
+    for (double** v : {&c->fast_r64, &c->fast_d64, &c->fast_q64}) PARIS_CHECK(alloc_vec(c, v));
     Mat64 A{c->cx, c->cy, c->cz, rhs};
     double s[3], tres, rel;
     PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>, red_grid(c, k_fast_residual64<T>, 256), kRowBlock, 0, A, p, c->L, c->bnd, lv[0].b, c->fast_r64,
@@ -930,48 +902,29 @@ static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result
     int nu1 = o->nu1 > 0 ? o->nu1 : 2, nu2 = o->nu2 > 0 ? o->nu2 : 2;
     double rz = 0.0;
     T* z = nullptr;
-    // the direction d = z + beta d_old is formed by the next matvec, and the
-    // update p += alpha d of an iteration waits for the next matvec (or for a
-    // true residual, or the exit); d and d_old alternate between two buffers
-    double* dbuf[2] = {c->fast_d64, c->fast_d64b};
-    int cur = 0;
-    double dir_beta = 0.0, alpha_pend = 0.0;
-    bool p_pend = false;
-    auto flush_p = [&]() -> int {
-        if (p_pend)
-            PARIS_LAUNCH_N(c, kname<T>("pcg_axpy"), c->N, k_pcg_axpy_p, row_grid(c->d.nx, c->d.ny, c->d.nz), 128, 0, p,
-                           dbuf[cur], alpha_pend, c->L);
-        p_pend = false;
-        return PARIS_OK;
-    };
-    if (!done) PARIS_CHECK(precondition<T>(c, nu1, nu2, &z, &rz));
+    if (!done) {
+        PARIS_CHECK(precondition<T>(c, nu1, nu2, &z, &rz));
+        PARIS_LAUNCH_N(c, kname<T>("pcg_dir"), c->N, k_pcg_dir<T>, div_up(c->N, 256), 256, 0, c->fast_d64, z, 0.0, c->N);
+    }
     int restarts = 0;
     while (!done && it < o->maxit) {
         double dq;
-        PARIS_LAUNCH_N(c, kname<T>("pcg_dir_matvec"), c->N, k_pcg_dir_matvec<T>, red_grid(c, k_pcg_dir_matvec<T>, 256),
-                       kRowBlock, 0, A, z, dbuf[cur], dbuf[1 - cur], c->fast_q64, dir_beta, p, alpha_pend,
-                       p_pend ? 1 : 0, c->L, c->bnd, c->red_part);
-        cur = 1 - cur;
-        p_pend = false;
+        PARIS_LAUNCH_N(c, "pcg_matvec_fp64", c->N, k_pcg_matvec, red_grid(c, k_pcg_matvec, 256), kRowBlock, 0, A, c->fast_d64, c->fast_q64, c->L, c->bnd, c->red_part);
         PARIS_CHECK(ctx_reduce_finish(c, 1, &dq));
         if (!(dq > 0.0)) break;
         double alpha = rz / dq;
-        PARIS_LAUNCH_N(c, kname<T>("pcg_update"), c->N, k_pcg_update2<T>, red_grid(c, k_pcg_update2<T>, 256), 256, 0,
-                       c->fast_r64, c->fast_q64, lv[0].b, z, alpha, c->N, c->red_part);
-        alpha_pend = alpha;
-        p_pend = true;
+        PARIS_LAUNCH_N(c, kname<T>("pcg_update"), c->N, k_pcg_update<T>, red_grid(c, k_pcg_update<T>, 256), kRowBlock, 0, p, c->fast_r64, c->fast_d64, c->fast_q64, lv[0].b, z, alpha, c->L,
+                     c->red_part);
         PARIS_CHECK(ctx_reduce_finish(c, 3, s));
         it++;
         done = converged(o, s[0], s[1], bn2, c->N, &tres, &rel);
         if (tres != tres) {
-            PARIS_CHECK(flush_p());
             ctx_set_error(c, "pressure residual is NaN after %d iterations", it);
             res->it = it; res->res = tres; res->rel_res = rel;
             return PARIS_NAN_DETECTED;
         }
         if (done) {
             // the true residual (also the right-hand side of a restart)
-            PARIS_CHECK(flush_p());
             PARIS_LAUNCH_N(c, kname<T>("mg_residual_fp64"), c->N, k_fast_residual64<T>,
                            red_grid(c, k_fast_residual64<T>, 256), kRowBlock, 0, A, p, c->L, c->bnd, lv[0].b,
                            c->fast_r64, c->red_part);
@@ -980,15 +933,16 @@ static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result
             if (done || restarts == kMaxRestarts) break;
             restarts++;
             PARIS_CHECK(precondition<T>(c, nu1, nu2, &z, &rz));
-            dir_beta = 0.0;
+            PARIS_LAUNCH_N(c, kname<T>("pcg_dir"), c->N, k_pcg_dir<T>, div_up(c->N, 256), 256, 0, c->fast_d64, z, 0.0,
+                           c->N);
             continue;
         }
         double r_zold = s[2], rz_new;
         PARIS_CHECK(precondition<T>(c, nu1, nu2, &z, &rz_new));
-        dir_beta = (rz_new - r_zold) / rz;   // flexible (Polak-Ribiere) form
+        double beta = (rz_new - r_zold) / rz;   // flexible (Polak-Ribiere) form
         rz = rz_new;
+        PARIS_LAUNCH_N(c, kname<T>("pcg_dir"), c->N, k_pcg_dir<T>, div_up(c->N, 256), 256, 0, c->fast_d64, z, beta, c->N);
     }
-    PARIS_CHECK(flush_p());
     res->it = done ? it : o->maxit + 1;
     res->res = tres;
     res->rel_res = rel;

@@ -38,6 +38,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "steps/s @256³ VOF+MG projection, mixed vs FP64 MG at 1e-10 residual"
 REL_TOL = 1e-10
+NU = [2, 2]   # pre- and post-smoothing sweeps of the B200 V-cycle (--nu1, --nu2)
 
 
 def parse():
@@ -51,6 +52,8 @@ def parse():
                     help="cells per direction (projection: 256; rising_bubble: 512 across, twice that in z); "
                          "under torchrun use --grid, which its own options cannot be confused with")
     ap.add_argument("--pcg", type=int, default=1, help="1: FP64 flexible CG preconditioned by the V-cycle, 0: defect correction")
+    ap.add_argument("--nu1", type=int, default=2, help="pre-smoothing sweeps of the B200 V-cycle")
+    ap.add_argument("--nu2", type=int, default=2, help="post-smoothing sweeps of the B200 V-cycle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0,
                     help="seconds of reference V-cycles in the cpu_baseline sample step")
@@ -169,6 +172,12 @@ ALGO_BYTES = {
     "mg_sweep_zero_f64": 40.0,
     "mg_sweep_lower_f32": 24.0,   # levels below the finest: the same bytes, served from L2
     "mg_sweep_lower_f64": 48.0,
+    "mg_sweep_pair_f32": 24.0,    # two sweeps in one pass: the bytes of one sweep
+    "mg_sweep_pair_f64": 48.0,
+    "mg_sweep_pair_zero_f32": 20.0,
+    "mg_sweep_pair_zero_f64": 40.0,
+    "mg_sweep_pair_lower_f32": 24.0,
+    "mg_sweep_pair_lower_f64": 48.0,
     "mg_smooth_f32": 12.0,        # half of a red-black sweep: (p 4 + 3 faces 12 + rhs 4 + p write 4)/2
     "mg_smooth_f64": 24.0,
     "mg_restrict_f32": 20.5,      # x 4 + b 4 + 3 faces 12 + coarse rhs 4/8
@@ -203,7 +212,7 @@ def gpu_step(gpu, capi, k, dt, mode, pcg):
         gpu.copy_field(dst, src)
     gpu.setup_poisson(dt)
     gpu.fill_field(capi.F_P, 0.0)
-    r = gpu.new_solver(0.0, maxit=200, mode=mode, rel_tol=REL_TOL, pcg=pcg)
+    r = gpu.new_solver(0.0, maxit=200, mode=mode, rel_tol=REL_TOL, pcg=pcg, nu1=NU[0], nu2=NU[1])
     gpu.project_velocity(dt)
     return r
 
@@ -245,10 +254,10 @@ def pressure_error(gpu, capi, args, dt, reset, cpu_oracle):
             gpu.copy_field(dst, src)
         gpu.setup_poisson(dt)
         gpu.fill_field(capi.F_P, 0.0)
-        rm = gpu.new_solver(0.0, maxit=200, mode=capi.MG_MIXED, rel_tol=REL_TOL, pcg=args.pcg)
+        rm = gpu.new_solver(0.0, maxit=200, mode=capi.MG_MIXED, rel_tol=REL_TOL, pcg=args.pcg, nu1=NU[0], nu2=NU[1])
         pm = gpu.download(capi.F_P)
         gpu.fill_field(capi.F_P, 0.0)
-        r64 = gpu.new_solver(0.0, maxit=200, mode=capi.MG_FP64, rel_tol=REL_TOL, pcg=args.pcg)
+        r64 = gpu.new_solver(0.0, maxit=200, mode=capi.MG_FP64, rel_tol=REL_TOL, pcg=args.pcg, nu1=NU[0], nu2=NU[1])
         p64 = gpu.download(capi.F_P)
         pm_i, p64_i = pm[g:-g, g:-g, g:-g], p64[g:-g, g:-g, g:-g]
         l2, mx = _rel_diff(pm_i, p64_i)
@@ -412,7 +421,7 @@ def run_b200(args, dist):
     gpu.linfunc(capi.F_RHO)
     gpu.setup_poisson(dt)
     gpu.fill_field(capi.F_P, 0.0)
-    gpu.new_solver(0.0, maxit=200, mode=capi.MG_MIXED, rel_tol=REL_TOL, pcg=args.pcg)
+    gpu.new_solver(0.0, maxit=200, mode=capi.MG_MIXED, rel_tol=REL_TOL, pcg=args.pcg, nu1=NU[0], nu2=NU[1])
     gpu.project_velocity(dt)
     cvof0 = gpu.download(capi.F_CVOF) if (dist.rank == 0 and not args.no_cpu_baseline) else None
     flag0 = gpu.download(capi.F_VOF_FLAG) if cvof0 is not None else None
@@ -562,7 +571,7 @@ def run_b200(args, dist):
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
         "config": projection_config(n, dist.world),
-        "solver": ("B200 MG: FP32 red-black V(2,2) cycles in an FP64 " +
+        "solver": (f"B200 MG: FP32 red-black V({NU[0]},{NU[1]}) cycles in an FP64 " +
                    ("flexible-CG (preconditioner) loop" if args.pcg else "defect-correction loop")),
         "fp64_steps_per_s": dist.world * args.steps / (ms64 / 1e3),
         ("mixed_dc_steps_per_s" if args.pcg else "mixed_pcg_steps_per_s"): dist.world * args.steps / (msdc / 1e3),
@@ -790,6 +799,7 @@ def run_bubble(args, dist):
 
 def main():
     args = parse()
+    NU[:] = [args.nu1, args.nu2]
     if args.n is None:
         args.n = 512 if args.workload == "rising_bubble" else 256
     dist = Dist()

@@ -171,6 +171,7 @@ static inline dim3 row_grid(long n0, int n1, int n2) { return dim3(div_up(n0, 12
 
 #include "mg_sweep.cuh"
 #include "mg_sweep_tma.cuh"
+#include "mg_sweep4.cuh"
 
 // 32-bit forms of smooth_cell / resid_cell / restrict_cell for the levels of
 // the single-block coarse cycle (at most a few thousand cells): the same
@@ -520,11 +521,12 @@ template <>
 const char* kname<float>(const char* base) {
     static const char* names[] = {"mg_smooth_f32", "mg_restrict_f32", "mg_prolong_f32", "mg_coarse_cycle_f32",
                                   "mg_correct_f32", "mg_residual_fp64(r32)", "mg_sweep_f32", "mg_sweep_zero_f32",
-                                  "pcg_update_fp64(z32)", "pcg_rz(z32)", "pcg_dir(z32)", "mg_sweep_lower_f32"};
+                                  "pcg_update_fp64(z32)", "pcg_rz(z32)", "pcg_dir(z32)", "mg_sweep_lower_f32",
+                                  "mg_sweep_pair_f32", "mg_sweep_pair_zero_f32", "mg_sweep_pair_lower_f32"};
     static const char* keys[] = {"mg_smooth", "mg_restrict", "mg_prolong", "mg_coarse_cycle", "mg_correct",
                                  "mg_residual_fp64", "mg_sweep", "mg_sweep_zero", "pcg_update", "pcg_rz", "pcg_dir",
-                                 "mg_sweep_lower"};
-    for (int q = 0; q < 12; q++)
+                                 "mg_sweep_lower", "mg_sweep_pair", "mg_sweep_pair_zero", "mg_sweep_pair_lower"};
+    for (int q = 0; q < 15; q++)
         if (!strcmp(base, keys[q])) return names[q];
     return base;
 }
@@ -532,11 +534,12 @@ template <>
 const char* kname<double>(const char* base) {
     static const char* names[] = {"mg_smooth_f64", "mg_restrict_f64", "mg_prolong_f64", "mg_coarse_cycle_f64",
                                   "mg_correct_f64", "mg_residual_fp64(r64)", "mg_sweep_f64", "mg_sweep_zero_f64",
-                                  "pcg_update_fp64(z64)", "pcg_rz(z64)", "pcg_dir(z64)", "mg_sweep_lower_f64"};
+                                  "pcg_update_fp64(z64)", "pcg_rz(z64)", "pcg_dir(z64)", "mg_sweep_lower_f64",
+                                  "mg_sweep_pair_f64", "mg_sweep_pair_zero_f64", "mg_sweep_pair_lower_f64"};
     static const char* keys[] = {"mg_smooth", "mg_restrict", "mg_prolong", "mg_coarse_cycle", "mg_correct",
                                  "mg_residual_fp64", "mg_sweep", "mg_sweep_zero", "pcg_update", "pcg_rz", "pcg_dir",
-                                 "mg_sweep_lower"};
-    for (int q = 0; q < 12; q++)
+                                 "mg_sweep_lower", "mg_sweep_pair", "mg_sweep_pair_zero", "mg_sweep_pair_lower"};
+    for (int q = 0; q < 15; q++)
         if (!strcmp(base, keys[q])) return names[q];
     return base;
 }
@@ -628,6 +631,15 @@ static void level_maps(FastLevel<float>& l) {
         delete t;
 }
 
+// Two consecutive sweeps of a smoothing pass run as one pass over memory
+// (k_rb_sweep4_cfg) when PARIS_SWEEP_PAIRS=1 is in the environment as a
+// handle first builds its levels; the two forms give the same iterate to the
+// bit.
+static bool pairs_wanted() {
+    const char* e = getenv("PARIS_SWEEP_PAIRS");
+    return e && e[0] == '1';
+}
+
 void mg_fast_free_maps(paris_ctx* c) {
     for (auto& l : c->fl32) {
         delete static_cast<LevelTma*>(l.tma);
@@ -652,6 +664,7 @@ static int fast_alloc(paris_ctx* c) {
         bool fusable = l.N >= kFusedCells && l.N > kCoarseCells && l.n[0] % 4 == 0 && l.n[1] % 2 == 0 &&
                        l.n[2] % 2 == 0 && L < nl - 1;
         if (fusable) PARIS_CUDA_TRY(c, cudaMalloc(&l.x2, l.N * sizeof(T)));
+        l.pairs = fusable && pairs_wanted();
         if constexpr (std::is_same<T, float>::value) level_maps(l);
     }
     return PARIS_OK;
@@ -736,6 +749,39 @@ static int sweep_fused(paris_ctx* c, int L, const FastLevel<T>& l, const T* xin,
     return PARIS_OK;
 }
 
+// planes per block of the pair sweep: as sweep_chunk, at least 8 planes per
+// block (a block recomputes three planes on either side of its chunk)
+template <typename T>
+static int sweep4_chunk(paris_ctx* c, const FastLevel<T>& l) {
+    using Cfg = typename SwGeo4<T>::Cfg;
+    static int per_sm = 0;
+    if (!per_sm) {
+        cudaFuncSetAttribute(k_rb_sweep4_cfg<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sweep4_smem_cfg<Cfg>());
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rb_sweep4_cfg<Cfg>, Cfg::NT,
+                                                          sweep4_smem_cfg<Cfg>()) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
+    }
+    long tiles = (long)div_up(l.n[0], Cfg::TX) * div_up(l.n[1], Cfg::TY);
+    long nbz = (long)per_sm * c->nsm / tiles;
+    long cap = l.n[2] / 8;
+    if (nbz > cap) nbz = cap;
+    if (nbz < 1) nbz = 1;
+    return (int)div_up(l.n[2], nbz);
+}
+
+// two sweeps (colour `first`, then the other; twice) from xin to xout
+template <typename T>
+static int sweep_pair(paris_ctx* c, int L, const FastLevel<T>& l, const T* xin, T* xout, const T* xc, int first) {
+    using Cfg = typename SwGeo4<T>::Cfg;
+    const char* label = L > 0 ? "mg_sweep_pair_lower" : (xin ? "mg_sweep_pair" : "mg_sweep_pair_zero");
+    int zc = sweep4_chunk<T>(c, l);
+    dim3 grid(div_up(l.n[0], Cfg::TX), div_up(l.n[1], Cfg::TY), div_up(l.n[2], zc));
+    PARIS_LAUNCH_N(c, kname<T>(label), l.N, k_rb_sweep4_cfg<Cfg>, grid, Cfg::NT, sweep4_smem_cfg<Cfg>(), view(l), xin,
+                   xout, xc, c->bnd, first, zc);
+    return PARIS_OK;
+}
+
 template <typename T>
 static LV<T> view_x(const FastLevel<T>& l, T* x) {
     LV<T> v = view(l);
@@ -757,8 +803,14 @@ static int vcycle(paris_ctx* c, int nu1, int nu2, T** x0) {
         if (l.x2 && nu1 > 0) {
             const T* in = nullptr;
             T* out = l.x;
-            for (int s = 0; s < nu1; s++) {
-                PARIS_CHECK(sweep_fused<T>(c, L, l, in, out, nullptr, 0));
+            for (int s = 0; s < nu1;) {
+                if (l.pairs && s + 1 < nu1) {
+                    PARIS_CHECK(sweep_pair<T>(c, L, l, in, out, nullptr, 0));
+                    s += 2;
+                } else {
+                    PARIS_CHECK(sweep_fused<T>(c, L, l, in, out, nullptr, 0));
+                    s += 1;
+                }
                 in = out;
                 out = out == l.x ? l.x2 : l.x;
             }
@@ -795,9 +847,16 @@ static int vcycle(paris_ctx* c, int nu1, int nu2, T** x0) {
         const FastLevel<T>& l = lv[L];
         if (l.x2 && nu2 > 0) {
             T* in = cur[L];
-            for (int s = 0; s < nu2; s++) {
+            for (int s = 0; s < nu2;) {
                 T* out = in == l.x ? l.x2 : l.x;
-                PARIS_CHECK(sweep_fused<T>(c, L, l, in, out, s == 0 ? cur[L + 1] : nullptr, 1));
+                const T* xc = s == 0 ? cur[L + 1] : nullptr;
+                if (l.pairs && s + 1 < nu2) {
+                    PARIS_CHECK(sweep_pair<T>(c, L, l, in, out, xc, 1));
+                    s += 2;
+                } else {
+                    PARIS_CHECK(sweep_fused<T>(c, L, l, in, out, xc, 1));
+                    s += 1;
+                }
                 in = out;
             }
             cur[L] = in;

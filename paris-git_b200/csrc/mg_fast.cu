@@ -598,7 +598,7 @@ static TmEncodeFn tm_encode_fn() {
 static bool tm_encode(CUtensorMap* m, const float* base, const int n[3]) {
     TmEncodeFn fn = tm_encode_fn();
     if (!fn) return false;
-    using Cfg = SwGeo<float>::Cfg;
+    using Cfg = SwTmaCfg;
     const cuuint64_t dims[3] = {(cuuint64_t)n[0], (cuuint64_t)n[1], (cuuint64_t)n[2]};
     const cuuint64_t strides[2] = {(cuuint64_t)n[0] * sizeof(float), (cuuint64_t)n[0] * n[1] * sizeof(float)};
     const cuuint32_t box[3] = {(cuuint32_t)(kSwTX + 8), (cuuint32_t)(Cfg::TY + 4), 1u};
@@ -620,7 +620,7 @@ static bool tma_wanted() {
 }
 
 static void level_maps(FastLevel<float>& l) {
-    using Cfg = SwGeo<float>::Cfg;
+    using Cfg = SwTmaCfg;
     if (!l.x2 || l.n[0] % kSwTX || l.n[1] % Cfg::TY || !tma_wanted()) return;
     LevelTma* t = new LevelTma();
     bool ok = tm_encode(&t->m.x, l.x, l.n) && tm_encode(&t->x2, l.x2, l.n) && tm_encode(&t->m.cx, l.cx, l.n) &&
@@ -708,7 +708,7 @@ static int sweep_chunk(paris_ctx* c, const FastLevel<T>& l) {
 
 // planes per block of the TMA-staged sweep, as sweep_chunk
 static int sweep_tma_chunk(paris_ctx* c, const FastLevel<float>& l) {
-    using Cfg = SwGeo<float>::Cfg;
+    using Cfg = SwTmaCfg;
     static int per_sm = 0;
     if (!per_sm) {
         cudaFuncSetAttribute(k_rb_sweep_tma<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -735,9 +735,10 @@ static int sweep_fused(paris_ctx* c, int L, const FastLevel<T>& l, const T* xin,
             const LevelTma* t = static_cast<const LevelTma*>(l.tma);
             SwTmaMaps M = t->m;
             if (xin == l.x2) M.x = t->x2;
+            using TC = SwTmaCfg;
             const int zc = sweep_tma_chunk(c, l);
-            dim3 grid(div_up(l.n[0], Cfg::TX), div_up(l.n[1], Cfg::TY), div_up(l.n[2], zc));
-            PARIS_LAUNCH_N(c, kname<T>(label), l.N, k_rb_sweep_tma<Cfg>, grid, Cfg::NT, sweep_tma_smem<Cfg>(),
+            dim3 grid(div_up(l.n[0], TC::TX), div_up(l.n[1], TC::TY), div_up(l.n[2], zc));
+            PARIS_LAUNCH_N(c, kname<T>(label), l.N, k_rb_sweep_tma<TC>, grid, TC::NT, sweep_tma_smem<TC>(),
                            view(l), xin, M, xout, xc, c->bnd, first, zc, c->err_dev);
             return PARIS_OK;
         }

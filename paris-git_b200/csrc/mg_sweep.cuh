@@ -52,6 +52,20 @@ static constexpr size_t sweep_smem() {
     return sweep2_smem_cfg<typename SwGeo<T>::Cfg>();
 }
 
+// VEC/2 coarse values of a staged chunk, loaded together
+template <typename T, int N>
+struct SwCVec;
+template <>
+struct SwCVec<float, 2> {
+    using V = float2;
+    __device__ static V zero() { return make_float2(0.f, 0.f); }
+};
+template <>
+struct SwCVec<double, 1> {
+    using V = double;
+    __device__ static V zero() { return 0.0; }
+};
+
 template <typename T>
 struct SwVec;
 template <>
@@ -241,34 +255,31 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
     const int srl = 4 + 2 * scol + RX * sry;
     const int spar = (sgj + first) & 1;
 
-    int coff[G::CPER];
-    T cval[2][G::CPER];
+    // coarse-grid correction of the chunks this thread stages: VEC/2 coarse
+    // values per chunk and plane (a chunk starts at an even cell and stays in
+    // one row), fetched one step ahead and added to the thread's own chunks as
+    // they arrive, before the barrier that publishes them
+    constexpr int CV = VEC / 2;
+    using CVec = typename SwCVec<T, CV>::V;
+    const bool cload = xc != nullptr && ld && cok;
     const int cn0 = n0 >> 1;
     const long cplane = (long)cn0 * (n1 >> 1);
-#pragma unroll
-    for (int q = 0; q < G::CPER; q++) {
-        coff[q] = -1;
-        cval[0][q] = cval[1][q] = (T)0;
-        int e = tid + q * NT;
-        if (xc && e < RP) {
-            int gi = sw_wrap(x0 - 4 + e % RX, n0, B.per[0]);
-            int gj = sw_wrap(y0 - 2 + e / RX, n1, B.per[1]);
-            if (gi >= 0 && gj >= 0) coff[q] = (gi >> 1) + cn0 * (gj >> 1);
-        }
-    }
+    long ccoff = 0;
+    if (cload) ccoff = ((cin % n0) >> 1) + (long)cn0 * ((cin / n0) >> 1);
+    CVec cval[2];
     auto fetch_coarse = [&](int h, int k) {
-        int gk = sw_wrap(k, n2, B.per[2]);
-        const T* cp = xc + cplane * (gk >> 1);
-#pragma unroll
-        for (int q = 0; q < G::CPER; q++) cval[h][q] = (gk >= 0 && coff[q] >= 0) ? cp[coff[q]] : (T)0;
+        const int gk = sw_wrap(k, n2, B.per[2]);
+        if (cload && gk >= 0)
+            cval[h] = *reinterpret_cast<const CVec*>(xc + cplane * (gk >> 1) + ccoff);
+        else
+            cval[h] = SwCVec<T, CV>::zero();
     };
     auto add_coarse = [&](int h, int k) {
-        T* d = rx_ + slot(k, G::XS) * RP;
+        if (!cload) return;
+        T* d = rx_ + slot(k, G::XS) * RP + creg / sizeof(T);
+        const T* c = reinterpret_cast<const T*>(&cval[h]);
 #pragma unroll
-        for (int q = 0; q < G::CPER; q++) {
-            int e = tid + q * NT;
-            if (e < RP) d[e] += cval[h][q];
-        }
+        for (int e = 0; e < VEC; e++) d[e] += c[e >> 1];
     };
     auto update = [&](int r, T* xk, const T* xm, const T* xp, const T* cxk, const T* cyk, const T* bk,
                       const T* czk, const T* czm) {
@@ -322,14 +333,6 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
     int xb = G::XS - 1, cb = 0, zb = G::ZS - 1;
     for (int f0 = z0 - 1; f0 <= z1; f0 += 2) {
         cp_async_wait_newest<G::D - 1>();
-        __syncthreads();
-        // slots of planes f0+2D+1, f0+2D+2 (iterate) and f0+2D, f0+2D+1
-        // (coefficients): those of planes f0-4, f0-3 and f0-3, f0-2
-        stage_x(f0 + 2 * G::D + 1, sw_add(xb, -2, G::XS));
-        stage_x(f0 + 2 * G::D + 2, sw_add(xb, -1, G::XS));
-        stage_c(f0 + 2 * G::D, sw_add(cb, -2, G::CS), sw_add(zb, -2, G::ZS), false);
-        stage_c(f0 + 2 * G::D + 1, sw_add(cb, -1, G::CS), sw_add(zb, -1, G::ZS), false);
-        cp_async_commit();
         if (xc) {   // the iterate planes that arrived: group 0's, then two per step
             if (f0 == z0 - 1) {
                 for (int k = z0 - 2; k <= z0 + 1; k++) {
@@ -342,8 +345,15 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
             }
             fetch_coarse(0, f0 + 3);
             fetch_coarse(1, f0 + 4);
-            __syncthreads();
         }
+        __syncthreads();
+        // slots of planes f0+2D+1, f0+2D+2 (iterate) and f0+2D, f0+2D+1
+        // (coefficients): those of planes f0-4, f0-3 and f0-3, f0-2
+        stage_x(f0 + 2 * G::D + 1, sw_add(xb, -2, G::XS));
+        stage_x(f0 + 2 * G::D + 2, sw_add(xb, -1, G::XS));
+        stage_c(f0 + 2 * G::D, sw_add(cb, -2, G::CS), sw_add(zb, -2, G::ZS), false);
+        stage_c(f0 + 2 * G::D + 1, sw_add(cb, -1, G::CS), sw_add(zb, -1, G::ZS), false);
+        cp_async_commit();
         // iterate planes f0-2 .. f0+2, coefficient planes f0-1 .. f0+1, cz f0-2 .. f0+1
         T* const xm2 = rx_ + xb * RP;
         T* const xm1 = rx_ + sw_add(xb, 1, G::XS) * RP;

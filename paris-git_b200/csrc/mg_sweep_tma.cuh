@@ -72,6 +72,10 @@ __device__ inline bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
     return true;
 }
 
+// the configuration of the TMA-staged sweep (its own, whatever the cp.async
+// sweep uses): 32x16 tiles, one step staged ahead, two blocks per SM
+using SwTmaCfg = SwCfg<float, 16, 1, 320, 2>;
+
 // the ring slots, two mbarriers, and 128 bytes to align the slots (a box's
 // destination must start on a 128-byte boundary)
 template <class C>

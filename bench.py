@@ -39,6 +39,8 @@ sys.path.insert(0, ROOT)
 METRIC = "steps/s @256³ VOF+MG projection, mixed vs FP64 MG at 1e-10 residual"
 REL_TOL = 1e-10
 NU = [2, 2]   # pre- and post-smoothing sweeps of the B200 V-cycle (--nu1, --nu2)
+OMEGA = [1.1]   # relaxation factor of its red-black smoother (--beta)
+REF_BETA = 1.2  # the reference's default BETA (paris.f90:3553), for its own multigrid
 
 
 def parse():
@@ -52,6 +54,8 @@ def parse():
                     help="cells per direction (projection: 256; rising_bubble: 512 across, twice that in z); "
                          "under torchrun use --grid, which its own options cannot be confused with")
     ap.add_argument("--pcg", type=int, default=1, help="1: FP64 flexible CG preconditioned by the V-cycle, 0: defect correction")
+    ap.add_argument("--beta", type=float, default=1.1,
+                    help="relaxation factor of the B200 multigrid's red-black smoother (the reference's BETA)")
     ap.add_argument("--nu1", type=int, default=2, help="pre-smoothing sweeps of the B200 V-cycle")
     ap.add_argument("--nu2", type=int, default=2, help="post-smoothing sweeps of the B200 V-cycle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -212,7 +216,7 @@ def gpu_step(gpu, capi, k, dt, mode, pcg):
         gpu.copy_field(dst, src)
     gpu.setup_poisson(dt)
     gpu.fill_field(capi.F_P, 0.0)
-    r = gpu.new_solver(0.0, maxit=200, mode=mode, rel_tol=REL_TOL, pcg=pcg, nu1=NU[0], nu2=NU[1])
+    r = gpu.new_solver(0.0, maxit=200, mode=mode, rel_tol=REL_TOL, pcg=pcg, nu1=NU[0], nu2=NU[1], beta=OMEGA[0])
     gpu.project_velocity(dt)
     return r
 
@@ -254,10 +258,10 @@ def pressure_error(gpu, capi, args, dt, reset, cpu_oracle):
             gpu.copy_field(dst, src)
         gpu.setup_poisson(dt)
         gpu.fill_field(capi.F_P, 0.0)
-        rm = gpu.new_solver(0.0, maxit=200, mode=capi.MG_MIXED, rel_tol=REL_TOL, pcg=args.pcg, nu1=NU[0], nu2=NU[1])
+        rm = gpu.new_solver(0.0, maxit=200, mode=capi.MG_MIXED, rel_tol=REL_TOL, pcg=args.pcg, nu1=NU[0], nu2=NU[1], beta=OMEGA[0])
         pm = gpu.download(capi.F_P)
         gpu.fill_field(capi.F_P, 0.0)
-        r64 = gpu.new_solver(0.0, maxit=200, mode=capi.MG_FP64, rel_tol=REL_TOL, pcg=args.pcg, nu1=NU[0], nu2=NU[1])
+        r64 = gpu.new_solver(0.0, maxit=200, mode=capi.MG_FP64, rel_tol=REL_TOL, pcg=args.pcg, nu1=NU[0], nu2=NU[1], beta=OMEGA[0])
         p64 = gpu.download(capi.F_P)
         pm_i, p64_i = pm[g:-g, g:-g, g:-g], p64[g:-g, g:-g, g:-g]
         l2, mx = _rel_diff(pm_i, p64_i)
@@ -314,13 +318,14 @@ class CpuReference:
     """The reference algorithm on the host cores (the FP64 restatement in
     oracle/, OpenMP over all cores): vofsweeps, linfunc, SetupPoisson, the
     reference multigrid (NewSolverMG, MGsolver.f90:346-405: V-cycles from
-    p = 0 until the RMS residual is below 1e-10 of the RMS right-hand side)
-    and project_velocity, on the same workload.
+    p = 0 until the RMS residual is below 1e-10 of the RMS right-hand side,
+    with the reference's default relaxation factor BETA = 1.2) and
+    project_velocity, on the same workload.
 
     The reference multigrid converges slowly at density ratio 1000: on this
-    workload it needs 309 cycles at 64^3 and 879 at 128^3 (asymptotic rate
-    0.981 per cycle there), and more at 256^3, so a complete step at 256^3
-    takes longer than a timing run can give it.  Each step therefore runs the
+    workload it needs 225 cycles at 64^3 (309 with BETA = 1), and more at
+    higher resolution, so a complete step at 256^3 takes longer than a timing
+    run can give it.  Each step therefore runs the
     V-cycles until the tolerance or until its time budget is spent, whichever
     comes first.  A step that stops at its budget has done less work than the
     reference needs, so the steps/s measured is an upper bound of the
@@ -348,7 +353,7 @@ class CpuReference:
         st, A = orc.setup_poisson(d, *self.u, rho, self.dt)
         rms_b = float(np.sqrt(np.mean(A[7] ** 2)))
         p = orc.zeros(d)
-        ok, cycles, tres, _ = orc.new_solver_mg_timed(d, A, p, REL_TOL * rms_b, budget_s)
+        ok, cycles, tres, _ = orc.new_solver_mg_timed(d, A, p, REL_TOL * rms_b, budget_s, beta=REF_BETA)
         orc.project_velocity(d, *self.u, p, rho, self.dt)
         t = time.perf_counter() - t0
         self.log.append({"s": round(t, 2), "cycles": cycles, "converged": bool(ok), "rel_res": tres / rms_b})
@@ -363,7 +368,7 @@ def projection_config(n, world):
             "cells": n ** 3, "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (141 MB per field)"}
 
 
-REF_SOLVER = "reference MG (MGsolver.f90 NewSolverMG, nrelax=3), FP64, on the host cores"
+REF_SOLVER = "reference MG (MGsolver.f90 NewSolverMG, nrelax=3, BETA=1.2), FP64, on the host cores"
 
 
 def run_reference(args, dist):
@@ -421,7 +426,7 @@ def run_b200(args, dist):
     gpu.linfunc(capi.F_RHO)
     gpu.setup_poisson(dt)
     gpu.fill_field(capi.F_P, 0.0)
-    gpu.new_solver(0.0, maxit=200, mode=capi.MG_MIXED, rel_tol=REL_TOL, pcg=args.pcg, nu1=NU[0], nu2=NU[1])
+    gpu.new_solver(0.0, maxit=200, mode=capi.MG_MIXED, rel_tol=REL_TOL, pcg=args.pcg, nu1=NU[0], nu2=NU[1], beta=OMEGA[0])
     gpu.project_velocity(dt)
     cvof0 = gpu.download(capi.F_CVOF) if (dist.rank == 0 and not args.no_cpu_baseline) else None
     flag0 = gpu.download(capi.F_VOF_FLAG) if cvof0 is not None else None
@@ -571,7 +576,8 @@ def run_b200(args, dist):
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
         "config": projection_config(n, dist.world),
-        "solver": (f"B200 MG: FP32 red-black V({NU[0]},{NU[1]}) cycles in an FP64 " +
+        "solver": (f"B200 MG: FP32 red-black V({NU[0]},{NU[1]}) cycles" +
+                   (f" (over-relaxed, factor {OMEGA[0]})" if OMEGA[0] != 1.0 else "") + " in an FP64 " +
                    ("flexible-CG (preconditioner) loop" if args.pcg else "defect-correction loop")),
         "fp64_steps_per_s": dist.world * args.steps / (ms64 / 1e3),
         ("mixed_dc_steps_per_s" if args.pcg else "mixed_pcg_steps_per_s"): dist.world * args.steps / (msdc / 1e3),
@@ -800,6 +806,7 @@ def run_bubble(args, dist):
 def main():
     args = parse()
     NU[:] = [args.nu1, args.nu2]
+    OMEGA[0] = args.beta
     if args.n is None:
         args.n = 512 if args.workload == "rising_bubble" else 256
     dist = Dist()

@@ -278,7 +278,9 @@ typedef struct paris_solve_opts {
     double  max_error;   /* stop when the residual norm (order `norm`, RMS) < max_error:
                             the reference's maxError/MaxDt (paris.f90:499)              */
     double  rel_tol;     /* if > 0, stop instead when ||r||_2 / ||b||_2 < rel_tol        */
-    double  beta;        /* BETA, relaxation factor of RedBlackRelax                     */
+    double  beta;        /* BETA, relaxation factor of RedBlackRelax (newsolver.f90:229); the
+                            FP64/MIXED modes over-relax their red-black smoother by it too:
+                            x + beta (x_GS - x); 1 = Gauss-Seidel, <= 0 taken as 1        */
     int32_t maxit;       /* MAXIT                                                         */
     int32_t norm;        /* ResNormOrderPressure: 1 or 2                                  */
     int32_t mode;        /* PARIS_MG_*                                                    */

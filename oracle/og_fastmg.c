@@ -9,7 +9,9 @@
  *   - coarse faces = mean of the four fine faces / 4 (rediscretisation);
  *   - restriction = mean of the 8 children, prolongation = injection;
  *   - red-black Gauss-Seidel V(nu1,nu2) cycles, black-red after the
- *     coarse correction (symmetric cycle), coarsest level smoothed;
+ *     coarse correction (symmetric cycle), coarsest level smoothed; with a
+ *     relaxation factor w != 1 each update is x + w (x_GS - x) (the
+ *     reference's BETA of RedBlackRelax, newsolver.f90:229);
  *   - an FP64 outer loop: defect correction p += V(b - A p), or
  *     preconditioned CG with the V-cycle as preconditioner, with A applied
  *     in flux form b + sum_f a_f (x_f - x_c); CG checks the true residual
@@ -41,6 +43,7 @@ typedef struct {
     int mixed;
     int nu1, nu2;
     int coarse_sweeps;
+    double omega;   /* relaxation factor of the red-black smoother (1: Gauss-Seidel) */
 } fm_mg;
 
 #define FIDX(l, i, j, k) ((i) + (long)(l)->n[0] * ((j) + (long)(l)->n[1] * (k)))
@@ -83,7 +86,10 @@ static void smooth_##SUF(const fm_mg* mg, fm_level* l, const T* b, T* x, int col
                 FM_NBR(T, l, per, x, i, j, k, 0, 0, 1, pt);                                  \
                 T d = a1 + a2 + a3 + a4 + a5 + a6;                                           \
                 T s = a1 * pw + a2 * pe + a3 * ps + a4 * pn + a5 * pb + a6 * pt + b[q];       \
-                x[q] = d > (T)0 ? s / d : x[q];                                              \
+                if (d > (T)0) {                                                              \
+                    const T g = s / d, w = (T)mg->omega;                                     \
+                    x[q] = w == (T)1 ? g : x[q] + w * (g - x[q]);                            \
+                }                                                                            \
             }                                                                                \
 }                                                                                            \
 /* r = b - A x */                                                                            \
@@ -205,11 +211,12 @@ static double dot(const double* a, const double* b, long n) {
 /* A from SetupPoisson: fine face coefficient east = A2, north = A4, top = A6.
  * p, b: interior arrays (nx*ny*nz).  Returns cycles run; hist[it] = ||r||/||b||. */
 int og_fastmg_solve(const paris_grid_desc* desc, const double* A, double* p, double rel_tol,
-                    int maxit, int mixed, int pcg, int nu1, int nu2, double* hist) {
+                    int maxit, int mixed, int pcg, int nu1, int nu2, double omega, double* hist) {
     fm_mg mg;
     memset(&mg, 0, sizeof(mg));
     for (int a = 0; a < 3; a++) mg.per[a] = desc->bdry_cond[a] == PARIS_BC_PERIODIC;
     mg.mixed = mixed; mg.nu1 = nu1; mg.nu2 = nu2; mg.coarse_sweeps = 8;
+    mg.omega = omega > 0.0 ? omega : 1.0;
     int n0[3] = {desc->nx, desc->ny, desc->nz};
     int nl = 1;
     while (1) {

@@ -28,7 +28,14 @@ struct LV {
     T *b, *x;
     int n0, n1, n2;
     long N;
+    T omega;   // relaxation factor of the red-black smoother (1: Gauss-Seidel)
 };
+
+// x_new of a relaxed cell: the Gauss-Seidel value g, over-relaxed by w
+template <typename T>
+__device__ inline T relax(T g, T x0, T w) {
+    return w == (T)1 ? g : x0 + w * (g - x0);
+}
 
 template <typename T>
 struct LVSet {
@@ -64,7 +71,7 @@ __device__ inline void smooth_cell(const LV<T>& v, const Bnd& B, int i, int j, i
     nbrs(v, v.x, B, i, j, k, m, xw, xe, xs, xn, xb, xt);
     T d = a1 + a2 + a3 + a4 + a5 + a6;
     T s = a1 * xw + a2 * xe + a3 * xs + a4 * xn + a5 * xb + a6 * xt + v.b[m];
-    if (d > (T)0) v.x[m] = s / d;
+    if (d > (T)0) v.x[m] = relax(s / d, v.omega != (T)1 ? v.x[m] : (T)0, v.omega);
 }
 
 template <typename T>
@@ -199,7 +206,7 @@ __device__ inline void smooth_cell32(const LV<T>& v, const Bnd& B, int i, int j,
     T a2 = v.cx[m], a4 = v.cy[m], a6 = v.cz[m];
     T d = a1 + a2 + a3 + a4 + a5 + a6;
     T s = a1 * xw + a2 * xe + a3 * xs + a4 * xn + a5 * xb + a6 * xt + v.b[m];
-    if (d > (T)0) v.x[m] = s / d;
+    if (d > (T)0) v.x[m] = relax(s / d, v.omega != (T)1 ? v.x[m] : (T)0, v.omega);
 }
 
 template <typename T>
@@ -394,7 +401,7 @@ struct Mat64 {
 
 __device__ inline double ax_compact(const Mat64& A, const double* __restrict__ x, const Layout& L, const Bnd& B,
                                     int i, int j, int k, long m) {
-    LV<double> v{A.cx, A.cy, A.cz, nullptr, nullptr, L.n[0], L.n[1], L.n[2], 0};
+    LV<double> v{A.cx, A.cy, A.cz, nullptr, nullptr, L.n[0], L.n[1], L.n[2], 0, 1.0};
     double a1, a3, a5, xw, xe, xs, xn, xb, xt;
     west_coefs(v, B, i, j, k, m, a1, a3, a5);
     double a2 = A.cx[m], a4 = A.cy[m], a6 = A.cz[m];
@@ -672,7 +679,7 @@ static int fast_alloc(paris_ctx* c) {
 
 template <typename T>
 static LV<T> view(const FastLevel<T>& l) {
-    return LV<T>{l.cx, l.cy, l.cz, l.b, l.x, l.n[0], l.n[1], l.n[2], l.N};
+    return LV<T>{l.cx, l.cy, l.cz, l.b, l.x, l.n[0], l.n[1], l.n[2], l.N, (T)l.omega};
 }
 
 template <typename T>
@@ -1057,14 +1064,18 @@ int mg_fast_solve_into(paris_ctx* c, const paris_solve_opts* o, paris_solve_resu
         else
             shift = 0.0;
     }
+    // the smoother's relaxation factor: the reference's BETA of RedBlackRelax
+    const double omega = o->beta > 0.0 ? o->beta : 1.0;
     int st;
     if (o->mode == PARIS_MG_MIXED) {
         PARIS_CHECK(fast_alloc<float>(c));
         PARIS_CHECK(fast_coefs<float>(c));
+        for (auto& l : c->fl32) l.omega = omega;
         st = o->pcg ? solve_pcg<float>(c, o, res, rhs, x) : solve_dc<float>(c, o, res, rhs, x);
     } else {
         PARIS_CHECK(fast_alloc<double>(c));
         PARIS_CHECK(fast_coefs<double>(c));
+        for (auto& l : c->fl64) l.omega = omega;
         st = o->pcg ? solve_pcg<double>(c, o, res, rhs, x) : solve_dc<double>(c, o, res, rhs, x);
     }
     if (c->err_host && *c->err_host) {   // the kernels before the last reduction have completed

@@ -98,20 +98,21 @@ __device__ inline int sw_wrap(int a, int n, int per) {
 template <typename T>
 struct SwUpd {
     __device__ static inline bool apply(T a1, T a2, T a3, T a4, T a5, T a6, T x1, T x2, T x3, T x4, T x5, T x6, T b,
-                                        T& out) {
+                                        T x0, T w, T& out) {
         T d = a1 + a2 + a3 + a4 + a5 + a6;
         T s = a1 * x1 + a2 * x2 + a3 * x3 + a4 * x4 + a5 * x5 + a6 * x6 + b;
-        if (d > (T)0) { out = s / d; return true; }
+        if (d > (T)0) { out = relax(s / d, x0, w); return true; }
         return false;
     }
 };
 template <>
 struct SwUpd<float> {
     __device__ static inline bool apply(float a1, float a2, float a3, float a4, float a5, float a6, float x1,
-                                        float x2, float x3, float x4, float x5, float x6, float b, float& out) {
+                                        float x2, float x3, float x4, float x5, float x6, float b, float x0, float w,
+                                        float& out) {
         const float d = ((a1 + a2) + (a3 + a4)) + (a5 + a6);
         const float s = ((a1 * x1 + a2 * x2) + (a3 * x3 + a4 * x4)) + ((a5 * x5 + a6 * x6) + b);
-        if (d > 0.f) { out = __fdividef(s, d); return true; }
+        if (d > 0.f) { out = relax(__fdividef(s, d), x0, w); return true; }
         return false;
     }
 };
@@ -285,8 +286,9 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
                       const T* czk, const T* czm) {
         T a1 = cxk[r - 1], a2 = cxk[r], a3 = cyk[r - RX], a4 = cyk[r], a5 = czm[r], a6 = czk[r];
         T out;
+        const T x0 = v.omega != (T)1 ? xk[r] : (T)0;
         if (SwUpd<T>::apply(a1, a2, a3, a4, a5, a6, xk[r - 1], xk[r + 1], xk[r - RX], xk[r + RX], xm[r], xp[r], bk[r],
-                            out))
+                            x0, v.omega, out))
             xk[r] = out;
     };
     // F at plane k (tile + ring) and S at plane k (tile) with its output; the

@@ -191,8 +191,9 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
                       const T* czk, const T* czm) {
         T a1 = cxk[r - 1], a2 = cxk[r], a3 = cyk[r - RX], a4 = cyk[r], a5 = czm[r], a6 = czk[r];
         T out;
+        const T x0 = v.omega != (T)1 ? xk[r] : (T)0;
         if (SwUpd<T>::apply(a1, a2, a3, a4, a5, a6, xk[r - 1], xk[r + 1], xk[r - RX], xk[r + RX], xm[r], xp[r], bk[r],
-                            out))
+                            x0, v.omega, out))
             xk[r] = out;
     };
     // one colour (0: X, 1: Y) at plane k on the ring of this thread's pair,

@@ -20,7 +20,7 @@ from sweep_case import problem
 pytestmark = pytest.mark.gpu
 
 
-def _solve(runtime, capi, desc, cvof, vel, pairs, mode, pcg, nu=2):
+def _solve(runtime, capi, desc, cvof, vel, pairs, mode, pcg, nu=2, beta=1.0):
     old = os.environ.get("PARIS_SWEEP_PAIRS")
     os.environ["PARIS_SWEEP_PAIRS"] = "1" if pairs else "0"
     try:
@@ -31,7 +31,7 @@ def _solve(runtime, capi, desc, cvof, vel, pairs, mode, pcg, nu=2):
             gpu.linfunc(capi.F_RHO)
             gpu.setup_poisson(1e-3)
             gpu.fill_field(capi.F_P, 0.0)
-            r = gpu.new_solver(0.0, maxit=5, mode=mode, rel_tol=1e-300, pcg=pcg, nu1=nu, nu2=nu)
+            r = gpu.new_solver(0.0, beta=beta, maxit=5, mode=mode, rel_tol=1e-300, pcg=pcg, nu1=nu, nu2=nu)
             return gpu.download(capi.F_P), r
     finally:
         if old is None:
@@ -67,5 +67,19 @@ def test_pair_sweep_odd_and_repeated_passes(gpu_lib, capi, runtime, orc, workloa
         warnings.simplefilter("ignore")
         p_pair, r_pair = _solve(runtime, capi, desc, cvof, vel, True, capi.MG_MIXED, 1, nu)
         p_one, r_one = _solve(runtime, capi, desc, cvof, vel, False, capi.MG_MIXED, 1, nu)
+    assert r_pair.it == r_one.it
+    assert np.array_equal(p_pair, p_one)
+
+
+@pytest.mark.parametrize("mode", ["mixed", "fp64"])
+def test_pair_sweep_over_relaxed(gpu_lib, capi, runtime, orc, workloads, mode):
+    """With the smoother over-relaxed (the solver's beta, here 1.15) the two
+    forms still read the same values and give the same pressure to the bit."""
+    desc, cvof, vel = problem(capi, orc, workloads, (96, 48, 80), (1, 0, 1, 1, 0, 1), seed=13)
+    m = capi.MG_MIXED if mode == "mixed" else capi.MG_FP64
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        p_pair, r_pair = _solve(runtime, capi, desc, cvof, vel, True, m, 1, beta=1.15)
+        p_one, r_one = _solve(runtime, capi, desc, cvof, vel, False, m, 1, beta=1.15)
     assert r_pair.it == r_one.it
     assert np.array_equal(p_pair, p_one)

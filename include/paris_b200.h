@@ -286,7 +286,10 @@ typedef struct paris_solve_opts {
     int32_t mode;        /* PARIS_MG_*                                                    */
     int32_t nu1, nu2;    /* pre/post smoothing sweeps of the FP64/MIXED cycles (2,2)      */
     int32_t pcg;         /* FP64/MIXED: 1 = use the V-cycle as a CG preconditioner        */
-    int32_t reserved[3];
+    int32_t nu_coarse;   /* FP64/MIXED: if > 0, the pre- and post-smoothing sweeps on the
+                            levels from coarse_from down (nu1/nu2 above them)              */
+    int32_t coarse_from; /* the first level (0 = finest) that takes nu_coarse; 0 taken as 1 */
+    int32_t reserved;
 } paris_solve_opts;
 
 typedef struct paris_solve_result {

@@ -11,7 +11,8 @@
  *   - red-black Gauss-Seidel V(nu1,nu2) cycles, black-red after the
  *     coarse correction (symmetric cycle), coarsest level smoothed; with a
  *     relaxation factor w != 1 each update is x + w (x_GS - x) (the
- *     reference's BETA of RedBlackRelax, newsolver.f90:229);
+ *     reference's BETA of RedBlackRelax, newsolver.f90:229); optionally
+ *     nu_coarse sweeps each way on the levels from coarse_from down;
  *   - an FP64 outer loop: defect correction p += V(b - A p), or
  *     preconditioned CG with the V-cycle as preconditioner, with A applied
  *     in flux form b + sum_f a_f (x_f - x_c); CG checks the true residual
@@ -44,7 +45,11 @@ typedef struct {
     int nu1, nu2;
     int coarse_sweeps;
     double omega;   /* relaxation factor of the red-black smoother (1: Gauss-Seidel) */
+    int nu_coarse, coarse_from;   /* sweeps from level coarse_from down, when nu_coarse > 0 */
 } fm_mg;
+
+/* sweeps of a smoothing pass on level L: nu, or nu_coarse from level coarse_from down */
+#define FM_NU(mg, L, nu) ((mg)->nu_coarse > 0 && (L) >= (mg)->coarse_from ? (mg)->nu_coarse : (nu))
 
 #define FIDX(l, i, j, k) ((i) + (long)(l)->n[0] * ((j) + (long)(l)->n[1] * (k)))
 
@@ -166,7 +171,7 @@ static void vcycle_##SUF(const fm_mg* mg, int L, T* const* B, T* const* X, T* co
         }                                                                                    \
         return;                                                                              \
     }                                                                                        \
-    for (int s = 0; s < mg->nu1; s++) {                                                      \
+    for (int s = 0; s < FM_NU(mg, L, mg->nu1); s++) {                                         \
         smooth_##SUF(mg, l, B[L], X[L], 0);                                                  \
         smooth_##SUF(mg, l, B[L], X[L], 1);                                                  \
     }                                                                                        \
@@ -175,7 +180,7 @@ static void vcycle_##SUF(const fm_mg* mg, int L, T* const* B, T* const* X, T* co
     memset(X[L + 1], 0, mg->L[L + 1].N * sizeof(T));                                         \
     vcycle_##SUF(mg, L + 1, B, X, R);                                                        \
     prolong_##SUF(l, &mg->L[L + 1], X[L + 1], X[L]);                                         \
-    for (int s = 0; s < mg->nu2; s++) {                                                      \
+    for (int s = 0; s < FM_NU(mg, L, mg->nu2); s++) {                                         \
         smooth_##SUF(mg, l, B[L], X[L], 1);                                                  \
         smooth_##SUF(mg, l, B[L], X[L], 0);                                                  \
     }                                                                                        \
@@ -211,12 +216,15 @@ static double dot(const double* a, const double* b, long n) {
 /* A from SetupPoisson: fine face coefficient east = A2, north = A4, top = A6.
  * p, b: interior arrays (nx*ny*nz).  Returns cycles run; hist[it] = ||r||/||b||. */
 int og_fastmg_solve(const paris_grid_desc* desc, const double* A, double* p, double rel_tol,
-                    int maxit, int mixed, int pcg, int nu1, int nu2, double omega, double* hist) {
+                    int maxit, int mixed, int pcg, int nu1, int nu2, double omega, int nu_coarse,
+                    int coarse_from, double* hist) {
     fm_mg mg;
     memset(&mg, 0, sizeof(mg));
     for (int a = 0; a < 3; a++) mg.per[a] = desc->bdry_cond[a] == PARIS_BC_PERIODIC;
     mg.mixed = mixed; mg.nu1 = nu1; mg.nu2 = nu2; mg.coarse_sweeps = 8;
     mg.omega = omega > 0.0 ? omega : 1.0;
+    mg.nu_coarse = nu_coarse > 0 ? nu_coarse : 0;
+    mg.coarse_from = coarse_from > 0 ? coarse_from : 1;
     int n0[3] = {desc->nx, desc->ny, desc->nz};
     int nl = 1;
     while (1) {

@@ -31,6 +31,9 @@ struct LV {
     T omega;   // relaxation factor of the red-black smoother (1: Gauss-Seidel)
 };
 
+// sweeps of a smoothing pass on level L: nu, or nuc from level cf down
+__host__ __device__ inline int nu_at(int L, int nu, int nuc, int cf) { return nuc > 0 && L >= cf ? nuc : nu; }
+
 // x_new of a relaxed cell: the Gauss-Seidel value g, over-relaxed by w
 template <typename T>
 __device__ inline T relax(T g, T x0, T w) {
@@ -244,7 +247,7 @@ __device__ inline int div_small(int t, int d, float rd) {
 // level L0 is written back.
 template <typename T>
 __global__ void __launch_bounds__(1024) k_fast_coarse_cycle(const LVSet<T> G, int L0, int nl, const Bnd B, int nu1,
-                                                            int nu2, int in_smem) {
+                                                            int nu2, int nuc, int cf, int in_smem) {
     const int tid = threadIdx.x, nt = blockDim.x;
     extern __shared__ __align__(16) unsigned char cc_raw[];
     __shared__ LV<T> S[kMaxLevels];   // level views, read by value in every phase
@@ -305,7 +308,7 @@ __global__ void __launch_bounds__(1024) k_fast_coarse_cycle(const LVSet<T> G, in
             for (int s = 0; s < kCoarseSweeps; s++) { smooth(v, 1, warp); smooth(v, 0, warp); }
             return;
         }
-        for (int s = 0; s < nu1; s++) { smooth(v, 0, warp); smooth(v, 1, warp); }
+        for (int s = 0; s < nu_at(L, nu1, nuc, cf); s++) { smooth(v, 0, warp); smooth(v, 1, warp); }
         const LV<T> c = S[L + 1];
         const int cn = c.n0 * c.n1;
         const float rcn = 1.0f / (float)cn, rc0 = 1.0f / (float)c.n0;
@@ -329,7 +332,7 @@ __global__ void __launch_bounds__(1024) k_fast_coarse_cycle(const LVSet<T> G, in
         }
         if (warp) __syncwarp();
         else __syncthreads();
-        for (int s = 0; s < nu2; s++) { smooth(v, 1, warp); smooth(v, 0, warp); }
+        for (int s = 0; s < nu_at(L, nu2, nuc, cf); s++) { smooth(v, 1, warp); smooth(v, 0, warp); }
     };
     int Lw = L0;   // first level worked by warp 0
     while (Lw < nl && S[Lw].N > kWarpCells) Lw++;
@@ -797,10 +800,12 @@ static LV<T> view_x(const FastLevel<T>& l, T* x) {
     return v;
 }
 
-// one V(nu1,nu2) cycle on level 0 from x0 = 0 with the right-hand side in b0;
+// one V(nu1,nu2) cycle on level 0 from x0 = 0 with the right-hand side in b0
+// (nuc sweeps each way instead on the levels from cf down, when nuc > 0);
 // *x0 receives the buffer holding the level-0 result (lv[0].x or lv[0].x2)
 template <typename T>
-static int vcycle(paris_ctx* c, int nu1, int nu2, T** x0) {
+static int vcycle(paris_ctx* c, int nu1_, int nu2_, T** x0) {
+    const int nuc = c->fast_nuc, cf = c->fast_cf;
     auto& lv = levels<T>(c);
     int nl = (int)lv.size();
     int Lc = 0;
@@ -808,6 +813,7 @@ static int vcycle(paris_ctx* c, int nu1, int nu2, T** x0) {
     T* cur[kMaxLevels];
     for (int L = 0; L < Lc; L++) {
         const FastLevel<T>& l = lv[L];
+        const int nu1 = nu_at(L, nu1_, nuc, cf);
         if (l.x2 && nu1 > 0) {
             const T* in = nullptr;
             T* out = l.x;
@@ -848,11 +854,12 @@ static int vcycle(paris_ctx* c, int nu1, int nu2, T** x0) {
                                                (int)csm));
         csm_set = csm;
     }
-    PARIS_LAUNCH_N(c, kname<T>("mg_coarse_cycle"), lv[Lc].N, k_fast_coarse_cycle<T>, 1, 1024, csm, S, Lc, nl, c->bnd, nu1, nu2,
-                   in_smem);
+    PARIS_LAUNCH_N(c, kname<T>("mg_coarse_cycle"), lv[Lc].N, k_fast_coarse_cycle<T>, 1, 1024, csm, S, Lc, nl, c->bnd, nu1_, nu2_,
+                   nuc, cf, in_smem);
     cur[Lc] = lv[Lc].x;
     for (int L = Lc - 1; L >= 0; L--) {
         const FastLevel<T>& l = lv[L];
+        const int nu2 = nu_at(L, nu2_, nuc, cf);
         if (l.x2 && nu2 > 0) {
             T* in = cur[L];
             for (int s = 0; s < nu2;) {
@@ -1066,6 +1073,10 @@ int mg_fast_solve_into(paris_ctx* c, const paris_solve_opts* o, paris_solve_resu
     }
     // the smoother's relaxation factor: the reference's BETA of RedBlackRelax
     const double omega = o->beta > 0.0 ? o->beta : 1.0;
+    // sweeps on the coarser levels (from coarse_from down) when nu_coarse > 0
+    if (o->nu_coarse < 0 || o->coarse_from < 0) return PARIS_BAD_ARGS;
+    c->fast_nuc = o->nu_coarse;
+    c->fast_cf = o->coarse_from > 0 ? o->coarse_from : 1;
     int st;
     if (o->mode == PARIS_MG_MIXED) {
         PARIS_CHECK(fast_alloc<float>(c));

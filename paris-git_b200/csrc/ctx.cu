@@ -208,6 +208,7 @@ extern "C" int paris_gpu_init(const paris_grid_desc* desc, paris_handle_t* out) 
     if (!s) s = upload_vec(c, &c->zh, c->h_zh);
     if (!s && cudaMalloc(&c->red_part, 8L * kRedBlocks * sizeof(double)) != cudaSuccess) s = PARIS_CUDA_ERROR;
     if (!s && cudaMalloc(&c->debris_count, sizeof(int)) != cudaSuccess) s = PARIS_CUDA_ERROR;
+    if (!s && cudaMalloc(&c->cg_scal, 8 * sizeof(double)) != cudaSuccess) s = PARIS_CUDA_ERROR;
     if (!s && cudaHostAlloc(&c->red_host, 8 * sizeof(double), cudaHostAllocMapped) != cudaSuccess) s = PARIS_CUDA_ERROR;
     if (!s && cudaHostAlloc(&c->err_host, sizeof(int), cudaHostAllocMapped) != cudaSuccess) s = PARIS_CUDA_ERROR;
     if (!s && cudaHostGetDevicePointer((void**)&c->err_dev, c->err_host, 0) != cudaSuccess) s = PARIS_CUDA_ERROR;
@@ -243,7 +244,7 @@ extern "C" int paris_gpu_finalize(paris_handle_t c) {
                     (void*)c->rhs, (void*)c->A, (void*)c->red_part, (void*)c->fast_r64,
                     (void*)c->fast_d64, (void*)c->fast_q64,
                     (void*)c->vflux, (void*)c->mixlist, (void*)c->mixsegn, (void*)c->kflag, (void*)c->st_list,
-                    (void*)c->st_count, (void*)c->debris_count, (void*)c->adj, (void*)c->stats_part, (void*)c->stats_out, (void*)c->mom_tab,
+                    (void*)c->st_count, (void*)c->debris_count, (void*)c->cg_scal, (void*)c->adj, (void*)c->stats_part, (void*)c->stats_out, (void*)c->mom_tab,
                     (void*)c->mc_tmp, (void*)c->mc_tmp2, (void*)c->mc_work, (void*)c->mc_fv, (void*)c->mc_flag,
                     (void*)c->mc_cg})
         free_ptr(p);

@@ -85,6 +85,7 @@ struct paris_ctx {
     double* fast_r64 = nullptr;    // PCG vectors (N each)
     double* fast_d64 = nullptr;
     double* fast_q64 = nullptr;
+    double* cg_scal = nullptr;     // device-side scalars of the CG loop (8 doubles, allocated at init)
     double* adj = nullptr;         // projection adjoint: 10 ghosted fields + N (allocated on first use)
     // asynchronous transfers: one stream per direction, a device staging copy
     // of each transferred field and the events that order them against `stream`

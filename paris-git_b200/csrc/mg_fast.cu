@@ -20,6 +20,10 @@ static constexpr int kMaxLevels = 16;
 static constexpr int kCoarseSweeps = 8;
 static constexpr long kWarpCells = 64;   // coarse levels of at most 4^3 cells run in one warp
 static constexpr long kFusedCells = 1L << 15;
+// device-side scalars of the CG loop (paris_ctx::cg_scal): r.z of the two
+// latest preconditioned residuals (alternating), d.q, and r.r, sum |r|, r.z_old
+// from the update
+static constexpr int kScRZ0 = 0, kScDQ = 2, kScRR = 3, kScRZold = 5;
 static constexpr size_t kCoarseSmemMax = 227 * 1024;   // opt-in shared memory per block   // levels of at least 64^3 cells use the fused sweep
 
 template <typename T>
@@ -481,8 +485,13 @@ __global__ void k_pcg_matvec(const Mat64 A, const double* __restrict__ d, double
 template <typename T>
 __global__ void k_pcg_update(double* __restrict__ p, double* __restrict__ r, const double* __restrict__ d,
                              const double* __restrict__ q, T* __restrict__ rT, const T* __restrict__ zold,
-                             double alpha, const Layout L, double* part) {
+                             const double* __restrict__ sc, int rzs, const Layout L, double* part) {
     __shared__ double sh[32];
+    // alpha = r.z / d.q from the device-side scalars; when d.q is not positive
+    // nothing is written and the host leaves the loop with p and r as they were
+    const double dq = sc[kScDQ];
+    if (!(dq > 0.0)) return;
+    const double alpha = sc[rzs] / dq;
     double s2 = 0.0, s1 = 0.0, sz = 0.0;
     ROWS_BEGIN(L.n[0], L.n[1], L.n[2])
         long m = cidx(L.n[0], L.n[1], i, j, k);
@@ -516,11 +525,28 @@ __global__ void k_pcg_rz(const T* __restrict__ z, const double* __restrict__ r, 
     if (threadIdx.x == 0) part[blockIdx.x] = s0;
 }
 
-// d = z + beta d
+// d = z + beta d, beta = (r.z_new - r.z_old) / r.z (flexible Polak-Ribiere)
+// from the device-side scalars, or 0 when rzs_old < 0 (a fresh start)
 template <typename T>
-__global__ void k_pcg_dir(double* __restrict__ d, const T* __restrict__ z, double beta, long N) {
+__global__ void k_pcg_dir(double* __restrict__ d, const T* __restrict__ z, const double* __restrict__ sc, int rzs_new,
+                          int rzs_old, long N) {
+    const double beta = rzs_old < 0 ? 0.0 : (sc[rzs_new] - sc[kScRZold]) / sc[rzs_old];
     long m = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (m < N) d[m] = (double)z[m] + beta * d[m];
+}
+
+// the partials of slot blockIdx.x summed in the fixed order of k_reduce_slots,
+// into dev[slot] and, when host is given (mapped memory), host[slot]
+__global__ void k_cg_reduce(const double* __restrict__ part, double* dev, double* host, int nb) {
+    __shared__ double sh[32];
+    const int slot = blockIdx.x;
+    double v = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) v = v + part[(long)slot * kRedBlocks + b];
+    v = block_sum<256>(v, sh);
+    if (threadIdx.x == 0) {
+        dev[slot] = v;
+        if (host) host[slot] = v;
+    }
 }
 
 // ---- host side ---------------------------------------------------------------
@@ -942,13 +968,13 @@ static int alloc_vec(paris_ctx* c, double** p) {
 }
 
 // z = V(rT): one V-cycle on the right-hand side already in lv[0].b; returns
-// the buffer holding z and r.z
+// the buffer holding z; r.z goes to the device-side scalar slot rzs
 template <typename T>
-static int precondition(paris_ctx* c, int nu1, int nu2, T** z, double* rz) {
+static int precondition(paris_ctx* c, int nu1, int nu2, T** z, int rzs) {
     PARIS_CHECK(vcycle<T>(c, nu1, nu2, z));
     PARIS_LAUNCH_N(c, kname<T>("pcg_rz"), c->N, k_pcg_rz<T>, red_grid(c, k_pcg_rz<T>, 256), 256, 0, *z, c->fast_r64,
                    c->N, c->red_part);
-    PARIS_CHECK(ctx_reduce_finish(c, 1, rz));
+    PARIS_LAUNCH(c, k_cg_reduce, 1, 256, 0, c->red_part, c->cg_scal + rzs, (double*)nullptr, c->red_nb);
     return PARIS_OK;
 }
 
@@ -974,22 +1000,28 @@ static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result
     res->res0 = tres;
     int it = 0;
     int nu1 = o->nu1 > 0 ? o->nu1 : 2, nu2 = o->nu2 > 0 ? o->nu2 : 2;
-    double rz = 0.0;
+    // The scalars alpha and beta are formed on the device from the reduced
+    // dot products (cg_scal), so an iteration waits on the host once, for the
+    // residual norms after the update; r.z alternates between two slots.
+    int rzs = kScRZ0;
     T* z = nullptr;
+    double* const sc = c->cg_scal;
     if (!done) {
-        PARIS_CHECK(precondition<T>(c, nu1, nu2, &z, &rz));
-        PARIS_LAUNCH_N(c, kname<T>("pcg_dir"), c->N, k_pcg_dir<T>, div_up(c->N, 256), 256, 0, c->fast_d64, z, 0.0, c->N);
+        PARIS_CHECK(precondition<T>(c, nu1, nu2, &z, rzs));
+        PARIS_LAUNCH_N(c, kname<T>("pcg_dir"), c->N, k_pcg_dir<T>, div_up(c->N, 256), 256, 0, c->fast_d64, z, sc, rzs,
+                       -1, c->N);
     }
     int restarts = 0;
     while (!done && it < o->maxit) {
-        double dq;
         PARIS_LAUNCH_N(c, "pcg_matvec_fp64", c->N, k_pcg_matvec, red_grid(c, k_pcg_matvec, 256), kRowBlock, 0, A, c->fast_d64, c->fast_q64, c->L, c->bnd, c->red_part);
-        PARIS_CHECK(ctx_reduce_finish(c, 1, &dq));
-        if (!(dq > 0.0)) break;
-        double alpha = rz / dq;
-        PARIS_LAUNCH_N(c, kname<T>("pcg_update"), c->N, k_pcg_update<T>, red_grid(c, k_pcg_update<T>, 256), kRowBlock, 0, p, c->fast_r64, c->fast_d64, c->fast_q64, lv[0].b, z, alpha, c->L,
+        PARIS_LAUNCH(c, k_cg_reduce, 1, 256, 0, c->red_part, sc + kScDQ, c->red_host_dev + 3, c->red_nb);
+        PARIS_LAUNCH_N(c, kname<T>("pcg_update"), c->N, k_pcg_update<T>, red_grid(c, k_pcg_update<T>, 256), kRowBlock, 0, p, c->fast_r64, c->fast_d64, c->fast_q64, lv[0].b, z, sc, rzs, c->L,
                      c->red_part);
-        PARIS_CHECK(ctx_reduce_finish(c, 3, s));
+        PARIS_LAUNCH(c, k_cg_reduce, 3, 256, 0, c->red_part, sc + kScRR, c->red_host_dev, c->red_nb);
+        PARIS_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        const double dq = c->red_host[3];
+        for (int q = 0; q < 3; q++) s[q] = c->red_host[q];
+        if (!(dq > 0.0)) break;   // the update wrote nothing: p and r are as they were
         it++;
         done = converged(o, s[0], s[1], bn2, c->N, &tres, &rel);
         if (tres != tres) {
@@ -1006,16 +1038,17 @@ static int solve_pcg(paris_ctx* c, const paris_solve_opts* o, paris_solve_result
             done = converged(o, s[0], s[1], bn2, c->N, &tres, &rel);
             if (done || restarts == kMaxRestarts) break;
             restarts++;
-            PARIS_CHECK(precondition<T>(c, nu1, nu2, &z, &rz));
-            PARIS_LAUNCH_N(c, kname<T>("pcg_dir"), c->N, k_pcg_dir<T>, div_up(c->N, 256), 256, 0, c->fast_d64, z, 0.0,
-                           c->N);
+            rzs = kScRZ0 + 1 - rzs;
+            PARIS_CHECK(precondition<T>(c, nu1, nu2, &z, rzs));
+            PARIS_LAUNCH_N(c, kname<T>("pcg_dir"), c->N, k_pcg_dir<T>, div_up(c->N, 256), 256, 0, c->fast_d64, z, sc,
+                           rzs, -1, c->N);
             continue;
         }
-        double r_zold = s[2], rz_new;
-        PARIS_CHECK(precondition<T>(c, nu1, nu2, &z, &rz_new));
-        double beta = (rz_new - r_zold) / rz;   // flexible (Polak-Ribiere) form
-        rz = rz_new;
-        PARIS_LAUNCH_N(c, kname<T>("pcg_dir"), c->N, k_pcg_dir<T>, div_up(c->N, 256), 256, 0, c->fast_d64, z, beta, c->N);
+        const int rzs_new = kScRZ0 + 1 - rzs;
+        PARIS_CHECK(precondition<T>(c, nu1, nu2, &z, rzs_new));
+        PARIS_LAUNCH_N(c, kname<T>("pcg_dir"), c->N, k_pcg_dir<T>, div_up(c->N, 256), 256, 0, c->fast_d64, z, sc,
+                       rzs_new, rzs, c->N);
+        rzs = rzs_new;
     }
     res->it = done ? it : o->maxit + 1;
     res->res = tres;

@@ -700,7 +700,8 @@ def run_bubble(args, dist):
     peak, peak_kind = measured_peak()
     s0 = gpu.calc_stats(force_valid=0)
     k = [0]
-    solve = {"max_error": 0.0, "rel_tol": BUBBLE_REL_TOL, "maxit": 200, "mode": capi.MG_MIXED, "pcg": 1}
+    solve = {"max_error": 0.0, "rel_tol": BUBBLE_REL_TOL, "maxit": 200, "mode": capi.MG_MIXED, "pcg": 1,
+             "beta": OMEGA[0], "nu1": NU[0], "nu2": NU[1], "nu_coarse": NU[2], "coarse_from": NU[3]}
 
     def step():
         dt, _ = gpu.time_step_size(B["cfl"], B["max_dt"])     # TimeStepSize, dtFlag 2

@@ -80,12 +80,27 @@ __device__ inline double quick_same(const double* __restrict__ phi, long n, long
 __device__ inline QuickCoef pick(bool up, const QuickCoef& a, const QuickCoef& b) {
     return QuickCoef{up ? a.xi : b.xi, up ? a.k : b.k, up ? a.rk : b.rk, up ? a.r1k : b.r1k, up ? a.rkm1 : b.rkm1};
 }
+// inter_q<true> for the coefficients of every face of a uniform grid whose
+// coordinates are exact (xi = 1/2, k = -1, so k*k = 1, k*k - 1 = 0, k - 1 = -2,
+// 1/k = -1, 1/(1-k) = 1/2, 1/(k-1) = -1/2): the same IEEE operations with
+// those constants, the exact products by -1 folded into the scalings
+// ((x * -1) * 1/2 and x * -1/2 round alike), so the same double as inter_q
+__device__ inline double inter_canon(double y0, double y1, double y2) {
+    const double a = ((y2 - y1) + 0.0 * y0) * -0.5;
+    const double b = ((y2 + y1) + -2.0 * y0) * 0.5;
+    return (y0 + a * 0.5) + b * 0.25;
+}
+template <bool C>
+__device__ inline double inter_u(const QuickCoef& c, double y0, double y1, double y2) {
+    return C ? inter_canon(y0, y1, y2) : inter_q<true>(&c, y0, y1, y2);
+}
+template <bool C>
 __device__ inline double quick_same_u(const double* __restrict__ phi, long n, long st, const QuickCoef& cu,
                                       const QuickCoef& cd) {
     const double pm2 = phi[n - 2 * st], pm1 = phi[n - st], p0 = phi[n], pp1 = phi[n + st];
     const bool up = pm1 + p0 > 0.0;
-    const QuickCoef c = pick(up, cu, cd);
-    return inter_q<true>(&c, up ? pm1 : p0, up ? p0 : pm1, up ? pm2 : pp1);
+    const QuickCoef c = C ? cu : pick(up, cu, cd);
+    return inter_u<C>(c, up ? pm1 : p0, up ? p0 : pm1, up ? pm2 : pp1);
 }
 
 // QUICK value of a component on the face jj+1/2 of another axis, upwinded
@@ -98,13 +113,14 @@ __device__ inline double quick_cross(const double* __restrict__ phi, const doubl
     const bool up = v0 + v1 > 0.0;
     return inter_q<R>(Q + 4 * t + (up ? 2 : 3), up ? a : b, up ? b : a, up ? am : bp);
 }
+template <bool C>
 __device__ inline double quick_cross_u(const double* __restrict__ phi, const double* __restrict__ vel, long n, long st,
                                        long sc, const QuickCoef& cu, const QuickCoef& cd) {
     const double v0 = vel[n], v1 = vel[n + sc];
     const double am = phi[n - st], a = phi[n], b = phi[n + st], bp = phi[n + 2 * st];
     const bool up = v0 + v1 > 0.0;
-    const QuickCoef c = pick(up, cu, cd);
-    return inter_q<true>(&c, up ? a : b, up ? b : a, up ? am : bp);
+    const QuickCoef c = C ? cu : pick(up, cu, cd);
+    return inter_u<C>(c, up ? a : b, up ? b : a, up ? am : bp);
 }
 
 // x / den, or x * (1/den) where that reciprocal is exact (same double)
@@ -160,7 +176,9 @@ __global__ void __launch_bounds__(256) k_conv_quick(Vel V, double* __restrict__ 
     }
 }
 
-// momentumConvectionQUICK on a uniform grid with exact reciprocals
+// momentumConvectionQUICK on a uniform grid with exact reciprocals; C: every
+// coefficient set is the exact-coordinate one (inter_canon)
+template <bool C>
 __global__ void __launch_bounds__(256) k_conv_quick_uniform(Vel V, double* __restrict__ du, double* __restrict__ dv,
                                                             double* __restrict__ dw, const Layout L, const Bnd B,
                                                             const QuickUniform Q) {
@@ -169,31 +187,31 @@ __global__ void __launch_bounds__(256) k_conv_quick_uniform(Vel V, double* __res
     const long n = lidx(L, i, j, k), sx = 1, sy = L.pitch, sz = L.plane;
     const double *u = V.u, *v = V.v, *w = V.w;
     if (i < L.n[0] - 1 || B.per[0]) {
-        double a = quick_same_u(u, n + sx, sx, Q.q[0][0], Q.q[0][1]), b = quick_same_u(u, n, sx, Q.q[0][0], Q.q[0][1]);
-        double w2 = quick_cross_u(u, v, n, sy, sx, Q.q[1][2], Q.q[1][3]);
-        double w2m = quick_cross_u(u, v, n - sy, sy, sx, Q.q[1][2], Q.q[1][3]);
-        double w3 = quick_cross_u(u, w, n, sz, sx, Q.q[2][2], Q.q[2][3]);
-        double w3m = quick_cross_u(u, w, n - sz, sz, sx, Q.q[2][2], Q.q[2][3]);
+        double a = quick_same_u<C>(u, n + sx, sx, Q.q[0][0], Q.q[0][1]), b = quick_same_u<C>(u, n, sx, Q.q[0][0], Q.q[0][1]);
+        double w2 = quick_cross_u<C>(u, v, n, sy, sx, Q.q[1][2], Q.q[1][3]);
+        double w2m = quick_cross_u<C>(u, v, n - sy, sy, sx, Q.q[1][2], Q.q[1][3]);
+        double w3 = quick_cross_u<C>(u, w, n, sz, sx, Q.q[2][2], Q.q[2][3]);
+        double w3m = quick_cross_u<C>(u, w, n - sz, sz, sx, Q.q[2][2], Q.q[2][3]);
         du[n] = -(a * a - b * b) * Q.rdh[0]
             - (0.5 * ((v[n] + v[n + sx]) * w2 - (v[n - sy] + v[n + sx - sy]) * w2m)) * Q.rd[1]
             - (0.5 * ((w[n] + w[n + sx]) * w3 - (w[n - sz] + w[n + sx - sz]) * w3m)) * Q.rd[2];
     }
     if (j < L.n[1] - 1 || B.per[1]) {
-        double a = quick_same_u(v, n + sy, sy, Q.q[1][0], Q.q[1][1]), b = quick_same_u(v, n, sy, Q.q[1][0], Q.q[1][1]);
-        double w1 = quick_cross_u(v, u, n, sx, sy, Q.q[0][2], Q.q[0][3]);
-        double w1m = quick_cross_u(v, u, n - sx, sx, sy, Q.q[0][2], Q.q[0][3]);
-        double w3 = quick_cross_u(v, w, n, sz, sy, Q.q[2][2], Q.q[2][3]);
-        double w3m = quick_cross_u(v, w, n - sz, sz, sy, Q.q[2][2], Q.q[2][3]);
+        double a = quick_same_u<C>(v, n + sy, sy, Q.q[1][0], Q.q[1][1]), b = quick_same_u<C>(v, n, sy, Q.q[1][0], Q.q[1][1]);
+        double w1 = quick_cross_u<C>(v, u, n, sx, sy, Q.q[0][2], Q.q[0][3]);
+        double w1m = quick_cross_u<C>(v, u, n - sx, sx, sy, Q.q[0][2], Q.q[0][3]);
+        double w3 = quick_cross_u<C>(v, w, n, sz, sy, Q.q[2][2], Q.q[2][3]);
+        double w3m = quick_cross_u<C>(v, w, n - sz, sz, sy, Q.q[2][2], Q.q[2][3]);
         dv[n] = (-0.5 * ((u[n] + u[n + sy]) * w1 - (u[n - sx] + u[n - sx + sy]) * w1m)) * Q.rd[0]
             - (a * a - b * b) * Q.rdh[1]
             - (0.5 * ((w[n] + w[n + sy]) * w3 - (w[n - sz] + w[n + sy - sz]) * w3m)) * Q.rd[2];
     }
     if (k < L.n[2] - 1 || B.per[2]) {
-        double a = quick_same_u(w, n + sz, sz, Q.q[2][0], Q.q[2][1]), b = quick_same_u(w, n, sz, Q.q[2][0], Q.q[2][1]);
-        double w1 = quick_cross_u(w, u, n, sx, sz, Q.q[0][2], Q.q[0][3]);
-        double w1m = quick_cross_u(w, u, n - sx, sx, sz, Q.q[0][2], Q.q[0][3]);
-        double w2 = quick_cross_u(w, v, n, sy, sz, Q.q[1][2], Q.q[1][3]);
-        double w2m = quick_cross_u(w, v, n - sy, sy, sz, Q.q[1][2], Q.q[1][3]);
+        double a = quick_same_u<C>(w, n + sz, sz, Q.q[2][0], Q.q[2][1]), b = quick_same_u<C>(w, n, sz, Q.q[2][0], Q.q[2][1]);
+        double w1 = quick_cross_u<C>(w, u, n, sx, sz, Q.q[0][2], Q.q[0][3]);
+        double w1m = quick_cross_u<C>(w, u, n - sx, sx, sz, Q.q[0][2], Q.q[0][3]);
+        double w2 = quick_cross_u<C>(w, v, n, sy, sz, Q.q[1][2], Q.q[1][3]);
+        double w2m = quick_cross_u<C>(w, v, n - sy, sy, sz, Q.q[1][2], Q.q[1][3]);
         dw[n] = (-0.5 * ((u[n] + u[n + sz]) * w1 - (u[n - sx] + u[n - sx + sz]) * w1m)) * Q.rd[0]
             - (0.5 * ((v[n] + v[n + sz]) * w2 - (v[n - sy] + v[n - sy + sz]) * w2m)) * Q.rd[1]
             - (a * a - b * b) * Q.rdh[2];
@@ -527,8 +545,14 @@ extern "C" int paris_momentum_convection(paris_handle_t c, int32_t scheme) {
         QuickUniform U;
         bool exact, uniform;
         PARIS_CHECK(mom_tables(c, &T, &exact, &U, &uniform));
-        if (uniform)
-            PARIS_LAUNCH_N(c, "mom_convection", c->N, k_conv_quick_uniform, cgrid(c->L), cblock(), 0, vel(c),
+        bool canon = uniform;   // every coefficient set xi = 1/2, k = -1 exactly
+        for (int a = 0; a < 3 && canon; a++)
+            for (int v = 0; v < 4; v++) canon = canon && U.q[a][v].xi == 0.5 && U.q[a][v].k == -1.0;
+        if (canon)
+            PARIS_LAUNCH_N(c, "mom_convection", c->N, k_conv_quick_uniform<true>, cgrid(c->L), cblock(), 0, vel(c),
+                           c->fld[PARIS_FIELD_DU], c->fld[PARIS_FIELD_DV], c->fld[PARIS_FIELD_DW], c->L, c->bnd, U);
+        else if (uniform)
+            PARIS_LAUNCH_N(c, "mom_convection", c->N, k_conv_quick_uniform<false>, cgrid(c->L), cblock(), 0, vel(c),
                            c->fld[PARIS_FIELD_DU], c->fld[PARIS_FIELD_DV], c->fld[PARIS_FIELD_DW], c->L, c->bnd, U);
         else if (exact)
             PARIS_LAUNCH_N(c, "mom_convection", c->N, k_conv_quick<true>, cgrid(c->L), cblock(), 0, vel(c),

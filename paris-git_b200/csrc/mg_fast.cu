@@ -355,6 +355,219 @@ __global__ void __launch_bounds__(1024) k_fast_coarse_cycle(const LVSet<T> G, in
     }
 }
 
+// ---- the coarse cycle in shared memory ------------------------------------
+// The same cycle as k_fast_coarse_cycle, with every level of at most 16^3
+// cells held in the block's shared memory and addressed by element offsets
+// from one shared array (shared-memory loads rather than generic ones), the
+// neighbours of a cell taken branch-free (the wrapped or clamped index always
+// loaded, the value dropped at a wall), the cell indices of each thread
+// decomposed once per pass, and the restriction split into a pass over the
+// fine cells (their residuals into a scratch array) and one over the coarse
+// cells (the 8 residuals summed in the order restrict_cell32 sums them).
+// The arithmetic of every update, residual and sum is that of
+// smooth_cell32 / resid_cell32 / restrict_cell32.
+struct CcLvl {
+    int n0, n1, n2, N;
+    int cx, cy, cz, b, x;   // element offsets of the arrays in shared memory
+};
+
+struct CcNb {   // a cell's index and its six neighbours' (always valid), and which exist
+    int m, mw, me, ms, mn, mb, mt;
+    bool hw, he, hs, hn, hb, ht;
+};
+
+__device__ inline CcNb cc_nb(const CcLvl& l, const Bnd& B, int i, int j, int k) {
+    const int n0 = l.n0, n1 = l.n1, n2 = l.n2, sy = n0, sz = n0 * n1;
+    CcNb q;
+    q.m = i + sy * j + sz * k;
+    q.mw = i > 0 ? q.m - 1 : q.m + n0 - 1;
+    q.me = i < n0 - 1 ? q.m + 1 : q.m - (n0 - 1);
+    q.ms = j > 0 ? q.m - sy : q.m + sy * (n1 - 1);
+    q.mn = j < n1 - 1 ? q.m + sy : q.m - sy * (n1 - 1);
+    q.mb = k > 0 ? q.m - sz : q.m + sz * (n2 - 1);
+    q.mt = k < n2 - 1 ? q.m + sz : q.m - sz * (n2 - 1);
+    q.hw = i > 0 || B.per[0];
+    q.he = i < n0 - 1 || B.per[0];
+    q.hs = j > 0 || B.per[1];
+    q.hn = j < n1 - 1 || B.per[1];
+    q.hb = k > 0 || B.per[2];
+    q.ht = k < n2 - 1 || B.per[2];
+    return q;
+}
+
+template <typename T>
+__device__ inline void cc_terms(const T* sm, const CcLvl& l, const CcNb& q, T& a1, T& a2, T& a3, T& a4, T& a5, T& a6,
+                                T& xw, T& xe, T& xs, T& xn, T& xb, T& xt) {
+    const T* x = sm + l.x;
+    const T c1 = sm[l.cx + q.mw], c3 = sm[l.cy + q.ms], c5 = sm[l.cz + q.mb];
+    const T vw = x[q.mw], ve = x[q.me], vs = x[q.ms], vn = x[q.mn], vb = x[q.mb], vt = x[q.mt];
+    a1 = q.hw ? c1 : (T)0;
+    a3 = q.hs ? c3 : (T)0;
+    a5 = q.hb ? c5 : (T)0;
+    xw = q.hw ? vw : (T)0;
+    xe = q.he ? ve : (T)0;
+    xs = q.hs ? vs : (T)0;
+    xn = q.hn ? vn : (T)0;
+    xb = q.hb ? vb : (T)0;
+    xt = q.ht ? vt : (T)0;
+    a2 = sm[l.cx + q.m];
+    a4 = sm[l.cy + q.m];
+    a6 = sm[l.cz + q.m];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) k_coarse_cycle_smem(const LVSet<T> G, int L0, int nl, const Bnd B, int nu1,
+                                                            int nu2, int nuc, int cf, int scratch) {
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
+    extern __shared__ __align__(16) unsigned char cc_raw[];
+    T* const sm = reinterpret_cast<T*>(cc_raw);
+    __shared__ CcLvl S[kMaxLevels];
+    __shared__ T omg[kMaxLevels];
+    if (tid == 0) {
+        int off = 0;
+        for (int L = L0; L < nl; L++) {
+            const LV<T>& g = G.l[L];
+            const int N = (int)g.N;
+            S[L] = CcLvl{g.n0, g.n1, g.n2, N, off, off + N, off + 2 * N, off + 3 * N, off + 4 * N};
+            omg[L] = g.omega;
+            off += 5 * N;
+        }
+    }
+    __syncthreads();
+    // the coefficients of every level and the right-hand side of L0, four
+    // loads in flight per thread and array
+    for (int L = L0; L < nl; L++) {
+        const LV<T>& g = G.l[L];
+        const CcLvl l = S[L];
+        for (int t0 = tid; t0 < l.N; t0 += 4 * nt) {
+            T v[4][4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int t = t0 + u * nt;
+                if (t < l.N) {
+                    v[u][0] = g.cx[t];
+                    v[u][1] = g.cy[t];
+                    v[u][2] = g.cz[t];
+                    v[u][3] = L == L0 ? g.b[t] : (T)0;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int t = t0 + u * nt;
+                if (t < l.N) {
+                    sm[l.cx + t] = v[u][0];
+                    sm[l.cy + t] = v[u][1];
+                    sm[l.cz + t] = v[u][2];
+                    if (L == L0) sm[l.b + t] = v[u][3];
+                }
+            }
+        }
+    }
+    __syncthreads();
+    auto sync = [&](bool warp) {
+        if (warp) __syncwarp();
+        else __syncthreads();
+    };
+    // one colour pass of red-black Gauss-Seidel over level l
+    auto smooth = [&](const CcLvl& l, T w, int color, bool warp) {
+        const int t0 = warp ? lane : tid, st = warp ? 32 : nt;
+        const int h0 = (l.n0 + 1) >> 1, hn = h0 * l.n1;
+        const int tot = hn * l.n2;
+        const float rhn = 1.0f / (float)hn, rh0 = 1.0f / (float)h0;
+        for (int t = t0; t < tot; t += st) {
+            const int k = div_small(t, hn, rhn), r = t - k * hn;
+            const int j = div_small(r, h0, rh0), ih = r - j * h0;
+            const int i = 2 * ih + ((j + k + color) & 1);
+            if (i >= l.n0) continue;
+            const CcNb q = cc_nb(l, B, i, j, k);
+            T a1, a2, a3, a4, a5, a6, xw, xe, xs, xn, xb, xt;
+            cc_terms(sm, l, q, a1, a2, a3, a4, a5, a6, xw, xe, xs, xn, xb, xt);
+            T d = a1 + a2 + a3 + a4 + a5 + a6;
+            T s = a1 * xw + a2 * xe + a3 * xs + a4 * xn + a5 * xb + a6 * xt + sm[l.b + q.m];
+            T* x = sm + l.x;
+            if (d > (T)0) x[q.m] = relax(s / d, w != (T)1 ? x[q.m] : (T)0, w);
+        }
+        sync(warp);
+    };
+    auto down = [&](int L, bool warp) {   // zero, pre-smooth and restrict level L, or solve the coarsest
+        const int t0 = warp ? lane : tid, st = warp ? 32 : nt;
+        const CcLvl l = S[L];
+        const T w = omg[L];
+        for (int t = t0; t < l.N; t += st) sm[l.x + t] = (T)0;
+        sync(warp);
+        if (L == nl - 1) {
+            for (int s = 0; s < kCoarseSweeps; s++) { smooth(l, w, 0, warp); smooth(l, w, 1, warp); }
+            for (int s = 0; s < kCoarseSweeps; s++) { smooth(l, w, 1, warp); smooth(l, w, 0, warp); }
+            return;
+        }
+        for (int s = 0; s < nu_at(L, nu1, nuc, cf); s++) { smooth(l, w, 0, warp); smooth(l, w, 1, warp); }
+        // residuals of the fine cells into the scratch array
+        {
+            const int fn = l.n0 * l.n1;
+            const float rfn = 1.0f / (float)fn, rf0 = 1.0f / (float)l.n0;
+            for (int t = t0; t < l.N; t += st) {
+                const int k = div_small(t, fn, rfn), r = t - k * fn;
+                const int j = div_small(r, l.n0, rf0), i = r - j * l.n0;
+                const CcNb q = cc_nb(l, B, i, j, k);
+                T a1, a2, a3, a4, a5, a6, xw, xe, xs, xn, xb, xt;
+                cc_terms(sm, l, q, a1, a2, a3, a4, a5, a6, xw, xe, xs, xn, xb, xt);
+                T d = a1 + a2 + a3 + a4 + a5 + a6;
+                sm[scratch + q.m] =
+                    sm[l.b + q.m] - d * sm[l.x + q.m] + a1 * xw + a2 * xe + a3 * xs + a4 * xn + a5 * xb + a6 * xt;
+            }
+        }
+        sync(warp);
+        // the coarse right-hand side: the mean of each 2x2x2 block
+        {
+            const CcLvl c = S[L + 1];
+            const int cn = c.n0 * c.n1;
+            const float rcn = 1.0f / (float)cn, rc0 = 1.0f / (float)c.n0;
+            const int sy = l.n0, sz = l.n0 * l.n1;
+            for (int t = t0; t < c.N; t += st) {
+                const int k = div_small(t, cn, rcn), r = t - k * cn;
+                const int j = div_small(r, c.n0, rc0), i = r - j * c.n0;
+                const int f = 2 * i + sy * (2 * j) + sz * (2 * k);
+                T s = 0;
+                for (int dk = 0; dk < 2; dk++)
+                    for (int dj = 0; dj < 2; dj++)
+                        for (int di = 0; di < 2; di++) s += sm[scratch + f + di + sy * dj + sz * dk];
+                sm[c.b + t] = (T)0.125 * s;
+            }
+        }
+        sync(warp);
+    };
+    auto up = [&](int L, bool warp) {     // prolong into level L and post-smooth it
+        const int t0 = warp ? lane : tid, st = warp ? 32 : nt;
+        const CcLvl l = S[L], c = S[L + 1];
+        const T w = omg[L];
+        const int fn = l.n0 * l.n1;
+        const float rfn = 1.0f / (float)fn, rf0 = 1.0f / (float)l.n0;
+        for (int t = t0; t < l.N; t += st) {
+            const int k = div_small(t, fn, rfn), r = t - k * fn;
+            const int j = div_small(r, l.n0, rf0), i = r - j * l.n0;
+            sm[l.x + t] += sm[c.x + (i >> 1) + c.n0 * ((j >> 1) + c.n1 * (k >> 1))];
+        }
+        sync(warp);
+        for (int s = 0; s < nu_at(L, nu2, nuc, cf); s++) { smooth(l, w, 1, warp); smooth(l, w, 0, warp); }
+    };
+    int Lw = L0;   // first level worked by warp 0
+    while (Lw < nl && S[Lw].N > kWarpCells) Lw++;
+    for (int L = L0; L < Lw; L++) down(L, false);
+    if (Lw < nl) {
+        if (tid < 32) {
+            for (int L = Lw; L < nl; L++) down(L, true);
+            for (int L = nl - 2; L >= Lw; L--) up(L, true);
+        }
+        __syncthreads();
+    }
+    for (int L = min(Lw, nl - 1) - 1; L >= L0; L--) up(L, false);
+    {
+        const LV<T>& g = G.l[L0];
+        const CcLvl l = S[L0];
+        for (int t = tid; t < l.N; t += nt) g.x[t] = sm[l.x + t];
+    }
+}
+
 // shared memory of k_fast_coarse_cycle: five arrays per level from L0 down
 template <typename T>
 static size_t coarse_smem(const std::vector<FastLevel<T>>& lv, int L0) {
@@ -871,17 +1084,24 @@ static int vcycle(paris_ctx* c, int nu1_, int nu2_, T** x0) {
     LVSet<T> S;
     for (int L = 0; L < nl; L++) S.l[L] = view(lv[L]);
     // the levels run in shared memory when they fit (always for L0 <= 16^3)
-    size_t csm = coarse_smem(lv, Lc);
+    // (the shared-memory cycle adds a scratch array of the largest restricted level)
+    const size_t scratch = coarse_smem(lv, Lc) / sizeof(T);
+    size_t csm = coarse_smem(lv, Lc) + (Lc < nl - 1 ? (size_t)lv[Lc].N * sizeof(T) : 0);
     const int in_smem = csm <= kCoarseSmemMax ? 1 : 0;
     if (!in_smem) csm = 0;
-    static size_t csm_set = 0;   // opt-in size set for this instantiation
-    if (csm > csm_set) {
-        PARIS_CUDA_TRY(c, cudaFuncSetAttribute(k_fast_coarse_cycle<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)csm));
-        csm_set = csm;
+    if (in_smem) {
+        static size_t csm_set = 0;   // opt-in size set for this instantiation
+        if (csm > csm_set) {
+            PARIS_CUDA_TRY(c, cudaFuncSetAttribute(k_coarse_cycle_smem<T>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+            csm_set = csm;
+        }
+        PARIS_LAUNCH_N(c, kname<T>("mg_coarse_cycle"), lv[Lc].N, k_coarse_cycle_smem<T>, 1, 1024, csm, S, Lc, nl,
+                       c->bnd, nu1_, nu2_, nuc, cf, (int)scratch);
+    } else {
+        PARIS_LAUNCH_N(c, kname<T>("mg_coarse_cycle"), lv[Lc].N, k_fast_coarse_cycle<T>, 1, 1024, 0, S, Lc, nl,
+                       c->bnd, nu1_, nu2_, nuc, cf, 0);
     }
-    PARIS_LAUNCH_N(c, kname<T>("mg_coarse_cycle"), lv[Lc].N, k_fast_coarse_cycle<T>, 1, 1024, csm, S, Lc, nl, c->bnd, nu1_, nu2_,
-                   nuc, cf, in_smem);
     cur[Lc] = lv[Lc].x;
     for (int L = Lc - 1; L >= 0; L--) {
         const FastLevel<T>& l = lv[L];

@@ -289,7 +289,7 @@ typedef struct paris_solve_opts {
     int32_t nu_coarse;   /* FP64/MIXED: if > 0, the pre- and post-smoothing sweeps on the
                             levels from coarse_from down (nu1/nu2 above them)              */
     int32_t coarse_from; /* the first level (0 = finest) that takes nu_coarse; 0 taken as 1 */
-    int32_t reserved;
+    int32_t coarse_to;   /* the last level that takes nu_coarse (0: every level below coarse_from) */
 } paris_solve_opts;
 
 typedef struct paris_solve_result {

@@ -12,7 +12,7 @@
  *     coarse correction (symmetric cycle), coarsest level smoothed; with a
  *     relaxation factor w != 1 each update is x + w (x_GS - x) (the
  *     reference's BETA of RedBlackRelax, newsolver.f90:229); optionally
- *     nu_coarse sweeps each way on the levels from coarse_from down;
+ *     nu_coarse sweeps each way on the levels coarse_from..coarse_to;
  *   - an FP64 outer loop: defect correction p += V(b - A p), or
  *     preconditioned CG with the V-cycle as preconditioner, with A applied
  *     in flux form b + sum_f a_f (x_f - x_c); CG checks the true residual
@@ -45,11 +45,15 @@ typedef struct {
     int nu1, nu2;
     int coarse_sweeps;
     double omega;   /* relaxation factor of the red-black smoother (1: Gauss-Seidel) */
-    int nu_coarse, coarse_from;   /* sweeps from level coarse_from down, when nu_coarse > 0 */
+    int nu_coarse, coarse_from, coarse_to;   /* sweeps on the levels coarse_from..coarse_to, when nu_coarse > 0 */
 } fm_mg;
 
-/* sweeps of a smoothing pass on level L: nu, or nu_coarse from level coarse_from down */
-#define FM_NU(mg, L, nu) ((mg)->nu_coarse > 0 && (L) >= (mg)->coarse_from ? (mg)->nu_coarse : (nu))
+/* sweeps of a smoothing pass on level L: nu, or nu_coarse on the levels coarse_from..coarse_to
+ * (coarse_to <= 0: every level from coarse_from down) */
+#define FM_NU(mg, L, nu)                                                                    \
+    ((mg)->nu_coarse > 0 && (L) >= (mg)->coarse_from && ((mg)->coarse_to <= 0 || (L) <= (mg)->coarse_to) \
+         ? (mg)->nu_coarse                                                                   \
+         : (nu))
 
 #define FIDX(l, i, j, k) ((i) + (long)(l)->n[0] * ((j) + (long)(l)->n[1] * (k)))
 
@@ -217,7 +221,7 @@ static double dot(const double* a, const double* b, long n) {
  * p, b: interior arrays (nx*ny*nz).  Returns cycles run; hist[it] = ||r||/||b||. */
 int og_fastmg_solve(const paris_grid_desc* desc, const double* A, double* p, double rel_tol,
                     int maxit, int mixed, int pcg, int nu1, int nu2, double omega, int nu_coarse,
-                    int coarse_from, double* hist) {
+                    int coarse_from, int coarse_to, double* hist) {
     fm_mg mg;
     memset(&mg, 0, sizeof(mg));
     for (int a = 0; a < 3; a++) mg.per[a] = desc->bdry_cond[a] == PARIS_BC_PERIODIC;
@@ -225,6 +229,7 @@ int og_fastmg_solve(const paris_grid_desc* desc, const double* A, double* p, dou
     mg.omega = omega > 0.0 ? omega : 1.0;
     mg.nu_coarse = nu_coarse > 0 ? nu_coarse : 0;
     mg.coarse_from = coarse_from > 0 ? coarse_from : 1;
+    mg.coarse_to = coarse_to > 0 ? coarse_to : 0;
     int n0[3] = {desc->nx, desc->ny, desc->nz};
     int nl = 1;
     while (1) {

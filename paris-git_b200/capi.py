@@ -67,8 +67,7 @@ class SolveOpts(ctypes.Structure):
         ("mode", ctypes.c_int32),
         ("nu1", ctypes.c_int32), ("nu2", ctypes.c_int32),
         ("pcg", ctypes.c_int32),
-        ("nu_coarse", ctypes.c_int32), ("coarse_from", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("nu_coarse", ctypes.c_int32), ("coarse_from", ctypes.c_int32), ("coarse_to", ctypes.c_int32),
     ]
 
 

@@ -79,7 +79,7 @@ struct paris_ctx {
     int ref_lmg = 0;
     std::vector<RefLevel> ref;     // index 1..LMG
     int fast_nl = 0;
-    int fast_nuc = 0, fast_cf = 1;   // sweeps on the levels from fast_cf down (0: nu1/nu2), set by each solve
+    int fast_nuc = 0, fast_cf = 1, fast_ct = 0;   // sweeps on the levels fast_cf..fast_ct (0: nu1/nu2), set by each solve
     std::vector<FastLevel<float>> fl32;
     std::vector<FastLevel<double>> fl64;
     double* fast_r64 = nullptr;    // PCG vectors (N each)

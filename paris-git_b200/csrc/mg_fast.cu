@@ -35,8 +35,11 @@ struct LV {
     T omega;   // relaxation factor of the red-black smoother (1: Gauss-Seidel)
 };
 
-// sweeps of a smoothing pass on level L: nu, or nuc from level cf down
-__host__ __device__ inline int nu_at(int L, int nu, int nuc, int cf) { return nuc > 0 && L >= cf ? nuc : nu; }
+// sweeps of a smoothing pass on level L: nu, or nuc on the levels cf..ct
+// (ct <= 0: every level from cf down)
+__host__ __device__ inline int nu_at(int L, int nu, int nuc, int cf, int ct) {
+    return nuc > 0 && L >= cf && (ct <= 0 || L <= ct) ? nuc : nu;
+}
 
 // x_new of a relaxed cell: the Gauss-Seidel value g, over-relaxed by w
 template <typename T>
@@ -251,7 +254,7 @@ __device__ inline int div_small(int t, int d, float rd) {
 // level L0 is written back.
 template <typename T>
 __global__ void __launch_bounds__(1024) k_fast_coarse_cycle(const LVSet<T> G, int L0, int nl, const Bnd B, int nu1,
-                                                            int nu2, int nuc, int cf, int in_smem) {
+                                                            int nu2, int nuc, int cf, int ct, int in_smem) {
     const int tid = threadIdx.x, nt = blockDim.x;
     extern __shared__ __align__(16) unsigned char cc_raw[];
     __shared__ LV<T> S[kMaxLevels];   // level views, read by value in every phase
@@ -312,7 +315,7 @@ __global__ void __launch_bounds__(1024) k_fast_coarse_cycle(const LVSet<T> G, in
             for (int s = 0; s < kCoarseSweeps; s++) { smooth(v, 1, warp); smooth(v, 0, warp); }
             return;
         }
-        for (int s = 0; s < nu_at(L, nu1, nuc, cf); s++) { smooth(v, 0, warp); smooth(v, 1, warp); }
+        for (int s = 0; s < nu_at(L, nu1, nuc, cf, ct); s++) { smooth(v, 0, warp); smooth(v, 1, warp); }
         const LV<T> c = S[L + 1];
         const int cn = c.n0 * c.n1;
         const float rcn = 1.0f / (float)cn, rc0 = 1.0f / (float)c.n0;
@@ -336,7 +339,7 @@ __global__ void __launch_bounds__(1024) k_fast_coarse_cycle(const LVSet<T> G, in
         }
         if (warp) __syncwarp();
         else __syncthreads();
-        for (int s = 0; s < nu_at(L, nu2, nuc, cf); s++) { smooth(v, 1, warp); smooth(v, 0, warp); }
+        for (int s = 0; s < nu_at(L, nu2, nuc, cf, ct); s++) { smooth(v, 1, warp); smooth(v, 0, warp); }
     };
     int Lw = L0;   // first level worked by warp 0
     while (Lw < nl && S[Lw].N > kWarpCells) Lw++;
@@ -417,7 +420,7 @@ __device__ inline void cc_terms(const T* sm, const CcLvl& l, const CcNb& q, T& a
 
 template <typename T>
 __global__ void __launch_bounds__(1024) k_coarse_cycle_smem(const LVSet<T> G, int L0, int nl, const Bnd B, int nu1,
-                                                            int nu2, int nuc, int cf, int scratch) {
+                                                            int nu2, int nuc, int cf, int ct, int scratch) {
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
     extern __shared__ __align__(16) unsigned char cc_raw[];
     T* const sm = reinterpret_cast<T*>(cc_raw);
@@ -500,7 +503,7 @@ __global__ void __launch_bounds__(1024) k_coarse_cycle_smem(const LVSet<T> G, in
             for (int s = 0; s < kCoarseSweeps; s++) { smooth(l, w, 1, warp); smooth(l, w, 0, warp); }
             return;
         }
-        for (int s = 0; s < nu_at(L, nu1, nuc, cf); s++) { smooth(l, w, 0, warp); smooth(l, w, 1, warp); }
+        for (int s = 0; s < nu_at(L, nu1, nuc, cf, ct); s++) { smooth(l, w, 0, warp); smooth(l, w, 1, warp); }
         // residuals of the fine cells into the scratch array
         {
             const int fn = l.n0 * l.n1;
@@ -548,7 +551,7 @@ __global__ void __launch_bounds__(1024) k_coarse_cycle_smem(const LVSet<T> G, in
             sm[l.x + t] += sm[c.x + (i >> 1) + c.n0 * ((j >> 1) + c.n1 * (k >> 1))];
         }
         sync(warp);
-        for (int s = 0; s < nu_at(L, nu2, nuc, cf); s++) { smooth(l, w, 1, warp); smooth(l, w, 0, warp); }
+        for (int s = 0; s < nu_at(L, nu2, nuc, cf, ct); s++) { smooth(l, w, 1, warp); smooth(l, w, 0, warp); }
     };
     int Lw = L0;   // first level worked by warp 0
     while (Lw < nl && S[Lw].N > kWarpCells) Lw++;
@@ -1040,11 +1043,11 @@ static LV<T> view_x(const FastLevel<T>& l, T* x) {
 }
 
 // one V(nu1,nu2) cycle on level 0 from x0 = 0 with the right-hand side in b0
-// (nuc sweeps each way instead on the levels from cf down, when nuc > 0);
+// (nuc sweeps each way instead on the levels cf..ct, when nuc > 0);
 // *x0 receives the buffer holding the level-0 result (lv[0].x or lv[0].x2)
 template <typename T>
 static int vcycle(paris_ctx* c, int nu1_, int nu2_, T** x0) {
-    const int nuc = c->fast_nuc, cf = c->fast_cf;
+    const int nuc = c->fast_nuc, cf = c->fast_cf, ct = c->fast_ct;
     auto& lv = levels<T>(c);
     int nl = (int)lv.size();
     int Lc = 0;
@@ -1052,7 +1055,7 @@ static int vcycle(paris_ctx* c, int nu1_, int nu2_, T** x0) {
     T* cur[kMaxLevels];
     for (int L = 0; L < Lc; L++) {
         const FastLevel<T>& l = lv[L];
-        const int nu1 = nu_at(L, nu1_, nuc, cf);
+        const int nu1 = nu_at(L, nu1_, nuc, cf, ct);
         if (l.x2 && nu1 > 0) {
             const T* in = nullptr;
             T* out = l.x;
@@ -1097,15 +1100,15 @@ static int vcycle(paris_ctx* c, int nu1_, int nu2_, T** x0) {
             csm_set = csm;
         }
         PARIS_LAUNCH_N(c, kname<T>("mg_coarse_cycle"), lv[Lc].N, k_coarse_cycle_smem<T>, 1, 1024, csm, S, Lc, nl,
-                       c->bnd, nu1_, nu2_, nuc, cf, (int)scratch);
+                       c->bnd, nu1_, nu2_, nuc, cf, ct, (int)scratch);
     } else {
         PARIS_LAUNCH_N(c, kname<T>("mg_coarse_cycle"), lv[Lc].N, k_fast_coarse_cycle<T>, 1, 1024, 0, S, Lc, nl,
-                       c->bnd, nu1_, nu2_, nuc, cf, 0);
+                       c->bnd, nu1_, nu2_, nuc, cf, ct, 0);
     }
     cur[Lc] = lv[Lc].x;
     for (int L = Lc - 1; L >= 0; L--) {
         const FastLevel<T>& l = lv[L];
-        const int nu2 = nu_at(L, nu2_, nuc, cf);
+        const int nu2 = nu_at(L, nu2_, nuc, cf, ct);
         if (l.x2 && nu2 > 0) {
             T* in = cur[L];
             for (int s = 0; s < nu2;) {
@@ -1327,9 +1330,10 @@ int mg_fast_solve_into(paris_ctx* c, const paris_solve_opts* o, paris_solve_resu
     // the smoother's relaxation factor: the reference's BETA of RedBlackRelax
     const double omega = o->beta > 0.0 ? o->beta : 1.0;
     // sweeps on the coarser levels (from coarse_from down) when nu_coarse > 0
-    if (o->nu_coarse < 0 || o->coarse_from < 0) return PARIS_BAD_ARGS;
+    if (o->nu_coarse < 0 || o->coarse_from < 0 || o->coarse_to < 0) return PARIS_BAD_ARGS;
     c->fast_nuc = o->nu_coarse;
     c->fast_cf = o->coarse_from > 0 ? o->coarse_from : 1;
+    c->fast_ct = o->coarse_to;
     int st;
     if (o->mode == PARIS_MG_MIXED) {
         PARIS_CHECK(fast_alloc<float>(c));

@@ -192,8 +192,8 @@ ALGO_BYTES = {
     "mg_restrict_f64": 41.0,
     "mg_prolong_f32": 8.5,        # x read+write 8 + coarse 4/8
     "mg_prolong_f64": 17.0,
-    "mg_residual_fp64(r32)": 44.0,  # 3 faces + rhs 32 + p 8 + r (FP32) 4
-    "mg_residual_fp64(r64)": 48.0,
+    "mg_residual_fp64(r32)": 52.0,  # 3 faces + rhs 32 + p 8 + r (FP32) 4 + r (FP64, the CG's) 8
+    "mg_residual_fp64(r64)": 56.0,
     "mg_correct_f32": 20.0,       # p read+write 16 + correction 4
     "mg_correct_f64": 24.0,
     "mg_coef0": 36.0,             # FP64 faces 24 -> FP32 faces 12

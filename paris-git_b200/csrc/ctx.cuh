@@ -86,6 +86,8 @@ struct paris_ctx {
     double* fast_d64 = nullptr;
     double* fast_q64 = nullptr;
     double* cg_scal = nullptr;     // device-side scalars of the CG loop (8 doubles, allocated at init)
+    double* bx_part = nullptr;     // set around a preconditioning V-cycle: where its last finest-level
+    int bx_blocks = 0;             // sweep writes the partials of r.z, and how many it wrote
     double* adj = nullptr;         // projection adjoint: 10 ghosted fields + N (allocated on first use)
     // asynchronous transfers: one stream per direction, a device staging copy
     // of each transferred field and the events that order them against `stream`

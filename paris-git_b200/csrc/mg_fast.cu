@@ -977,11 +977,15 @@ static int sweep_tma_chunk(paris_ctx* c, const FastLevel<float>& l) {
     return (int)div_up(l.n[2], nbz);
 }
 
+// bx_part: also write the per-block partials of b.x (see k_rb_sweep2_cfg);
+// *bx_blocks receives their count (0 when this form of the sweep cannot)
 template <typename T>
-static int sweep_fused(paris_ctx* c, int L, const FastLevel<T>& l, const T* xin, T* xout, const T* xc, int first) {
+static int sweep_fused(paris_ctx* c, int L, const FastLevel<T>& l, const T* xin, T* xout, const T* xc, int first,
+                       double* bx_part = nullptr, int* bx_blocks = nullptr) {
     using Cfg = typename SwGeo<T>::Cfg;
     // level 0 streams from HBM; the lower levels are resident in L2
     const char* label = L > 0 ? "mg_sweep_lower" : (xin ? "mg_sweep" : "mg_sweep_zero");
+    if (bx_blocks) *bx_blocks = 0;
     if constexpr (std::is_same<T, float>::value) {
         if (l.tma) {
             const LevelTma* t = static_cast<const LevelTma*>(l.tma);
@@ -997,8 +1001,10 @@ static int sweep_fused(paris_ctx* c, int L, const FastLevel<T>& l, const T* xin,
     }
     int zc = sweep_chunk<T>(c, l);
     dim3 grid(div_up(l.n[0], Cfg::TX), div_up(l.n[1], Cfg::TY), div_up(l.n[2], zc));
+    if (bx_part && (long)grid.x * grid.y * grid.z > kRedBlocks) bx_part = nullptr;
     PARIS_LAUNCH_N(c, kname<T>(label), l.N, k_rb_sweep2_cfg<Cfg>, grid, Cfg::NT,
-                   sweep_smem<T>(), view(l), xin, xout, xc, c->bnd, first, zc);
+                   sweep_smem<T>(), view(l), xin, xout, xc, c->bnd, first, zc, bx_part);
+    if (bx_part && bx_blocks) *bx_blocks = (int)(grid.x * grid.y * grid.z);
     return PARIS_OK;
 }
 
@@ -1118,7 +1124,12 @@ static int vcycle(paris_ctx* c, int nu1_, int nu2_, T** x0) {
                     PARIS_CHECK(sweep_pair<T>(c, L, l, in, out, xc, 1));
                     s += 2;
                 } else {
-                    PARIS_CHECK(sweep_fused<T>(c, L, l, in, out, xc, 1));
+                    // the last sweep of the cycle on the finest level also forms
+                    // the partials of r.z for the CG, when asked to
+                    const bool last = L == 0 && s + 1 == nu2 && c->bx_part;
+                    int nb = 0;
+                    PARIS_CHECK(sweep_fused<T>(c, L, l, in, out, xc, 1, last ? c->bx_part : nullptr, &nb));
+                    if (last && nb > 0) c->bx_blocks = nb;
                     s += 1;
                 }
                 in = out;
@@ -1194,9 +1205,18 @@ static int alloc_vec(paris_ctx* c, double** p) {
 // the buffer holding z; r.z goes to the device-side scalar slot rzs
 template <typename T>
 static int precondition(paris_ctx* c, int nu1, int nu2, T** z, int rzs) {
+    // r.z from the cycle's last finest-level sweep (r as the FP32 right-hand
+    // side it smooths, rT; the same FP64 r in the FP64 cycle), or a pass of its own
+    c->bx_part = c->red_part;
+    c->bx_blocks = 0;
     PARIS_CHECK(vcycle<T>(c, nu1, nu2, z));
-    PARIS_LAUNCH_N(c, kname<T>("pcg_rz"), c->N, k_pcg_rz<T>, red_grid(c, k_pcg_rz<T>, 256), 256, 0, *z, c->fast_r64,
-                   c->N, c->red_part);
+    c->bx_part = nullptr;
+    if (c->bx_blocks > 0) {
+        c->red_nb = c->bx_blocks;
+    } else {
+        PARIS_LAUNCH_N(c, kname<T>("pcg_rz"), c->N, k_pcg_rz<T>, red_grid(c, k_pcg_rz<T>, 256), 256, 0, *z,
+                       c->fast_r64, c->N, c->red_part);
+    }
     PARIS_LAUNCH(c, k_cg_reduce, 1, 256, 0, c->red_part, c->cg_scal + rzs, (double*)nullptr, c->red_nb);
     return PARIS_OK;
 }

@@ -20,6 +20,10 @@
 // arrives, fetched into registers one step ahead.  Ring-buffer slots rotate
 // with the step.
 //
+// With bx_part, the sweep also sums b x over the cells it stores (in FP64) and
+// writes one partial per block: on the last sweep of a V-cycle on the finest
+// level that is r.z, the dot product the CG needs next.
+//
 // Requirements (checked by the host): n0 a multiple of 16 / sizeof(T) and all
 // dimensions even (true of every level above the coarsest).
 #pragma once
@@ -159,7 +163,7 @@ template <class C>
 __global__ void __launch_bounds__(C::NT, C::MINB)
     k_rb_sweep2_cfg(const LV<typename C::type> v, const typename C::type* __restrict__ xin,
                     typename C::type* __restrict__ xout, const typename C::type* __restrict__ xc, const Bnd B,
-                    int first, int zc) {
+                    int first, int zc, double* __restrict__ bx_part) {
     using T = typename C::type;
     using G = Sw2<C>;
     constexpr int NT = G::NT;
@@ -303,6 +307,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
             if ((fok[q] >> off) & 1) update(fr0[q] + off, xk, xm, xp, cxk, cyk, bk, czk, czm);
         }
     };
+    double bx = 0.0;   // with bx_part: sum of b x over the cells this thread stores
     auto s_at = [&](int k, T* xk, const T* xm, const T* xp, const T* cxk, const T* cyk, const T* bk, const T* czk,
                     const T* czm) {
         if (k < z0 || k >= z1 || !s_out) return;
@@ -313,6 +318,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
         pr.x = xk[srl];
         pr.y = xk[srl + 1];
         *reinterpret_cast<V2*>(xout + sgi + (long)n0 * sgj + plane * k) = pr;
+        if (bx_part) bx += (double)bk[srl] * (double)pr.x + (double)bk[srl + 1] * (double)pr.y;
     };
 
     // prologue: group 0 = iterate z0-2..z0+1, coefficients z0-1, z0, cz z0-2;
@@ -377,4 +383,9 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
         zb = sw_add(zb, 2, G::ZS);
     }
     cp_async_wait_all_groups();
+    if (bx_part) {   // b.x of the block: one partial per block, in launch order
+        __shared__ double bsh[32];
+        bx = block_sum<G::NT>(bx, bsh);
+        if (tid == 0) bx_part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = bx;
+    }
 }

@@ -28,3 +28,22 @@ def problem(capi, orc, workloads, n, bc, seed):
         vel[2][g - 1, :, :] = 0.0
         vel[2][g + n[2] - 1, :, :] = 0.0
     return desc, cvof, vel
+
+
+def assert_same_solve(p_a, r_a, p_b, r_b, pcg, mixed):
+    """Two forms of the sweep smooth to the same bits, so a defect-correction
+    solve (pcg 0) gives the same pressure to the bit.  With the CG outer loop
+    the single fused sweep also forms r.z on its last finest-level pass (from
+    the FP32 right-hand side it smooths, in the mixed cycle) where the other
+    forms take a pass of their own, so there the CG scalars differ in their
+    last bits: the same iteration count, and pressures equal to 1e-6 (mixed)
+    or 1e-11 (FP64) of their largest value."""
+    assert r_a.it == r_b.it
+    if not pcg:
+        assert r_a.rel_res == r_b.rel_res
+        assert np.array_equal(p_a, p_b)
+        return
+    scale = float(np.abs(p_b).max())
+    tol = 1e-6 if mixed else 1e-11
+    assert abs(r_a.rel_res - r_b.rel_res) <= (1e-4 if mixed else 1e-9) * abs(r_b.rel_res)
+    assert float(np.abs(p_a - p_b).max()) <= tol * scale

@@ -2,7 +2,8 @@
 
 The two kernels share the tiles, the wavefront and the arithmetic of the
 fused red-black sweep and differ only in how the planes reach shared memory,
-so a solve with either must give the same pressure to the bit.  The
+so a defect-correction solve with either gives the same pressure to the bit
+(a CG solve the same to rounding: assert_same_solve).  The
 environment variable PARIS_SWEEP_TMA, read when a handle first builds its
 FP32 multigrid levels, selects the TMA staging (1) or the cp.async one (0,
 the default); both arms run the sweeps one at a time (PARIS_SWEEP_PAIRS=0).
@@ -14,7 +15,7 @@ import os
 import numpy as np
 import pytest
 
-from sweep_case import problem as _problem
+from sweep_case import assert_same_solve, problem as _problem
 
 pytestmark = pytest.mark.gpu
 
@@ -52,7 +53,5 @@ def test_tma_sweep_matches_cp_async(gpu_lib, capi, runtime, orc, workloads, n, b
         warnings.simplefilter("ignore")
         p_tma, r_tma = _solve(runtime, capi, desc, cvof, vel, True, pcg)
         p_cpa, r_cpa = _solve(runtime, capi, desc, cvof, vel, False, pcg)
-    assert r_tma.it == r_cpa.it
-    assert r_tma.rel_res == r_cpa.rel_res
-    assert np.array_equal(p_tma, p_cpa)
+    assert_same_solve(p_tma, r_tma, p_cpa, r_cpa, pcg, True)
 

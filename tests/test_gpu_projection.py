@@ -248,3 +248,17 @@ def test_warm_start_with_a_large_constant(gpu_lib, capi, runtime, orc, workloads
     assert abs(orc.interior(desc, pw).mean() - wi.mean()) <= 1e-6 * abs(wi.mean())
     d = orc.interior(desc, pw) - orc.interior(desc, p)
     assert np.abs(d - d.mean()).max() <= 1e-8 * np.abs(p).max()
+
+
+def test_fast_mg_rejects_negative_sweep_options(gpu_lib, capi, runtime, orc, workloads):
+    """nu_coarse, coarse_from and coarse_to must not be negative: the solver
+    refuses them with PARIS_BAD_ARGS before touching p."""
+    n = 32
+    desc, cvof, rho, vel = drop_problem(capi, orc, workloads, n, bc="periodic", ndrops=4)
+    with runtime.ParisGpu(desc) as gpu:
+        upload_state(gpu, capi, cvof, rho, vel)
+        gpu.setup_poisson(1e-3)
+        for bad in ({"nu_coarse": -1}, {"coarse_from": -1}, {"coarse_to": -1}):
+            with pytest.raises(runtime.ParisError) as e:
+                gpu.new_solver(0.0, maxit=5, mode=capi.MG_MIXED, rel_tol=1e-10, pcg=1, **bad)
+            assert e.value.status == capi.BAD_ARGS

@@ -1328,6 +1328,10 @@ static bool singular(const paris_ctx* c) {
 int mg_fast_solve_into(paris_ctx* c, const paris_solve_opts* o, paris_solve_result* res, const double* rhs,
                        double* x) {
     if (!c->have_matrix) return PARIS_BAD_ARGS;
+    if (o->nu_coarse < 0 || o->coarse_from < 0 || o->coarse_to < 0) {
+        ctx_set_error(c, "NewSolver: negative nu_coarse, coarse_from or coarse_to");
+        return PARIS_BAD_ARGS;
+    }
     // A singular system is solved from its initial guess with the mean taken
     // out, and the mean is put back afterwards.  A warm start with a large
     // constant part (the hydrostatic pressure of the previous step) otherwise
@@ -1349,8 +1353,7 @@ int mg_fast_solve_into(paris_ctx* c, const paris_solve_opts* o, paris_solve_resu
     }
     // the smoother's relaxation factor: the reference's BETA of RedBlackRelax
     const double omega = o->beta > 0.0 ? o->beta : 1.0;
-    // sweeps on the coarser levels (from coarse_from down) when nu_coarse > 0
-    if (o->nu_coarse < 0 || o->coarse_from < 0 || o->coarse_to < 0) return PARIS_BAD_ARGS;
+    // sweeps on the coarser levels (coarse_from..coarse_to) when nu_coarse > 0
     c->fast_nuc = o->nu_coarse;
     c->fast_cf = o->coarse_from > 0 ? o->coarse_from : 1;
     c->fast_ct = o->coarse_to;

@@ -939,7 +939,8 @@ static int fast_coefs(paris_ctx* c) {
 }
 
 // Planes per block of the fused sweep: enough blocks for one wave of resident
-// blocks, at least 4 planes per block.
+// blocks, at least 4 planes per block (2 where that leaves fewer blocks than
+// SMs).
 template <typename T>
 static int sweep_chunk(paris_ctx* c, const FastLevel<T>& l) {
     using Cfg = typename SwGeo<T>::Cfg;
@@ -953,6 +954,7 @@ static int sweep_chunk(paris_ctx* c, const FastLevel<T>& l) {
     long tiles = (long)div_up(l.n[0], Cfg::TX) * div_up(l.n[1], Cfg::TY);
     long nbz = (long)per_sm * c->nsm / tiles;
     long cap = l.n[2] / 4;
+    if (tiles * cap < c->nsm) cap = l.n[2] / 2;   // small levels (64^3, 32^3): two planes per block
     if (nbz > cap) nbz = cap;
     if (nbz < 1) nbz = 1;
     return (int)div_up(l.n[2], nbz);

@@ -29,6 +29,7 @@ struct FastLevel {
     T* x2;   // second iterate of the fused sweeps (they read one and write the other)
     void* tma = nullptr;   // FP32: tensor maps of the level for the TMA-staged sweep (mg_fast.cu)
     bool pairs = false;    // two consecutive sweeps run as one pass (k_rb_sweep4_cfg)
+    bool rs = false;       // the last pre-smoothing sweep forms the coarse right-hand side (k_rb_sweep_rs)
     double omega = 1.0;    // relaxation factor of the red-black smoother, set by each solve
 };
 

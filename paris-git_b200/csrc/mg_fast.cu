@@ -189,6 +189,7 @@ static inline dim3 row_grid(long n0, int n1, int n2) { return dim3(div_up(n0, 12
 #include "mg_sweep.cuh"
 #include "mg_sweep_tma.cuh"
 #include "mg_sweep4.cuh"
+#include "mg_sweep_rs.cuh"
 
 // 32-bit forms of smooth_cell / resid_cell / restrict_cell for the levels of
 // the single-block coarse cycle (at most a few thousand cells): the same
@@ -892,6 +893,19 @@ static bool pairs_wanted() {
     return e && e[0] == '1';
 }
 
+// The last pre-smoothing sweep of a fused FP32 level can also form the
+// residual and the coarse right-hand side (k_rb_sweep_rs): on the finest level
+// (PARIS_SWEEP_RS=1 in the environment when a handle first builds its levels)
+// or on every fused level (2).  It gives the same iterates to the bit, but
+// measured on a B200 at 256^3 the fused sweep took 291 us against 148 us for
+// the sweep plus 75 us for the restriction kernel (its wider rings and the
+// 32x8 tiles that fit three blocks per SM), so it is off by default.
+static int rs_levels() {
+    const char* e = getenv("PARIS_SWEEP_RS");
+    if (!e) return 0;
+    return e[0] == '1' ? 1 : (e[0] == '2' ? 2 : 0);
+}
+
 void mg_fast_free_maps(paris_ctx* c) {
     for (auto& l : c->fl32) {
         delete static_cast<LevelTma*>(l.tma);
@@ -917,6 +931,7 @@ static int fast_alloc(paris_ctx* c) {
                        l.n[2] % 2 == 0 && L < nl - 1;
         if (fusable) PARIS_CUDA_TRY(c, cudaMalloc(&l.x2, l.N * sizeof(T)));
         l.pairs = fusable && pairs_wanted();
+        l.rs = fusable && std::is_same<T, float>::value && (rs_levels() == 2 || (rs_levels() == 1 && L == 0));
         if constexpr (std::is_same<T, float>::value) level_maps(l);
     }
     return PARIS_OK;
@@ -1010,6 +1025,39 @@ static int sweep_fused(paris_ctx* c, int L, const FastLevel<T>& l, const T* xin,
     return PARIS_OK;
 }
 
+// planes per block of the fused-restriction sweep: one wave of resident
+// blocks, an even number of planes, at least 4
+static int sweep_rs_chunk(paris_ctx* c, const FastLevel<float>& l) {
+    using Cfg = SwRsCfg;
+    static int per_sm = 0;
+    if (!per_sm) {
+        cudaFuncSetAttribute(k_rb_sweep_rs<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sweep_rs_smem<Cfg>());
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rb_sweep_rs<Cfg>, Cfg::NT,
+                                                          sweep_rs_smem<Cfg>()) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
+    }
+    long tiles = (long)div_up(l.n[0], Cfg::TX) * div_up(l.n[1], Cfg::TY);
+    long nbz = (long)per_sm * c->nsm / tiles;
+    long cap = l.n[2] / 4;
+    if (nbz > cap) nbz = cap;
+    if (nbz < 1) nbz = 1;
+    int zc = (int)div_up(l.n[2], nbz);
+    return zc + (zc & 1);
+}
+
+// the last pre-smoothing sweep of level L with the restriction into the
+// right-hand side of level L+1
+static int sweep_rs(paris_ctx* c, const FastLevel<float>& l, const FastLevel<float>& lc, const float* xin,
+                    float* xout, int first) {
+    using Cfg = SwRsCfg;
+    const int zc = sweep_rs_chunk(c, l);
+    dim3 grid(div_up(l.n[0], Cfg::TX), div_up(l.n[1], Cfg::TY), div_up(l.n[2], zc));
+    PARIS_LAUNCH_N(c, "mg_sweep_restrict_f32", l.N, k_rb_sweep_rs<Cfg>, grid, Cfg::NT, sweep_rs_smem<Cfg>(), view(l),
+                   xin, xout, lc.b, c->bnd, first, zc);
+    return PARIS_OK;
+}
+
 // planes per block of the pair sweep: as sweep_chunk, at least 8 planes per
 // block (a block recomputes three planes on either side of its chunk)
 template <typename T>
@@ -1064,6 +1112,7 @@ static int vcycle(paris_ctx* c, int nu1_, int nu2_, T** x0) {
     for (int L = 0; L < Lc; L++) {
         const FastLevel<T>& l = lv[L];
         const int nu1 = nu_at(L, nu1_, nuc, cf, ct);
+        bool restricted = false;   // the last pre-smoothing sweep formed lv[L+1].b
         if (l.x2 && nu1 > 0) {
             const T* in = nullptr;
             T* out = l.x;
@@ -1071,6 +1120,10 @@ static int vcycle(paris_ctx* c, int nu1_, int nu2_, T** x0) {
                 if (l.pairs && s + 1 < nu1) {
                     PARIS_CHECK(sweep_pair<T>(c, L, l, in, out, nullptr, 0));
                     s += 2;
+                } else if (l.rs && s + 1 == nu1) {
+                    if constexpr (std::is_same<T, float>::value) PARIS_CHECK(sweep_rs(c, l, lv[L + 1], in, out, 0));
+                    restricted = true;
+                    s += 1;
                 } else {
                     PARIS_CHECK(sweep_fused<T>(c, L, l, in, out, nullptr, 0));
                     s += 1;
@@ -1089,8 +1142,9 @@ static int vcycle(paris_ctx* c, int nu1_, int nu2_, T** x0) {
             cur[L] = l.x;
         }
         LV<T> cv = view(lv[L + 1]);
-        PARIS_LAUNCH_N(c, kname<T>("mg_restrict"), l.N, k_fast_restrict2<T>, dim3(div_up(cv.n0, 32), cv.n1, cv.n2),
-                       dim3(32, 4), 0, view_x(l, cur[L]), cv, c->bnd);
+        if (!restricted)
+            PARIS_LAUNCH_N(c, kname<T>("mg_restrict"), l.N, k_fast_restrict2<T>,
+                           dim3(div_up(cv.n0, 32), cv.n1, cv.n2), dim3(32, 4), 0, view_x(l, cur[L]), cv, c->bnd);
     }
     LVSet<T> S;
     for (int L = 0; L < nl; L++) S.l[L] = view(lv[L]);

@@ -605,11 +605,18 @@ __global__ void k_fast_coarsen(const LV<T> f, const LV<T> c, T* ccx, T* ccy, T* 
 }
 
 // ---- FP64 outer loop --------------------------------------------------------
-__device__ inline double pfield(const double* __restrict__ p, const Layout& L, const Bnd& B, int i, int j, int k) {
-    if (i < 0 || i >= L.n[0]) { if (!B.per[0]) return 0.0; i = i < 0 ? i + L.n[0] : i - L.n[0]; }
-    if (j < 0 || j >= L.n[1]) { if (!B.per[1]) return 0.0; j = j < 0 ? j + L.n[1] : j - L.n[1]; }
-    if (k < 0 || k >= L.n[2]) { if (!B.per[2]) return 0.0; k = k < 0 ? k + L.n[2] : k - L.n[2]; }
-    return p[lidx(L, i, j, k)];
+// the six neighbours of interior cell (i,j,k) of a ghosted field, at offsets
+// from its index n: the periodic image across a boundary, 0 at a wall
+__device__ inline void pnbrs(const double* __restrict__ p, const Layout& L, const Bnd& B, int i, int j, int k, long n,
+                             double& xw, double& xe, double& xs, double& xn, double& xb, double& xt) {
+    const int n0 = L.n[0], n1 = L.n[1], n2 = L.n[2];
+    const long sy = L.pitch, sz = L.plane;
+    xw = i > 0 ? p[n - 1] : (B.per[0] ? p[n + n0 - 1] : 0.0);
+    xe = i < n0 - 1 ? p[n + 1] : (B.per[0] ? p[n - (n0 - 1)] : 0.0);
+    xs = j > 0 ? p[n - sy] : (B.per[1] ? p[n + sy * (n1 - 1)] : 0.0);
+    xn = j < n1 - 1 ? p[n + sy] : (B.per[1] ? p[n - sy * (n1 - 1)] : 0.0);
+    xb = k > 0 ? p[n - sz] : (B.per[2] ? p[n + sz * (n2 - 1)] : 0.0);
+    xt = k < n2 - 1 ? p[n + sz] : (B.per[2] ? p[n - sz * (n2 - 1)] : 0.0);
 }
 
 // (A x)_m with the symmetric face form: A1 = cx(i-1), A2 = cx(i), ...
@@ -652,9 +659,10 @@ __global__ void k_fast_residual64(const Mat64 A, const double* __restrict__ p, c
         long n = lidx(L, i, j, k);
         double b = A.rhs[m];
         const double pc = p[n];
-        double r = b + (a1 * (pfield(p, L, B, i - 1, j, k) - pc) + a2 * (pfield(p, L, B, i + 1, j, k) - pc) +
-                        a3 * (pfield(p, L, B, i, j - 1, k) - pc) + a4 * (pfield(p, L, B, i, j + 1, k) - pc) +
-                        a5 * (pfield(p, L, B, i, j, k - 1) - pc) + a6 * (pfield(p, L, B, i, j, k + 1) - pc));
+        double xw, xe, xs, xn, xb, xt;
+        pnbrs(p, L, B, i, j, k, n, xw, xe, xs, xn, xb, xt);
+        double r = b + (a1 * (xw - pc) + a2 * (xe - pc) + a3 * (xs - pc) + a4 * (xn - pc) + a5 * (xb - pc) +
+                        a6 * (xt - pc));
         if (rT) rT[m] = (T)r;
         if (r64) r64[m] = r;
         s2 += r * r;

@@ -39,7 +39,7 @@ sys.path.insert(0, ROOT)
 METRIC = "steps/s @256³ VOF+MG projection, mixed vs FP64 MG at 1e-10 residual"
 REL_TOL = 1e-10
 NU = [2, 2, 4, 1, 2]   # pre/post sweeps of the B200 V-cycle; sweeps from level NU[3] down (--nu1 --nu2 --nu-coarse --coarse-from --coarse-to)
-OMEGA = [1.1]   # relaxation factor of its red-black smoother (--beta)
+OMEGA = [1.1, 1.25]   # relaxation factor of its red-black smoother on the finest level and below it (--beta --beta-coarse)
 REF_BETA = 1.2  # the reference's default BETA (paris.f90:3553), for its own multigrid
 
 
@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--pcg", type=int, default=1, help="1: FP64 flexible CG preconditioned by the V-cycle, 0: defect correction")
     ap.add_argument("--beta", type=float, default=1.1,
                     help="relaxation factor of the B200 multigrid's red-black smoother (the reference's BETA)")
+    ap.add_argument("--beta-coarse", type=float, default=1.25,
+                    help="the smoother's relaxation factor on the levels below the finest (0: --beta)")
     ap.add_argument("--nu-coarse", type=int, default=4,
                     help="pre/post sweeps of the B200 V-cycle on the levels from --coarse-from down (0: --nu1/--nu2)")
     ap.add_argument("--coarse-from", type=int, default=1, help="first level (0 = finest) that takes --nu-coarse")
@@ -221,7 +223,7 @@ def gpu_step(gpu, capi, k, dt, mode, pcg):
     gpu.setup_poisson(dt)
     gpu.fill_field(capi.F_P, 0.0)
     r = gpu.new_solver(0.0, maxit=200, mode=mode, rel_tol=REL_TOL, pcg=pcg, nu1=NU[0], nu2=NU[1], beta=OMEGA[0],
-                       nu_coarse=NU[2], coarse_from=NU[3], coarse_to=NU[4])
+                       nu_coarse=NU[2], coarse_from=NU[3], coarse_to=NU[4], beta_coarse=OMEGA[1])
     gpu.project_velocity(dt)
     return r
 
@@ -264,11 +266,11 @@ def pressure_error(gpu, capi, args, dt, reset, cpu_oracle):
         gpu.setup_poisson(dt)
         gpu.fill_field(capi.F_P, 0.0)
         rm = gpu.new_solver(0.0, maxit=200, mode=capi.MG_MIXED, rel_tol=REL_TOL, pcg=args.pcg, nu1=NU[0], nu2=NU[1], beta=OMEGA[0],
-                       nu_coarse=NU[2], coarse_from=NU[3], coarse_to=NU[4])
+                       nu_coarse=NU[2], coarse_from=NU[3], coarse_to=NU[4], beta_coarse=OMEGA[1])
         pm = gpu.download(capi.F_P)
         gpu.fill_field(capi.F_P, 0.0)
         r64 = gpu.new_solver(0.0, maxit=200, mode=capi.MG_FP64, rel_tol=REL_TOL, pcg=args.pcg, nu1=NU[0], nu2=NU[1], beta=OMEGA[0],
-                       nu_coarse=NU[2], coarse_from=NU[3], coarse_to=NU[4])
+                       nu_coarse=NU[2], coarse_from=NU[3], coarse_to=NU[4], beta_coarse=OMEGA[1])
         p64 = gpu.download(capi.F_P)
         pm_i, p64_i = pm[g:-g, g:-g, g:-g], p64[g:-g, g:-g, g:-g]
         l2, mx = _rel_diff(pm_i, p64_i)
@@ -434,7 +436,7 @@ def run_b200(args, dist):
     gpu.setup_poisson(dt)
     gpu.fill_field(capi.F_P, 0.0)
     gpu.new_solver(0.0, maxit=200, mode=capi.MG_MIXED, rel_tol=REL_TOL, pcg=args.pcg, nu1=NU[0], nu2=NU[1], beta=OMEGA[0],
-                       nu_coarse=NU[2], coarse_from=NU[3], coarse_to=NU[4])
+                       nu_coarse=NU[2], coarse_from=NU[3], coarse_to=NU[4], beta_coarse=OMEGA[1])
     gpu.project_velocity(dt)
     cvof0 = gpu.download(capi.F_CVOF) if (dist.rank == 0 and not args.no_cpu_baseline) else None
     flag0 = gpu.download(capi.F_VOF_FLAG) if cvof0 is not None else None
@@ -587,7 +589,8 @@ def run_b200(args, dist):
         "solver": (f"B200 MG: FP32 red-black V({NU[0]},{NU[1]}) cycles" +
                    (f" ({NU[2]} sweeps each way on levels {NU[3]}.." + (str(NU[4]) if NU[4] else "coarsest") + ")"
                     if NU[2] else "") +
-                   (f" (over-relaxed, factor {OMEGA[0]})" if OMEGA[0] != 1.0 else "") + " in an FP64 " +
+                   (f" (over-relaxed, factor {OMEGA[0]}" + (f"; {OMEGA[1]} below the finest level" if OMEGA[1] > 0 else "")
+                    + ")" if OMEGA[0] != 1.0 or OMEGA[1] > 0 else "") + " in an FP64 " +
                    ("flexible-CG (preconditioner) loop" if args.pcg else "defect-correction loop")),
         "fp64_steps_per_s": dist.world * args.steps / (ms64 / 1e3),
         ("mixed_dc_steps_per_s" if args.pcg else "mixed_pcg_steps_per_s"): dist.world * args.steps / (msdc / 1e3),
@@ -704,7 +707,7 @@ def run_bubble(args, dist):
     k = [0]
     solve = {"max_error": 0.0, "rel_tol": BUBBLE_REL_TOL, "maxit": 200, "mode": capi.MG_MIXED, "pcg": 1,
              "beta": OMEGA[0], "nu1": NU[0], "nu2": NU[1], "nu_coarse": NU[2], "coarse_from": NU[3],
-             "coarse_to": NU[4]}
+             "coarse_to": NU[4], "beta_coarse": OMEGA[1]}
 
     def step():
         dt, _ = gpu.time_step_size(B["cfl"], B["max_dt"])     # TimeStepSize, dtFlag 2
@@ -818,7 +821,7 @@ def run_bubble(args, dist):
 def main():
     args = parse()
     NU[:] = [args.nu1, args.nu2, args.nu_coarse, args.coarse_from, args.coarse_to]
-    OMEGA[0] = args.beta
+    OMEGA[:] = [args.beta, args.beta_coarse]
     if args.n is None:
         args.n = 512 if args.workload == "rising_bubble" else 256
     dist = Dist()

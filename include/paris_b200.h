@@ -290,6 +290,9 @@ typedef struct paris_solve_opts {
                             levels from coarse_from down (nu1/nu2 above them)              */
     int32_t coarse_from; /* the first level (0 = finest) that takes nu_coarse; 0 taken as 1 */
     int32_t coarse_to;   /* the last level that takes nu_coarse (0: every level below coarse_from) */
+    int32_t reserved;    /* 0                                                              */
+    double  beta_coarse; /* FP64/MIXED: if > 0, the smoother's relaxation factor on every level
+                            below the finest (beta on the finest); <= 0: beta everywhere   */
 } paris_solve_opts;
 
 typedef struct paris_solve_result {

@@ -20,8 +20,8 @@
 #include "og.h"
 
 int og_fastmg_solve(const paris_grid_desc* desc, const double* A, double* p, double rel_tol, int maxit,
-                    int mixed, int pcg, int nu1, int nu2, double omega, int nu_coarse, int coarse_from,
-                    int coarse_to, double* hist);
+                    int mixed, int pcg, int nu1, int nu2, double omega, double omega_coarse, int nu_coarse,
+                    int coarse_from, int coarse_to, double* hist);
 
 typedef struct {
     og_grid* g;
@@ -126,7 +126,7 @@ int og_projection_forward_B(const paris_grid_desc* desc, double dt, const double
                 }
                 A[7 * N + t] = -div;
             }
-    int it = og_fastmg_solve(desc, A, x, rel_tol, maxit, 0, 1, 2, 2, 1.0, 0, 1, 0, NULL);
+    int it = og_fastmg_solve(desc, A, x, rel_tol, maxit, 0, 1, 2, 2, 1.0, 0.0, 0, 1, 0, NULL);
     interior_to_ghosted(g, x, p);
     for (int d = 0; d < 3; d++) memcpy(O[d], U[d], g->ntot * sizeof(double));
     for (int k = 0; k < g->nz; k++)
@@ -182,7 +182,7 @@ int og_projection_adjoint(const paris_grid_desc* desc, double dt, const double* 
                 }
                 A[7 * N + t] = s;
             }
-    int it = og_fastmg_solve(desc, A, x, rel_tol, maxit, 0, 1, 2, 2, 1.0, 0, 1, 0, NULL);
+    int it = og_fastmg_solve(desc, A, x, rel_tol, maxit, 0, 1, 2, 2, 1.0, 0.0, 0, 1, 0, NULL);
     interior_to_ghosted(g, x, lam);
     for (int d = 0; d < 3; d++) {
         memset(S[d], 0, g->ntot * sizeof(double));

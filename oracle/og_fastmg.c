@@ -11,7 +11,8 @@
  *   - red-black Gauss-Seidel V(nu1,nu2) cycles, black-red after the
  *     coarse correction (symmetric cycle), coarsest level smoothed; with a
  *     relaxation factor w != 1 each update is x + w (x_GS - x) (the
- *     reference's BETA of RedBlackRelax, newsolver.f90:229); optionally
+ *     reference's BETA of RedBlackRelax, newsolver.f90:229), optionally
+ *     another factor on the levels below the finest; optionally
  *     nu_coarse sweeps each way on the levels coarse_from..coarse_to;
  *   - an FP64 outer loop: defect correction p += V(b - A p), or
  *     preconditioned CG with the V-cycle as preconditioner, with A applied
@@ -35,6 +36,7 @@ typedef struct {
     float *fx, *fy, *fz;    /* FP32 copies */
     double *b, *x, *r;      /* FP64 work */
     float *bf, *xf, *rf;    /* FP32 work */
+    double omega;           /* relaxation factor of the red-black smoother (1: Gauss-Seidel) */
 } fm_level;
 
 typedef struct {
@@ -44,7 +46,6 @@ typedef struct {
     int mixed;
     int nu1, nu2;
     int coarse_sweeps;
-    double omega;   /* relaxation factor of the red-black smoother (1: Gauss-Seidel) */
     int nu_coarse, coarse_from, coarse_to;   /* sweeps on the levels coarse_from..coarse_to, when nu_coarse > 0 */
 } fm_mg;
 
@@ -96,7 +97,7 @@ static void smooth_##SUF(const fm_mg* mg, fm_level* l, const T* b, T* x, int col
                 T d = a1 + a2 + a3 + a4 + a5 + a6;                                           \
                 T s = a1 * pw + a2 * pe + a3 * ps + a4 * pn + a5 * pb + a6 * pt + b[q];       \
                 if (d > (T)0) {                                                              \
-                    const T g = s / d, w = (T)mg->omega;                                     \
+                    const T g = s / d, w = (T)l->omega;                                      \
                     x[q] = w == (T)1 ? g : x[q] + w * (g - x[q]);                            \
                 }                                                                            \
             }                                                                                \
@@ -220,13 +221,12 @@ static double dot(const double* a, const double* b, long n) {
 /* A from SetupPoisson: fine face coefficient east = A2, north = A4, top = A6.
  * p, b: interior arrays (nx*ny*nz).  Returns cycles run; hist[it] = ||r||/||b||. */
 int og_fastmg_solve(const paris_grid_desc* desc, const double* A, double* p, double rel_tol,
-                    int maxit, int mixed, int pcg, int nu1, int nu2, double omega, int nu_coarse,
-                    int coarse_from, int coarse_to, double* hist) {
+                    int maxit, int mixed, int pcg, int nu1, int nu2, double omega, double omega_coarse,
+                    int nu_coarse, int coarse_from, int coarse_to, double* hist) {
     fm_mg mg;
     memset(&mg, 0, sizeof(mg));
     for (int a = 0; a < 3; a++) mg.per[a] = desc->bdry_cond[a] == PARIS_BC_PERIODIC;
     mg.mixed = mixed; mg.nu1 = nu1; mg.nu2 = nu2; mg.coarse_sweeps = 8;
-    mg.omega = omega > 0.0 ? omega : 1.0;
     mg.nu_coarse = nu_coarse > 0 ? nu_coarse : 0;
     mg.coarse_from = coarse_from > 0 ? coarse_from : 1;
     mg.coarse_to = coarse_to > 0 ? coarse_to : 0;
@@ -244,6 +244,8 @@ int og_fastmg_solve(const paris_grid_desc* desc, const double* A, double* p, dou
         fm_level* l = &mg.L[L];
         for (int a = 0; a < 3; a++) l->n[a] = n0[a] >> L;
         l->N = (long)l->n[0] * l->n[1] * l->n[2];
+        l->omega = omega > 0.0 ? omega : 1.0;
+        if (L > 0 && omega_coarse > 0.0) l->omega = omega_coarse;
         l->cx = calloc(l->N, 8); l->cy = calloc(l->N, 8); l->cz = calloc(l->N, 8);
         l->fx = calloc(l->N, 4); l->fy = calloc(l->N, 4); l->fz = calloc(l->N, 4);
         l->b = calloc(l->N, 8); l->x = calloc(l->N, 8); l->r = calloc(l->N, 8);

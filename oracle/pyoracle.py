@@ -58,7 +58,7 @@ def lib():
             "og_setvofbc_host": (I, [G, P, P]),
             "og_linfunc": (I, [G, P, P, D, D, I]),
             "og_init_spheres": (I, [G, I, P, P, P, P, I, I, P, P, P]),
-            "og_fastmg_solve": (I, [G, P, P, D, I, I, I, I, I, D, I, I, I, P]),
+            "og_fastmg_solve": (I, [G, P, P, D, I, I, I, I, I, D, D, I, I, I, P]),
             "og_get_all_heights": (I, [G, P, P, P]),
             "og_get_all_curvatures": (I, [G, P, P, P, P, P, P]),
             "og_surface_force": (I, [G, P, P, P, P, P, P]),
@@ -274,16 +274,17 @@ def grid_coords(desc):
 
 
 def fastmg_solve(desc, A, p_int, rel_tol, maxit=100, mixed=True, pcg=False, nu1=2, nu2=2, omega=1.0,
-                 nu_coarse=0, coarse_from=0, coarse_to=0):
+                 nu_coarse=0, coarse_from=0, coarse_to=0, omega_coarse=0.0):
     """The B200 solver's own MG restated on the CPU; p_int: interior (nz,ny,nx);
-    omega: relaxation factor of the red-black smoother; nu_coarse sweeps each
-    way on the levels coarse_from (0: 1) .. coarse_to (0: the coarsest) when
+    omega: relaxation factor of the red-black smoother (omega_coarse > 0: the
+    factor on the levels below the finest); nu_coarse sweeps each way on the
+    levels coarse_from (0: 1) .. coarse_to (0: the coarsest) when
     nu_coarse > 0."""
     hist = np.zeros(maxit)
     p = np.ascontiguousarray(p_int, dtype=np.float64)
     it = lib().og_fastmg_solve(ctypes.byref(desc), _p(np.ascontiguousarray(A)), _p(p), rel_tol, maxit,
-                               1 if mixed else 0, 1 if pcg else 0, nu1, nu2, float(omega), int(nu_coarse),
-                               int(coarse_from), int(coarse_to), _p(hist))
+                               1 if mixed else 0, 1 if pcg else 0, nu1, nu2, float(omega), float(omega_coarse),
+                               int(nu_coarse), int(coarse_from), int(coarse_to), _p(hist))
     return p, it, hist[:it]
 
 

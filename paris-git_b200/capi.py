@@ -68,6 +68,8 @@ class SolveOpts(ctypes.Structure):
         ("nu1", ctypes.c_int32), ("nu2", ctypes.c_int32),
         ("pcg", ctypes.c_int32),
         ("nu_coarse", ctypes.c_int32), ("coarse_from", ctypes.c_int32), ("coarse_to", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("beta_coarse", ctypes.c_double),
     ]
 
 

@@ -1416,7 +1416,9 @@ int mg_fast_solve_into(paris_ctx* c, const paris_solve_opts* o, paris_solve_resu
             shift = 0.0;
     }
     // the smoother's relaxation factor: the reference's BETA of RedBlackRelax
+    // on the finest level, beta_coarse (when given) below it
     const double omega = o->beta > 0.0 ? o->beta : 1.0;
+    const double omega_c = o->beta_coarse > 0.0 ? o->beta_coarse : omega;
     // sweeps on the coarser levels (coarse_from..coarse_to) when nu_coarse > 0
     c->fast_nuc = o->nu_coarse;
     c->fast_cf = o->coarse_from > 0 ? o->coarse_from : 1;
@@ -1425,12 +1427,12 @@ int mg_fast_solve_into(paris_ctx* c, const paris_solve_opts* o, paris_solve_resu
     if (o->mode == PARIS_MG_MIXED) {
         PARIS_CHECK(fast_alloc<float>(c));
         PARIS_CHECK(fast_coefs<float>(c));
-        for (auto& l : c->fl32) l.omega = omega;
+        for (size_t L = 0; L < c->fl32.size(); L++) c->fl32[L].omega = L == 0 ? omega : omega_c;
         st = o->pcg ? solve_pcg<float>(c, o, res, rhs, x) : solve_dc<float>(c, o, res, rhs, x);
     } else {
         PARIS_CHECK(fast_alloc<double>(c));
         PARIS_CHECK(fast_coefs<double>(c));
-        for (auto& l : c->fl64) l.omega = omega;
+        for (size_t L = 0; L < c->fl64.size(); L++) c->fl64[L].omega = L == 0 ? omega : omega_c;
         st = o->pcg ? solve_pcg<double>(c, o, res, rhs, x) : solve_dc<double>(c, o, res, rhs, x);
     }
     if (c->err_host && *c->err_host) {   // the kernels before the last reduction have completed

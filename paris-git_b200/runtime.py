@@ -198,12 +198,13 @@ class ParisGpu:
         self._check(self.lib.paris_setup_test_mg(self.h), "Setup_testMG")
 
     def new_solver(self, max_error, beta=1.0, maxit=100, norm=2, mode=capi.MG_MIXED, rel_tol=0.0,
-                   nu1=2, nu2=2, pcg=0, nu_coarse=0, coarse_from=0, coarse_to=0):
+                   nu1=2, nu2=2, pcg=0, nu_coarse=0, coarse_from=0, coarse_to=0, beta_coarse=0.0):
         """NewSolver(A,p,maxError,beta,maxit,it,ierr,norm); returns the SolveResult."""
         o = capi.SolveOpts()
         o.max_error, o.rel_tol, o.beta = float(max_error), float(rel_tol), float(beta)
         o.maxit, o.norm, o.mode, o.nu1, o.nu2, o.pcg = int(maxit), int(norm), int(mode), nu1, nu2, int(pcg)
         o.nu_coarse, o.coarse_from, o.coarse_to = int(nu_coarse), int(coarse_from), int(coarse_to)
+        o.beta_coarse = float(beta_coarse)
         r = capi.SolveResult()
         st = self.lib.paris_new_solver(self.h, ctypes.byref(o), ctypes.byref(r))
         if st == capi.NOT_CONVERGED:

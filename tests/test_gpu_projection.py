@@ -184,38 +184,41 @@ def test_project_velocity_bitwise(gpu_lib, capi, runtime, orc, workloads, bc):
         assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("beta,nuc,cf,ct", [(1.0, 0, 0, 0), (1.1, 0, 0, 0), (1.1, 4, 1, 0), (1.1, 3, 2, 0),
-                                             (1.1, 4, 1, 2)])
+@pytest.mark.parametrize("beta,bcoarse,nuc,cf,ct", [(1.0, 0.0, 0, 0, 0), (1.1, 0.0, 0, 0, 0), (1.1, 0.0, 4, 1, 0),
+                                                     (1.1, 0.0, 3, 2, 0), (1.1, 0.0, 4, 1, 2), (1.1, 1.25, 4, 1, 2)])
 @pytest.mark.parametrize("bc,n", [("periodic", 64), ("wall", 64), ("periodic", 128)])
-def test_fast_mg_fused_levels_follow_oracle(gpu_lib, capi, runtime, orc, workloads, bc, n, beta, nuc, cf, ct):
+def test_fast_mg_fused_levels_follow_oracle(gpu_lib, capi, runtime, orc, workloads, bc, n, beta, bcoarse, nuc, cf,
+                                            ct):
     """From 32^3 up the finest levels run the fused red-black sweep; the FP64
     V-cycle must follow the oracle's FP64 cycle: the same number of PCG
     iterations to 1e-10 and the same final residual to rounding; the mixed
     cycle the oracle's FP32 cycle within one iteration.  beta is the
-    smoother's relaxation factor (1: Gauss-Seidel, 1.1: over-relaxed); nuc
-    sweeps each way on the levels cf..ct (ct 0: down to the coarsest; nuc 0:
-    two, as on the finest)."""
+    smoother's relaxation factor (1: Gauss-Seidel, 1.1: over-relaxed), bcoarse
+    (when > 0) its factor on the levels below the finest; nuc sweeps each way
+    on the levels cf..ct (ct 0: down to the coarsest; nuc 0: two, as on the
+    finest)."""
     desc, cvof, rho, vel = drop_problem(capi, orc, workloads, n, bc=bc, ndrops=12)
     dt = 1e-3
     st, A = orc.setup_poisson(desc, *vel, rho, dt)
     p_ref, it_ref, hist = orc.fastmg_solve(desc, A, np.zeros((n, n, n)), 1e-10, maxit=60, mixed=False, pcg=True,
-                                           omega=beta, nu_coarse=nuc, coarse_from=cf, coarse_to=ct)
+                                           omega=beta, nu_coarse=nuc, coarse_from=cf, coarse_to=ct,
+                                           omega_coarse=bcoarse)
     with runtime.ParisGpu(desc) as gpu:
         upload_state(gpu, capi, cvof, rho, vel)
         gpu.setup_poisson(dt)
         r = gpu.new_solver(0.0, beta=beta, maxit=60, mode=capi.MG_FP64, rel_tol=1e-10, pcg=1, nu_coarse=nuc,
-                           coarse_from=cf, coarse_to=ct)
+                           coarse_from=cf, coarse_to=ct, beta_coarse=bcoarse)
         p = orc.interior(desc, gpu.download(capi.F_P))
         gpu.fill_field(capi.F_P, 0.0)
         rm = gpu.new_solver(0.0, beta=beta, maxit=60, mode=capi.MG_MIXED, rel_tol=1e-10, pcg=1, nu_coarse=nuc,
-                            coarse_from=cf, coarse_to=ct)
+                            coarse_from=cf, coarse_to=ct, beta_coarse=bcoarse)
     assert r.it == it_ref
     assert abs(r.rel_res - hist[-1]) <= 1e-6 * hist[-1]
     d = (p - p.mean()) - (p_ref - p_ref.mean())
     assert np.abs(d).max() <= 1e-9 * np.abs(p_ref - p_ref.mean()).max()
     assert rm.rel_res < 1e-10 and rm.it <= it_ref + 2
     _, itm_ref, _ = orc.fastmg_solve(desc, A, np.zeros((n, n, n)), 1e-10, maxit=60, mixed=True, pcg=True,
-                                     omega=beta, nu_coarse=nuc, coarse_from=cf, coarse_to=ct)
+                                     omega=beta, nu_coarse=nuc, coarse_from=cf, coarse_to=ct, omega_coarse=bcoarse)
     assert abs(rm.it - itm_ref) <= 1
 
 

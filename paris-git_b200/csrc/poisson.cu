@@ -35,11 +35,32 @@ struct Metric {
 // coefficients A2, A4, A6 and the right-hand side A8 of every cell, plus the
 // checks of check_and_debug_Poisson / check_poisson_setup.
 // part slots: 0 = sum A8, 1 = number of cells failing a check
+// x / d of the divergence, or x * rd where every d of the axis is the same
+// power of two: 1/d is then exact and the product is the same double
+template <bool R>
+__device__ inline double div_metric(double x, double d, double rd) {
+    return R ? x * rd : x / d;
+}
+
+// num / den is a number >= 0 (no NaN; -0 counts as 0) whenever den is
+// nonzero, num is zero or of den's sign, and not both are infinite
+__device__ inline bool quot_nonneg(double num, double den) {
+    if (isinf(num) && isinf(den)) return false;
+    return (num >= 0.0 && den > 0.0) || (num <= 0.0 && den < 0.0);
+}
+
+// A1, A3, A5 (the west, south and bottom faces) are stored by the
+// neighbours as their A2, A4, A6; here they only enter the check of the cell.
+// When all six coefficients are numbers >= 0, A7 = A1 + .. + A6 is at least
+// the largest of them (each rounded partial sum of non-negative terms is at
+// least its last term), so A2, A4 and A6 decide the check whenever one of
+// them is >= 1e-50, and the three quotients are formed only otherwise.
+template <bool R>
 __global__ void __launch_bounds__(256, 3) k_setup_poisson(const double* __restrict__ u, const double* __restrict__ v,
                                 const double* __restrict__ w, const double* __restrict__ rho,
                                 double* __restrict__ cx, double* __restrict__ cy, double* __restrict__ cz,
                                 double* __restrict__ rhs, const Layout L, const Bnd B, const Metric M,
-                                double dt, double volsrc, double* part) {
+                                double rdx, double rdy, double rdz, double dt, double volsrc, double* part) {
     __shared__ double sh[32];
     double s_rhs = 0.0, s_bad = 0.0;
     const int g = L.ng;
@@ -47,18 +68,28 @@ __global__ void __launch_bounds__(256, 3) k_setup_poisson(const double* __restri
         long t = cidx(L.n[0], L.n[1], i, j, k);
         long n = lidx(L, i, j, k);
         double r0 = rho[n];
-        double a1 = 2.0 * dt * face_mask(B, L, 0, i - 1) / (M.dx[i + g] * M.dxh[i - 1 + g] * (rho[n - 1] + r0));
-        double a2 = 2.0 * dt * face_mask(B, L, 0, i) / (M.dx[i + g] * M.dxh[i + g] * (rho[n + 1] + r0));
-        double a3 = 2.0 * dt * face_mask(B, L, 1, j - 1) / (M.dy[j + g] * M.dyh[j - 1 + g] * (rho[n - L.pitch] + r0));
-        double a4 = 2.0 * dt * face_mask(B, L, 1, j) / (M.dy[j + g] * M.dyh[j + g] * (rho[n + L.pitch] + r0));
-        double a5 = 2.0 * dt * face_mask(B, L, 2, k - 1) / (M.dz[k + g] * M.dzh[k - 1 + g] * (rho[n - L.plane] + r0));
-        double a6 = 2.0 * dt * face_mask(B, L, 2, k) / (M.dz[k + g] * M.dzh[k + g] * (rho[n + L.plane] + r0));
-        double a7 = a1 + a2 + a3 + a4 + a5 + a6;
-        double a8 = -(volsrc + (u[n] - u[n - 1]) / M.dx[i + g] + (v[n] - v[n - L.pitch]) / M.dy[j + g] +
-                      (w[n] - w[n - L.plane]) / M.dz[k + g]);
+        const double n1 = 2.0 * dt * face_mask(B, L, 0, i - 1), d1 = M.dx[i + g] * M.dxh[i - 1 + g] * (rho[n - 1] + r0);
+        const double n2 = 2.0 * dt * face_mask(B, L, 0, i), d2 = M.dx[i + g] * M.dxh[i + g] * (rho[n + 1] + r0);
+        const double n3 = 2.0 * dt * face_mask(B, L, 1, j - 1),
+                     d3 = M.dy[j + g] * M.dyh[j - 1 + g] * (rho[n - L.pitch] + r0);
+        const double n4 = 2.0 * dt * face_mask(B, L, 1, j), d4 = M.dy[j + g] * M.dyh[j + g] * (rho[n + L.pitch] + r0);
+        const double n5 = 2.0 * dt * face_mask(B, L, 2, k - 1),
+                     d5 = M.dz[k + g] * M.dzh[k - 1 + g] * (rho[n - L.plane] + r0);
+        const double n6 = 2.0 * dt * face_mask(B, L, 2, k), d6 = M.dz[k + g] * M.dzh[k + g] * (rho[n + L.plane] + r0);
+        const double a2 = n2 / d2, a4 = n4 / d4, a6 = n6 / d6;
+        double a8 = -(volsrc + div_metric<R>(u[n] - u[n - 1], M.dx[i + g], rdx) +
+                      div_metric<R>(v[n] - v[n - L.pitch], M.dy[j + g], rdy) +
+                      div_metric<R>(w[n] - w[n - L.plane], M.dz[k + g], rdz));
         cx[t] = a2; cy[t] = a4; cz[t] = a6; rhs[t] = a8;
-        bool bad = a1 != a1 || a2 != a2 || a3 != a3 || a4 != a4 || a5 != a5 || a6 != a6 || a7 != a7 || a8 != a8;
-        if (a7 < 1e-50) bad = true;   // no solid cells on this grid: A7 tiny is an error
+        bool bad = a8 != a8;
+        const bool decided = quot_nonneg(n1, d1) && quot_nonneg(n3, d3) && quot_nonneg(n5, d5) && a2 >= 0.0 &&
+                             a4 >= 0.0 && a6 >= 0.0 && fmax(a2, fmax(a4, a6)) >= 1e-50;
+        if (!decided) {
+            const double a1 = n1 / d1, a3 = n3 / d3, a5 = n5 / d5;
+            const double a7 = a1 + a2 + a3 + a4 + a5 + a6;
+            bad = bad || a1 != a1 || a2 != a2 || a3 != a3 || a4 != a4 || a5 != a5 || a6 != a6 || a7 != a7;
+            if (a7 < 1e-50) bad = true;   // no solid cells on this grid: A7 tiny is an error
+        }
         s_rhs += a8;
         s_bad += bad ? 1.0 : 0.0;
     ROWS_END
@@ -101,6 +132,19 @@ __global__ void k_full_A(const double* __restrict__ rho, const double* __restric
 
 static Metric metric(const paris_ctx* c) { return Metric{c->dx, c->dxh, c->dy, c->dyh, c->dz, c->dzh}; }
 
+// every interior spacing d[g..g+n) of an axis (host copy, the doubles the
+// device holds) is the same power of two: *r = its exact reciprocal
+static bool uniform_pow2(const std::vector<double>& d, int n, int g, double* r) {
+    if ((int)d.size() < n + g) return false;
+    for (int i = g; i < n + g; i++)
+        if (d[i] != d[g]) return false;
+    int e;
+    const double m = std::frexp(d[g], &e);
+    if (m != 0.5) return false;
+    *r = 1.0 / d[g];
+    return true;
+}
+
 int poisson_build_full_A(paris_ctx* c) {
     if (c->A_from_upload) { c->A_valid = 1; return PARIS_OK; }
     if (!c->A) PARIS_CUDA_TRY(c, cudaMalloc(&c->A, 8 * c->N * sizeof(double)));
@@ -116,9 +160,18 @@ extern "C" int paris_setup_poisson(paris_handle_t c, double dt, double volume_so
     if (!(dt > 0.0)) return PARIS_BAD_ARGS;
     cudaSetDevice(c->dev);
     PARIS_CHECK(ctx_ensure_matrix(c));
-    PARIS_LAUNCH_N(c, "setup_poisson", c->N, k_setup_poisson, red_grid(c, k_setup_poisson, 256), kRowBlock, 0, c->fld[PARIS_FIELD_U], c->fld[PARIS_FIELD_V],
-                 c->fld[PARIS_FIELD_W], c->fld[PARIS_FIELD_RHO], c->cx, c->cy, c->cz, c->rhs, c->L, c->bnd,
-                 metric(c), dt, volume_source, c->red_part);
+    double rd[3];
+    if (uniform_pow2(c->h_dx, c->d.nx, c->L.ng, &rd[0]) && uniform_pow2(c->h_dy, c->d.ny, c->L.ng, &rd[1]) &&
+        uniform_pow2(c->h_dz, c->d.nz, c->L.ng, &rd[2]))
+        PARIS_LAUNCH_N(c, "setup_poisson", c->N, k_setup_poisson<true>, red_grid(c, k_setup_poisson<true>, 256),
+                       kRowBlock, 0, c->fld[PARIS_FIELD_U], c->fld[PARIS_FIELD_V], c->fld[PARIS_FIELD_W],
+                       c->fld[PARIS_FIELD_RHO], c->cx, c->cy, c->cz, c->rhs, c->L, c->bnd, metric(c), rd[0], rd[1],
+                       rd[2], dt, volume_source, c->red_part);
+    else
+        PARIS_LAUNCH_N(c, "setup_poisson", c->N, k_setup_poisson<false>, red_grid(c, k_setup_poisson<false>, 256),
+                       kRowBlock, 0, c->fld[PARIS_FIELD_U], c->fld[PARIS_FIELD_V], c->fld[PARIS_FIELD_W],
+                       c->fld[PARIS_FIELD_RHO], c->cx, c->cy, c->cz, c->rhs, c->L, c->bnd, metric(c), 0.0, 0.0, 0.0,
+                       dt, volume_source, c->red_part);
     double out[2];
     PARIS_CHECK(ctx_reduce_finish(c, 2, out));
     c->have_matrix = 1;

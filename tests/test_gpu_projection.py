@@ -44,9 +44,13 @@ def upload_state(gpu, capi, cvof, rho, vel, p=None):
     gpu.upload(capi.F_P, p if p is not None else np.zeros_like(cvof))
 
 
+@pytest.mark.parametrize("n", [16, 24])
 @pytest.mark.parametrize("bc", ["periodic", "wall"])
-def test_setup_poisson_bitwise(gpu_lib, capi, runtime, orc, workloads, bc):
-    desc, cvof, rho, vel = drop_problem(capi, orc, workloads, 16, bc=bc)
+def test_setup_poisson_bitwise(gpu_lib, capi, runtime, orc, workloads, bc, n):
+    """A (all eight components, as the reference stores them) equals the
+    oracle's bit for bit: at 16^3 the spacing is a power of two and the
+    divergence multiplies by its exact reciprocal, at 24^3 it divides."""
+    desc, cvof, rho, vel = drop_problem(capi, orc, workloads, n, bc=bc)
     dt = 1e-3
     st, A_ref = orc.setup_poisson(desc, *vel, rho, dt)
     assert st == 0
@@ -55,6 +59,33 @@ def test_setup_poisson_bitwise(gpu_lib, capi, runtime, orc, workloads, bc):
         gpu.setup_poisson(dt)
         A = gpu.download(capi.F_A)
     assert np.array_equal(A, A_ref)
+
+
+@pytest.mark.parametrize("n", [16, 24])
+@pytest.mark.parametrize("case", ["nan_rho", "nan_u", "heavy", "negative_rho"])
+def test_setup_poisson_checks(gpu_lib, capi, runtime, orc, workloads, case, n):
+    """SetupPoisson refuses what the reference's checks refuse: a NaN in A,
+    or A7 below 1e-50 outside a solid (a density of 1e60 everywhere, or a
+    negative density that makes the coefficients of a cell negative)."""
+    desc, cvof, rho, vel = drop_problem(capi, orc, workloads, n, bc="wall")
+    g = desc.ng
+    c = (g + n // 2, g + n // 3, g + n // 4)
+    if case == "nan_rho":
+        rho[c] = np.nan
+    elif case == "nan_u":
+        vel[0][c] = np.nan
+    elif case == "heavy":
+        rho[...] = 1e60
+    else:
+        rho[c] = -3.0 * np.abs(rho).max()
+    dt = 1e-3
+    st, _ = orc.setup_poisson(desc, *vel, rho, dt)
+    assert st == capi.SETUP_ERROR
+    with runtime.ParisGpu(desc) as gpu:
+        upload_state(gpu, capi, cvof, rho, vel)
+        with pytest.raises(runtime.ParisError) as e:
+            gpu.setup_poisson(dt)
+        assert e.value.status == capi.SETUP_ERROR
 
 
 def test_linfunc_bitwise(gpu_lib, capi, runtime, orc, workloads):

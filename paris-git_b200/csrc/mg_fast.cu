@@ -594,7 +594,9 @@ template <typename T>
 __global__ void k_fast_coarsen(const LV<T> f, const LV<T> c, T* ccx, T* ccy, T* ccz) {
     long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (t >= c.N) return;
-    int i = (int)(t % c.n0), j = (int)((t / c.n0) % c.n1), k = (int)(t / ((long)c.n0 * c.n1));
+    // a coarse level holds fewer than 2^32 cells: 32-bit index arithmetic
+    const unsigned tt = (unsigned)t, r = tt / (unsigned)c.n0;
+    const int i = (int)(tt - r * (unsigned)c.n0), k = (int)(r / (unsigned)c.n1), j = (int)(r - (unsigned)k * c.n1);
     int I = 2 * i, J = 2 * j, K = 2 * k;
     ccx[t] = (T)0.0625 * (f.cx[cidx(f.n0, f.n1, I + 1, J, K)] + f.cx[cidx(f.n0, f.n1, I + 1, J + 1, K)] +
                           f.cx[cidx(f.n0, f.n1, I + 1, J, K + 1)] + f.cx[cidx(f.n0, f.n1, I + 1, J + 1, K + 1)]);

@@ -65,22 +65,35 @@ __device__ inline void flux_cell_of(const SweepArgs& a, unsigned t, int& i, int&
 
 // 1. the mixed flux cells, kVofSeg per block; each thread loads its kVofPer
 // cells (strided by the block size, so the loads coalesce) before testing
-// them, and the block appends its mixed cells with one atomic add
+// them, and the block appends its mixed cells with one atomic add.  A
+// thread divides only for its first cell and steps the others on by the
+// block size; the per-(cell slot, warp) counts are scanned by one warp.
+static_assert(kVofPer * (kVofListThreads / 32) == 32, "one count per lane of the scanning warp");
 __global__ void __launch_bounds__(kVofListThreads) k_vof_mixed_list(const SweepArgs a, unsigned F) {
-    __shared__ int wcount[kVofPer][kVofListThreads / 32];
-    __shared__ int room;
+    __shared__ int wcount[kVofPer * (kVofListThreads / 32)];
+    __shared__ int wbase[kVofPer * (kVofListThreads / 32)];
+    __shared__ int total, room;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int e0 = a.L.n[0] + (a.d == 0 ? 2 : 0), e1 = a.L.n[1] + (a.d == 1 ? 2 : 0);
+    const unsigned t0 = blockIdx.x * (unsigned)kVofSeg + threadIdx.x;
+    int i, j, k;
+    flux_cell_of(a, t0 < F ? t0 : 0u, i, j, k);
+    // flux_cell_of shifts the sweep direction's index by -1; step in the
+    // unshifted (i, j, k) of the enumeration
+    int ii = i + (a.d == 0), jj = j + (a.d == 1), kk = k + (a.d == 2);
     long n[kVofPer];
     double cc[kVofPer];
 #pragma unroll
     for (int q = 0; q < kVofPer; q++) {
-        const unsigned t = blockIdx.x * (unsigned)kVofSeg + q * kVofListThreads + threadIdx.x;
-        n[q] = -1;
-        if (t < F) {
-            int i, j, k;
-            flux_cell_of(a, t, i, j, k);
-            n[q] = lidx(a.L, i, j, k);
+        const unsigned t = t0 + q * kVofListThreads;
+        if (q > 0) {
+            ii += kVofListThreads;
+            while (ii >= e0) {
+                ii -= e0;
+                if (++jj >= e1) { jj = 0; kk++; }
+            }
         }
+        n[q] = t < F ? lidx(a.L, ii - (a.d == 0), jj - (a.d == 1), kk - (a.d == 2)) : -1;
     }
 #pragma unroll
     for (int q = 0; q < kVofPer; q++) cc[q] = n[q] >= 0 ? a.c[n[q]] : 0.0;
@@ -88,24 +101,31 @@ __global__ void __launch_bounds__(kVofListThreads) k_vof_mixed_list(const SweepA
 #pragma unroll
     for (int q = 0; q < kVofPer; q++) {
         m[q] = __ballot_sync(0xffffffffu, cc[q] > 0.0 && cc[q] != 1.0);
-        if (lane == 0) wcount[q][w] = __popc(m[q]);
+        if (lane == 0) wcount[q * (kVofListThreads / 32) + w] = __popc(m[q]);
     }
     __syncthreads();
-    // the block's mixed cells in the order (q, warp, lane)
-    int base[kVofPer], total = 0;
+    // the block's mixed cells in the order (q, warp, lane): exclusive scan of
+    // the 32 counts in that order
+    if (w == 0) {
+        const int c = wcount[lane];
+        int s = c;
 #pragma unroll
-    for (int q = 0; q < kVofPer; q++)
-        for (int v = 0; v < kVofListThreads / 32; v++) {
-            if (v == w) base[q] = total;
-            total += wcount[q][v];
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += v;
         }
-    if (total == 0) return;
-    if (threadIdx.x == 0) room = atomicAdd(a.count, total);
+        wbase[lane] = s - c;
+        if (lane == 31) {
+            total = s;
+            if (s > 0) room = atomicAdd(a.count, s);
+        }
+    }
     __syncthreads();
+    if (total == 0) return;
 #pragma unroll
     for (int q = 0; q < kVofPer; q++)
         if ((m[q] >> lane) & 1u) {
-            const long e = (long)room + base[q] + __popc(m[q] & ((1u << lane) - 1u));
+            const long e = (long)room + wbase[q * (kVofListThreads / 32) + w] + __popc(m[q] & ((1u << lane) - 1u));
             if (e < a.cap) a.list[e] = n[q];
         }
 }
@@ -356,14 +376,26 @@ extern "C" int paris_vof_sweeps(paris_handle_t c, int32_t tswap, double dt) {
 // do_all_ghost.  b1..b4 of initialize_linfunc (vofmodules.f90:133-147).
 __global__ void k_linfunc(const double* __restrict__ c, double* __restrict__ f, const Layout L, double a1,
                           double a2, int harm, int filt) {
-    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    const int g = L.ng, tx = L.n[0] + 2 * g, ty = L.n[1] + 2 * g, tz = L.n[2] + 2 * g;
-    if (t >= (long)tx * ty * tz) return;
-    int ii = (int)(t % tx), jj = (int)((t / tx) % ty), kk = (int)(t / ((long)tx * ty));
-    int i = ii - g, j = jj - g, k = kk - g;
-    long n = lidx(L, i, j, k);
+    // the whole ghosted array: the flat index is the cell's index itself; its
+    // (ii, jj, kk) are needed only by the filter
+    const long n = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (n >= L.total) return;
+    bool inner = false;
+    if (filt) {
+        const int g = L.ng, tx = L.n[0] + 2 * g, ty = L.n[1] + 2 * g, tz = L.n[2] + 2 * g;
+        int ii, jj, kk;
+        if (L.total <= 0xffffffffL) {
+            const unsigned t = (unsigned)n, r = t / (unsigned)tx;
+            ii = (int)(t - r * (unsigned)tx);
+            kk = (int)(r / (unsigned)ty);
+            jj = (int)(r - (unsigned)kk * (unsigned)ty);
+        } else {
+            ii = (int)(n % tx); jj = (int)((n / tx) % ty); kk = (int)(n / ((long)tx * ty));
+        }
+        inner = ii > 0 && ii < tx - 1 && jj > 0 && jj < ty - 1 && kk > 0 && kk < tz - 1;
+    }
     double cf;
-    if (filt && ii > 0 && ii < tx - 1 && jj > 0 && jj < ty - 1 && kk > 0 && kk < tz - 1) {
+    if (inner) {
         const double b1 = 8.0 / 64, b2 = 4.0 / 64, b3 = 2.0 / 64, b4 = 1.0 / 64;
         long sy = L.pitch, sz = L.plane;
         cf = b1 * c[n] + b2 * (c[n - 1] + c[n - sy] + c[n - sz] + c[n + 1] + c[n + sy] + c[n + sz]) +
@@ -390,7 +422,7 @@ extern "C" int paris_linfunc(paris_handle_t c, int32_t which) {
     double a2 = which == PARIS_FIELD_RHO ? c->d.rho2 : c->d.mu2;
     int mean = which == PARIS_FIELD_RHO ? c->d.dens_mean : c->d.visc_mean;
     int harm = mean == PARIS_MEAN_HARM;
-    long tot = (long)(c->d.nx + 4) * (c->d.ny + 4) * (c->d.nz + 4);
+    const long tot = c->L.total;
     PARIS_LAUNCH_N(c, "linfunc", tot, k_linfunc, div_up(tot, 256), 256, 0, c->fld[PARIS_FIELD_CVOF], c->fld[which], c->L, a1, a2,
                  harm, c->d.nfilter > 0 ? 1 : 0);
     PARIS_CHECK(ctx_ghost_fill(c, c->fld[which]));

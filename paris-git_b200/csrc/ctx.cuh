@@ -30,6 +30,7 @@ struct FastLevel {
     void* tma = nullptr;   // FP32: tensor maps of the level for the TMA-staged sweep (mg_fast.cu)
     bool pairs = false;    // two consecutive sweeps run as one pass (k_rb_sweep4_cfg)
     bool rs = false;       // the last pre-smoothing sweep forms the coarse right-hand side (k_rb_sweep_rs)
+    int merged = 0;        // FP32: the fused sweep with one barrier per step (1: 32x12 tiles, 2: 32x14)
     double omega = 1.0;    // relaxation factor of the red-black smoother, set by each solve
 };
 

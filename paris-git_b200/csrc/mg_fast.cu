@@ -916,6 +916,16 @@ static int rs_levels() {
     return e[0] == '1' ? 1 : (e[0] == '2' ? 2 : 0);
 }
 
+// The FP32 fused sweep with one barrier per step (the merged phases of
+// k_rb_sweep2_cfg<C, true>) when PARIS_SWEEP_MERGED=1 (32x12 tiles) or 2
+// (32x14 tiles) is in the environment as a handle first builds its levels;
+// the same iterate to the bit.
+static int merged_wanted() {
+    const char* e = getenv("PARIS_SWEEP_MERGED");
+    if (!e) return 0;
+    return e[0] == '1' ? 1 : (e[0] == '2' ? 2 : 0);
+}
+
 void mg_fast_free_maps(paris_ctx* c) {
     for (auto& l : c->fl32) {
         delete static_cast<LevelTma*>(l.tma);
@@ -942,6 +952,7 @@ static int fast_alloc(paris_ctx* c) {
         if (fusable) PARIS_CUDA_TRY(c, cudaMalloc(&l.x2, l.N * sizeof(T)));
         l.pairs = fusable && pairs_wanted();
         l.rs = fusable && std::is_same<T, float>::value && (rs_levels() == 2 || (rs_levels() == 1 && L == 0));
+        l.merged = fusable && std::is_same<T, float>::value ? merged_wanted() : 0;
         if constexpr (std::is_same<T, float>::value) level_maps(l);
     }
     return PARIS_OK;
@@ -966,13 +977,13 @@ static int fast_coefs(paris_ctx* c) {
 // Planes per block of the fused sweep: enough blocks for one wave of resident
 // blocks, at least 4 planes per block (2 where that leaves fewer blocks than
 // SMs).
-template <typename T>
-static int sweep_chunk(paris_ctx* c, const FastLevel<T>& l) {
-    using Cfg = typename SwGeo<T>::Cfg;
+template <class Cfg, bool M, typename T>
+static int sweep_chunk_cfg(paris_ctx* c, const FastLevel<T>& l) {
+    constexpr size_t smem = sweep2_smem_cfg<Cfg, M>();
     static int per_sm = 0;   // resident blocks per SM (the same on every B200)
     if (!per_sm) {
-        cudaFuncSetAttribute(k_rb_sweep2_cfg<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<T>());
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rb_sweep2_cfg<Cfg>, Cfg::NT, sweep_smem<T>()) !=
+        cudaFuncSetAttribute(k_rb_sweep2_cfg<Cfg, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rb_sweep2_cfg<Cfg, M>, Cfg::NT, smem) !=
                 cudaSuccess || per_sm < 1)
             per_sm = 1;
     }
@@ -983,6 +994,25 @@ static int sweep_chunk(paris_ctx* c, const FastLevel<T>& l) {
     if (nbz > cap) nbz = cap;
     if (nbz < 1) nbz = 1;
     return (int)div_up(l.n[2], nbz);
+}
+template <typename T>
+static int sweep_chunk(paris_ctx* c, const FastLevel<T>& l) {
+    return sweep_chunk_cfg<typename SwGeo<T>::Cfg, false>(c, l);
+}
+
+// the merged-phase sweep of an FP32 level with configuration Cfg
+template <class Cfg>
+static int sweep_merged(paris_ctx* c, const FastLevel<float>& l, const char* label, const float* xin, float* xout,
+                        const float* xc, int first, double* bx_part, int* bx_blocks) {
+    const int zc = sweep_chunk_cfg<Cfg, true>(c, l);
+    dim3 grid(div_up(l.n[0], Cfg::TX), div_up(l.n[1], Cfg::TY), div_up(l.n[2], zc));
+    if (bx_part && (long)grid.x * grid.y * grid.z > kRedBlocks) bx_part = nullptr;
+    auto* const kern = &k_rb_sweep2_cfg<Cfg, true>;
+    constexpr size_t smem = sweep2_smem_cfg<Cfg, true>();
+    PARIS_LAUNCH_N(c, kname<float>(label), l.N, kern, grid, Cfg::NT, smem, view(l), xin, xout, xc, c->bnd, first, zc,
+                   bx_part);
+    if (bx_part && bx_blocks) *bx_blocks = (int)(grid.x * grid.y * grid.z);
+    return PARIS_OK;
 }
 
 // planes per block of the TMA-staged sweep, as sweep_chunk
@@ -1025,6 +1055,8 @@ static int sweep_fused(paris_ctx* c, int L, const FastLevel<T>& l, const T* xin,
                            view(l), xin, M, xout, xc, c->bnd, first, zc, c->err_dev);
             return PARIS_OK;
         }
+        if (l.merged == 1) return sweep_merged<SwMCfg12>(c, l, label, xin, xout, xc, first, bx_part, bx_blocks);
+        if (l.merged == 2) return sweep_merged<SwMCfg14>(c, l, label, xin, xout, xc, first, bx_part, bx_blocks);
     }
     int zc = sweep_chunk<T>(c, l);
     dim3 grid(div_up(l.n[0], Cfg::TX), div_up(l.n[1], Cfg::TY), div_up(l.n[2], zc));

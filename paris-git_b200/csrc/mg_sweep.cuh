@@ -48,8 +48,12 @@ template <>
 struct SwGeo<double> {
     using Cfg = SwCfg<double, 8, 1, 256, 2>;   // 32x8 tiles: two blocks per SM within shared memory
 };
+// the merged-phase form (FP32, opt-in): its deeper rings fit two blocks per
+// SM with 32x12 or 32x14 tiles
+using SwMCfg12 = SwCfg<float, 12, 1, 256, 2>;
+using SwMCfg14 = SwCfg<float, 14, 1, 288, 2>;
 
-template <class C>
+template <class C, bool M = false>
 static constexpr size_t sweep2_smem_cfg();
 template <typename T>
 static constexpr size_t sweep_smem() {
@@ -133,13 +137,23 @@ __device__ inline int sw_add(int s, int d, int S) {
 // bookkeeping of a step are shared by two planes, and each thread has two
 // independent updates per phase.  Live planes: iterate f0-2..f1+1,
 // coefficients f0-1..f1, cz f0-2..f1, each plus 2D staged ahead.
-template <class C>
+//
+// M (merged phases): the second colour of step s-1 (planes f0-3, f0-2) and
+// the first colour of step s (planes f0, f0+1) run in one phase between two
+// barriers.  They touch disjoint cells: the first colour writes its cells of
+// planes f0, f0+1 and reads second-colour cells of planes f0-1..f0+2, which
+// the second colour of step s-1 does not write; that one writes its cells of
+// planes f0-3, f0-2 and reads first-colour cells of planes f0-4..f0-1, final
+// since the phases before.  One barrier per step instead of two, for a ring
+// two planes deeper (iterate f0-4..f0+2, coefficients f0-3..f0+1, cz
+// f0-4..f0+1, plus 2D staged ahead).
+template <class C, bool M = false>
 struct Sw2 {
     using T = typename C::type;
     static constexpr int NT = C::NT, TY = C::TY, D = C::D;
     static constexpr int TX = C::TX;
     static constexpr int RX = TX + 8, RY = TY + 4, RP = RX * RY;
-    static constexpr int XS = 5 + 2 * D, CS = 3 + 2 * D, ZS = 4 + 2 * D;
+    static constexpr int XS = (M ? 7 : 5) + 2 * D, CS = (M ? 5 : 3) + 2 * D, ZS = (M ? 6 : 4) + 2 * D;
     static constexpr int SLOTS = XS + 3 * CS + ZS;
     static constexpr int FROW = (TX + 2) / 2;
     static constexpr int FCELLS = FROW * (TY + 2);
@@ -154,18 +168,18 @@ struct Sw2 {
     static_assert(CH <= NT, "one chunk of each array per thread");
 };
 
-template <class C>
+template <class C, bool M>
 static constexpr size_t sweep2_smem_cfg() {
-    return sizeof(typename C::type) * (size_t)Sw2<C>::RP * Sw2<C>::SLOTS;
+    return sizeof(typename C::type) * (size_t)Sw2<C, M>::RP * Sw2<C, M>::SLOTS;
 }
 
-template <class C>
+template <class C, bool M = false>
 __global__ void __launch_bounds__(C::NT, C::MINB)
     k_rb_sweep2_cfg(const LV<typename C::type> v, const typename C::type* __restrict__ xin,
                     typename C::type* __restrict__ xout, const typename C::type* __restrict__ xc, const Bnd B,
                     int first, int zc, double* __restrict__ bx_part) {
     using T = typename C::type;
-    using G = Sw2<C>;
+    using G = Sw2<C, M>;
     constexpr int NT = G::NT;
     constexpr int RX = G::RX, RP = G::RP, TY = G::TY, VEC = G::VEC;
     extern __shared__ __align__(16) unsigned char sw_raw[];
@@ -336,10 +350,49 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
         stage_c(z0 + 2 * g, slot(z0 + 2 * g, G::CS), slot(z0 + 2 * g, G::ZS), false);
         cp_async_commit();
     }
+    // the coarse correction of the iterate planes that arrived for step f0:
+    // group 0's, then two per step
+    auto coarse_step = [&](int f0) {
+        if (f0 == z0 - 1) {
+            for (int k = z0 - 2; k <= z0 + 1; k++) {
+                fetch_coarse(0, k);
+                add_coarse(0, k);
+            }
+        } else {
+            if (f0 + 1 <= z1 + 1) add_coarse(0, f0 + 1);   // planes above z1+1 are never staged
+            if (f0 + 2 <= z1 + 1) add_coarse(1, f0 + 2);
+        }
+        fetch_coarse(0, f0 + 3);
+        fetch_coarse(1, f0 + 4);
+    };
+    if constexpr (M) {
+        // slot of plane k >= kb - S in a ring of S slots
+        auto sl = [&](int k, int S) { return (k - kb + S) % S; };
+        auto X = [&](int k) { return rx_ + sl(k, G::XS) * RP; };
+        auto CX = [&](int k) { return rcx + sl(k, G::CS) * RP; };
+        auto CY = [&](int k) { return rcy + sl(k, G::CS) * RP; };
+        auto BB = [&](int k) { return rb + sl(k, G::CS) * RP; };
+        auto CZ = [&](int k) { return rcz + sl(k, G::ZS) * RP; };
+        for (int f0 = z0 - 1; f0 <= z1 + 2; f0 += 2) {
+            cp_async_wait_newest<G::D - 1>();
+            if (xc) coarse_step(f0);
+            __syncthreads();
+            stage_x(f0 + 2 * G::D + 1, sl(f0 + 2 * G::D + 1, G::XS));
+            stage_x(f0 + 2 * G::D + 2, sl(f0 + 2 * G::D + 2, G::XS));
+            stage_c(f0 + 2 * G::D, sl(f0 + 2 * G::D, G::CS), sl(f0 + 2 * G::D, G::ZS), false);
+            stage_c(f0 + 2 * G::D + 1, sl(f0 + 2 * G::D + 1, G::CS), sl(f0 + 2 * G::D + 1, G::ZS), false);
+            cp_async_commit();
+            s_at(f0 - 3, X(f0 - 3), X(f0 - 4), X(f0 - 2), CX(f0 - 3), CY(f0 - 3), BB(f0 - 3), CZ(f0 - 3), CZ(f0 - 4));
+            s_at(f0 - 2, X(f0 - 2), X(f0 - 3), X(f0 - 1), CX(f0 - 2), CY(f0 - 2), BB(f0 - 2), CZ(f0 - 2), CZ(f0 - 3));
+            if (f0 <= z1) f_at(f0, X(f0), X(f0 - 1), X(f0 + 1), CX(f0), CY(f0), BB(f0), CZ(f0), CZ(f0 - 1));
+            if (f0 + 1 <= z1)
+                f_at(f0 + 1, X(f0 + 1), X(f0), X(f0 + 2), CX(f0 + 1), CY(f0 + 1), BB(f0 + 1), CZ(f0 + 1), CZ(f0));
+        }
+    }
     // ring positions of plane f0-2 (iterate, cz) and f0-1 (coefficients),
     // advanced by two each step (plane z0-2 sits in slot 0 of every ring)
     int xb = G::XS - 1, cb = 0, zb = G::ZS - 1;
-    for (int f0 = z0 - 1; f0 <= z1; f0 += 2) {
+    for (int f0 = z0 - 1; f0 <= z1 && !M; f0 += 2) {
         cp_async_wait_newest<G::D - 1>();
         if (xc) {   // the iterate planes that arrived: group 0's, then two per step
             if (f0 == z0 - 1) {
